@@ -1,0 +1,213 @@
+/*
+ * dcaacc.h — C ABI of the B200 QMC measurement accumulators (libdcaacc.so).
+ *
+ * Two accumulators, each behind an opaque handle, with the method set of the reference's
+ * accumulator classes that the CT-AUX / CT-INT solvers call:
+ *
+ *   two-particle (G4):   TpAccumulator<Parameters, DistType::NONE, linalg::GPU>
+ *     include/dca/phys/dca_step/cluster_solver/shared_tools/accumulation/tp/tp_accumulator_gpu.hpp:59-263
+ *   single-particle:     SpAccumulator<Parameters, linalg::GPU>
+ *     include/dca/phys/dca_step/cluster_solver/shared_tools/accumulation/sp/sp_accumulator_gpu.hpp:42-130
+ *
+ * Conventions shared by every entry point:
+ *   - Every function returns a dcaacc_status (0 = success).  On failure,
+ *     dcaacc_last_error() returns a thread-local, human readable message.
+ *   - Complex numbers are interleaved (re, im) doubles.
+ *   - Matrices are column major with an explicit leading dimension, as linalg::Matrix is.
+ *   - Multidimensional outputs use the reference's func::function layout: first index fastest.
+ *   - A handle is bound to the CUDA device that was current when it was created, and is used by
+ *     one host thread at a time (one accumulator object per accumulator thread, as in
+ *     stdthread_qmci_cluster_solver.hpp:523-580).
+ */
+#ifndef DCAACC_H
+#define DCAACC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference throws std::logic_error for misuse (tp_accumulator_gpu.hpp:329-330,
+ * :456-468), std::runtime_error for a failed launch (tp_accumulator_kernels.cu:695-699) and rethrows
+ * std::bad_alloc (tp_accumulator_gpu.hpp:314-317); the C++ wrapper maps these codes back. */
+typedef enum dcaacc_status {
+  DCAACC_OK = 0,
+  DCAACC_INVALID_ARG = 1,    /* bad shape, index table or configuration (logic_error) */
+  DCAACC_NOT_READY = 2,      /* call order violated, e.g. accumulate before reset (logic_error) */
+  DCAACC_OOM = 3,            /* device or host allocation failed (bad_alloc) */
+  DCAACC_CUDA_ERR = 4,       /* a CUDA call or kernel launch failed (runtime_error) */
+  DCAACC_DEVICE_INDEX_ERR = 5, /* a kernel's own bounds check tripped; no memory was touched */
+  DCAACC_UNSUPPORTED = 6     /* valid request that this build does not implement (logic_error) */
+} dcaacc_status;
+
+/* Four-point channels: the reference's FourPointType values (include/dca/phys/four_point_type.hpp:27-33). */
+enum {
+  DCAACC_PH_TRANSVERSE = 1,
+  DCAACC_PH_MAGNETIC = 2,
+  DCAACC_PH_CHARGE = 3,
+  DCAACC_PP_UP_DOWN = 4
+};
+
+/* Arithmetic of the two-particle pipeline. */
+enum {
+  /* FP64 everywhere (the reference's double TP accumulation, mc_options.hpp.in TPAccumulationPrecision). */
+  DCAACC_PRECISION_FP64 = 0,
+  /* Mixed: the NDFT and cluster transform on the tensor cores in split-BF16 with FP32 accumulation,
+   * G in FP32, per-batch G4 partial sums in FP32, running G4 in FP64. */
+  DCAACC_PRECISION_MIXED = 1
+};
+
+/* One spin sector of one measurement: the walker configuration and its M matrix.
+ * Mirrors what CachedNdft::sortConfiguration (cached_ndft_base.hpp:89-129) and
+ * SpAccumulator::accumulate (sp_accumulator.hpp:178-201) read from a Configuration. */
+typedef struct dcaacc_sector {
+  int32_t n;                  /* expansion order (number of vertices); 0 is allowed */
+  const double* tau;          /* [n] imaginary times in [0, beta) (host memory) */
+  const int32_t* left_band;   /* [n] (host memory) */
+  const int32_t* right_band;  /* [n] */
+  const int32_t* left_site;   /* [n] */
+  const int32_t* right_site;  /* [n] */
+  const double* M;            /* n x n, column major (host or device memory, see m_on_device) */
+  int32_t ldm;                /* leading dimension of M, >= n */
+  int32_t m_on_device;        /* 1: M is a device pointer on the handle's device */
+} dcaacc_sector;
+
+/* Static description of the two-particle accumulation: the data the reference reads from
+ * Parameters and its static domains in TpAccumulatorBase's constructor (tp_accumulator_base.hpp:184-208)
+ * and G4Helper::set (g4_helper.cu:34-87). */
+typedef struct dcaacc_tp_config {
+  int32_t n_bands;            /* nb  (BDmn) */
+  int32_t n_sites;            /* Nc  (RClusterDmn = KClusterDmn size) */
+  int32_t n_w_half;           /* four-point fermionic frequencies; Nw = 2 * n_w_half (WTpDmn) */
+  int32_t n_sp_freq;          /* positive single-particle frequencies of the G0 mesh (WDmn = 2 * n_sp_freq) */
+  int32_t n_k_ex;             /* number of momentum transfers (KExchangeDmn) */
+  const int32_t* k_ex;        /* [n_k_ex] cluster-momentum indices of the transfers */
+  int32_t n_w_ex;             /* number of frequency transfers (WExchangeDmn) */
+  const int32_t* w_ex;        /* [n_w_ex] transfers as index shifts (frequency_exchange_domain.cpp:26-48) */
+  int32_t n_channels;
+  const int32_t* channels;    /* [n_channels] DCAACC_PH_* / DCAACC_PP_* */
+  double beta;
+  const double* r_vecs;       /* [n_sites][2] real-space cluster sites */
+  const double* k_vecs;       /* [n_sites][2] cluster momenta */
+  const double* a_vecs;       /* [n_bands][2] intra-cell band positions (electron_band_domain a_vec) */
+  const int32_t* k_add;       /* [n_sites * n_sites], (i,j) at i + Nc*j: index of k_i + k_j */
+  const int32_t* k_sub;       /* [n_sites * n_sites], (i,j) at i + Nc*j: index of k_j - k_i */
+  int32_t non_density;        /* 1: columns of M use the vertex's left band/site (cached_ndft_base.hpp:74-78) */
+  int32_t precision;          /* DCAACC_PRECISION_* */
+  int32_t max_batch;          /* measurements buffered before one fused G4 update (>= 1) */
+  int32_t max_order;          /* upper bound on any sector's n (device buffers are sized for it) */
+  int32_t accumulators;       /* > 1: several handles may add into one G4 (atomic updates) */
+} dcaacc_tp_config;
+
+typedef struct dcaacc_tp dcaacc_tp;
+
+const char* dcaacc_last_error(void);
+
+/* TpAccumulator(G0, parameters) — tp_accumulator_gpu.hpp:265-269.
+ * G0: complex FP64, layout (b1, s1, b2, s2, k, w) over the full single-particle mesh
+ * (2 * n_sp_freq frequencies), i.e. func::function<TpComplex, dmn_variadic<NuDmn, NuDmn, KDmn, WDmn>>.
+ * The handle allocates all device memory it will use (sized by max_order and max_batch). */
+int dcaacc_tp_create(const dcaacc_tp_config* cfg, const double* G0, dcaacc_tp** out);
+
+/* ~TpAccumulator. Null is accepted. */
+void dcaacc_tp_destroy(dcaacc_tp* acc);
+
+/* resetAccumulation(dca_loop) — tp_accumulator_gpu.hpp:285-296: zeroes G4, re-slices G0, arms accumulate. */
+int dcaacc_tp_reset(dcaacc_tp* acc);
+
+/* accumulate(M, configs, sign) — tp_accumulator_gpu.hpp:322-367.
+ * sectors: [2] (spin 0, spin 1).  sign: +1 / -1.  flops_out (may be null) receives the
+ * reference's flop estimate for the call.  In FP64 mode the measurement is processed
+ * immediately; in mixed mode it is queued and processed with its batch (see flush). */
+int dcaacc_tp_accumulate(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t sign, double* flops_out);
+
+/* Batched form: n_meas measurements, sectors [2 * n_meas], signs [n_meas]. */
+int dcaacc_tp_accumulate_batch(dcaacc_tp* acc, int32_t n_meas, const dcaacc_sector* sectors,
+                               const int32_t* signs, double* flops_out);
+
+/* Processes queued measurements now (mixed mode).  No-op when nothing is queued. */
+int dcaacc_tp_flush(dcaacc_tp* acc);
+
+/* finalize() — tp_accumulator_gpu.hpp:471-484: flushes, then copies G4 to the host side of the handle. */
+int dcaacc_tp_finalize(dcaacc_tp* acc);
+
+/* get_G4()[channel] — tp_accumulator_gpu.hpp:503-510.  Copies G4 of one channel (complex FP64,
+ * layout (b1,b2,b3,b4,k1,w1,k2,w2,q,wq)) into out, which holds count complex numbers.
+ * Valid after finalize. */
+int dcaacc_tp_get_g4(const dcaacc_tp* acc, int32_t channel, double* out, size_t count);
+
+/* Number of complex entries of one channel's G4: nb^4 Nc^2 Nw^2 Nq Nwq (dca_data.hpp:108-112). */
+size_t dcaacc_tp_g4_size(const dcaacc_tp* acc);
+
+/* sumTo(other) — the CPU accumulator adds its G4 into other's and clears its own
+ * (tp_accumulator_cpu.hpp:896-904).  Here: other.G4 += this.G4 on the device, this.G4 = 0. */
+int dcaacc_tp_sum_to(dcaacc_tp* acc, dcaacc_tp* other);
+
+/* Debug / parity: copies the last measurement's G for one spin (complex, layout
+ * (b1,b2,k1,k2,w1,w2) over the extended frequency mesh; the reference's G_ without the spin
+ * index, tp_accumulator_base.hpp:79-80).  FP64 mode only. */
+int dcaacc_tp_get_g(const dcaacc_tp* acc, int32_t spin, double* out, size_t count);
+
+/* get_stream() / syncStreams(): the CUDA stream the handle enqueues on (cudaStream_t as void*).
+ * set_stream makes the handle use the caller's stream instead of its own. */
+int dcaacc_tp_set_stream(dcaacc_tp* acc, void* stream);
+void* dcaacc_tp_get_stream(const dcaacc_tp* acc);
+
+/* synchronizeCopy(): returns once host inputs of earlier accumulate calls may be reused. */
+int dcaacc_tp_synchronize(dcaacc_tp* acc);
+
+/* deviceFingerprint() — tp_accumulator_gpu.hpp:148-156: device bytes held by the handle. */
+size_t dcaacc_tp_device_fingerprint(const dcaacc_tp* acc);
+
+/* Number of this library's kernels launched by the handle since creation. */
+uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc);
+
+/* ---------------------------------------------------------------------------------------------
+ * Single-particle accumulator (delayed NFFT): SpAccumulator / Dnfft1DGpu.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct dcaacc_sp_config {
+  int32_t n_bands;
+  int32_t n_sites;
+  int32_t n_sp_freq;          /* positive frequencies of the output mesh (WDmn = 2 * n_sp_freq) */
+  double beta;
+  const int32_t* r_sub;       /* [n_sites * n_sites], (i,j) at i + Nc*j: index of r_j - r_i */
+  int32_t accumulate_m_sqr;   /* also accumulate sign * M^2 (sp_accumulator.hpp:195-196) */
+  int32_t max_order;
+} dcaacc_sp_config;
+
+typedef struct dcaacc_sp dcaacc_sp;
+
+/* SpAccumulator(parameters, accumulate_m_sqr) — sp_accumulator_gpu.hpp:134-144. */
+int dcaacc_sp_create(const dcaacc_sp_config* cfg, dcaacc_sp** out);
+void dcaacc_sp_destroy(dcaacc_sp* acc);
+
+/* resetAccumulation() — sp_accumulator_gpu.hpp:146-158. */
+int dcaacc_sp_reset(dcaacc_sp* acc);
+
+/* accumulate(Ms, configs, factor) — sp_accumulator_gpu.hpp:160-195.  sectors: [2]. */
+int dcaacc_sp_accumulate(dcaacc_sp* acc, const dcaacc_sector* sectors, double sign);
+
+/* finalize() — sp_accumulator_gpu.hpp:215-229, with the fold / DFT / window division of
+ * Dnfft1D::finalize (dnfft_1d.hpp:292-298, :401-489) on the device. */
+int dcaacc_sp_finalize(dcaacc_sp* acc);
+
+/* get_sign_times_M_r_w() / get_sign_times_M_r_w_sqr(): complex FP64, layout (b1,s1,b2,s2,r,w),
+ * count = (2 nb)^2 Nc (2 n_sp_freq) complex numbers.  Valid after finalize. */
+int dcaacc_sp_get_m_r_w(const dcaacc_sp* acc, double* out, size_t count);
+int dcaacc_sp_get_m_r_w_sqr(const dcaacc_sp* acc, double* out, size_t count);
+
+/* sumTo(other) — sp_accumulator_gpu.hpp:231-236: other.f_tau += this.f_tau (time domain). */
+int dcaacc_sp_sum_to(const dcaacc_sp* acc, dcaacc_sp* other);
+
+int dcaacc_sp_set_stream(dcaacc_sp* acc, void* stream);
+int dcaacc_sp_synchronize(dcaacc_sp* acc);
+size_t dcaacc_sp_device_fingerprint(const dcaacc_sp* acc);
+uint64_t dcaacc_sp_kernel_launches(const dcaacc_sp* acc);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* DCAACC_H */
