@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark of the two-particle accumulation hot path (G4 measurements per second).
+
+Workload (default "c3"): single-band Hubbard on the 16-site 4x4 cluster, Nw = 64 fermionic
+frequencies, all 16 momentum transfers, one frequency transfer, channels PH-magnetic + PH-charge,
+per-spin expansion orders n ~ U[50, 400], batches of 64 measurements, synthetic inputs
+(dca_b200.workloads).  One step = one batch of 64 measurements through the whole accumulation
+(twiddles, NDFT + cluster transform + G, G4 update); G4 (2 x 268 MB FP64) and each batch's G
+(1 GB) exceed the 126 MB L2, so no L2 flush is needed between steps.
+
+  value      measurements/s with M already resident in HBM (device pointers), CUDA-event timed
+  e2e        the same through the public API with M in pinned host memory (host->device copies
+             inside the timed region) and a 4 KiB G4 read-back per step, wall-clock timed
+  roofline   the dominant stage, timed with CUDA events on the accumulator's stream
+  cpu_baseline  the reference's own CPU TpAccumulator (oracle/_ref/tp_ref, FP64) on a bounded
+             sample, one single-threaded process per core
+
+--impl reference times the reference's CPU accumulator alone (the same workload and unit).
+Multi-GPU (torchrun): independent replicas, one per GPU; value = all ranks' measurements / the
+slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "G4 meas/s on B200: batched split-BF16 vs plain FP64 at ≤1e-6 rel err; updateG4 HBM %"
+UNIT = "meas/s"
+FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", default="c3")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+# Helpers
+# ------------------------------------------------------------------------------------------------
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, FALLBACK_BF16_TFLOPS, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baseline: the reference's own TpAccumulator<CPU>, one single-threaded process per core
+# ------------------------------------------------------------------------------------------------
+def _cpu_workers(per_worker_bytes):
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        cores = max(1, min(cores, int(avail * 0.6 // per_worker_bytes)))
+    except Exception:
+        pass
+    return max(1, min(cores, 64))
+
+
+def run_cpu_reference(w, n_meas_per_worker, warmup, workers=None, tag="sample"):
+    """Runs oracle/_ref/tp_ref (or the restatement oracle if it is absent) in parallel workers.
+    Returns (meas_per_s, workers, kind, seconds)."""
+    from dca_b200 import workloads as W
+    from oracle import casefile as CF
+    from oracle import pyoracle
+    cl = w.cluster()
+    g0 = W.make_g0(w.model, cl, w.beta, w.chemical_potential(), w.n_sp)
+    g4_bytes = 16 * (w.nb ** 4) * cl.nc ** 2 * (2 * w.nw_half) ** 2 * len(w.exchange_momenta(cl.nc)) * len(
+        w.exchange_frequencies()) * len(w.channels)
+    P = workers or _cpu_workers(g4_bytes * 1.5 + 256e6)
+    kind = "reference" if os.path.exists(pyoracle.REF_BIN) else "port"
+    with tempfile.TemporaryDirectory() as d:
+        procs = []
+        for i in range(P):
+            ms = W.make_measurements(w, n_meas_per_worker, start=10_000 + i * n_meas_per_worker)
+            case = os.path.join(d, f"w{i}.case")
+            CF.write_case(case, w, cl, g0, ms)
+            out = os.path.join(d, f"w{i}.out")
+            if kind == "reference":
+                cmd = [pyoracle.REF_BIN, case, out, "--no-sp", "--time", "--warmup", str(warmup)]
+            else:
+                cmd = [sys.executable, "-c",
+                       "import sys,time;sys.path.insert(0,%r);from oracle import pyoracle;t=time.time();"
+                       "pyoracle.run_case(%r,%r,True,False);print('tp_seconds=%%f'%%(time.time()-t),file=sys.stderr)"
+                       % (ROOT, case, out)]
+            env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+            procs.append(subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
+                                          env=env))
+        secs = []
+        for pr in procs:
+            _, err = pr.communicate()
+            if pr.returncode != 0:
+                raise RuntimeError(f"CPU baseline worker failed: {err}")
+            for tok in err.split():
+                if tok.startswith("tp_seconds="):
+                    secs.append(float(tok.split("=")[1]))
+    timed = n_meas_per_worker - (warmup if kind == "reference" else 0)
+    t = max(secs)
+    return P * timed / t, P, kind, t, timed
+
+
+# ------------------------------------------------------------------------------------------------
+# Our arm
+# ------------------------------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+
+    from dca_b200 import workloads as W
+    from dca_b200.accumulators import TpAccumulator, TpParameters
+
+    torch.cuda.set_device(local)
+    w = W.WORKLOADS[args.workload]
+    cl = w.cluster()
+    g0 = W.make_g0(w.model, cl, w.beta, w.chemical_potential(), w.n_sp)
+    B = w.batch
+    pool = W.make_measurements(w, 2 * B, start=rank * 1_000_000)
+    configs = [list(m.sectors) for m in pool]
+    signs = [m.sign for m in pool]
+    dev_M = [[torch.from_numpy(np.ascontiguousarray(s.M.T)).cuda().t() for s in m.sectors] for m in pool]
+    pinned = []
+    for m in pool:
+        pair = []
+        for s in m.sectors:
+            t = torch.empty((s.n, s.n), dtype=torch.float64, pin_memory=True)
+            t.copy_(torch.from_numpy(np.ascontiguousarray(s.M.T)))
+            pair.append(t.numpy().T)  # column-major view of pinned memory
+        pinned.append(pair)
+
+    params = TpParameters.from_workload(w, cl, precision=1, max_batch=B)
+    acc = TpAccumulator(g0, params)
+    acc.resetAccumulation(0)
+    stream = torch.cuda.ExternalStream(acc.get_stream())
+
+    def step(i, M_src):
+        base = (i % 2) * B
+        for j in range(base, base + B):
+            acc.accumulate(M_src[j], configs[j], signs[j])
+        acc.flush()
+
+    for i in range(args.warmup):
+        step(i, dev_M)
+    torch.cuda.synchronize()
+    acc.enable_timing(True)
+    launches0 = acc.kernel_launches()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(args.steps):
+        step(i, dev_M)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms_local = ev0.elapsed_time(ev1)
+    launches = acc.kernel_launches() - launches0
+    stages = acc.stage_times()
+    ms = max_over_ranks(ms_local, world)
+    n_meas_total = world * args.steps * B
+    value = n_meas_total / (ms / 1e3)
+
+    # End to end: pinned host M (copied to the device inside the timed region), 4 KiB read-back.
+    e2e_acc = acc
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(i, pinned)
+        e2e_acc.peek_G4(0, 0, 256)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    h2d = sum(8 * s.n * s.n for m in pool[:B] for s in m.sectors)
+    e2e = {"value": n_meas_total / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": 256 * 16}
+
+    # Plain FP64, unbatched (the path the mixed one is compared with) and the error between them.
+    fp64 = None
+    err = None
+    if not args.no_fp64:
+        n_cmp = B
+        ref_acc = TpAccumulator(g0, TpParameters.from_workload(w, cl, precision=0, max_batch=1))
+        ref_acc.resetAccumulation(0)
+        for j in range(2):  # warm-up
+            ref_acc.accumulate(dev_M[j], configs[j], signs[j])
+        torch.cuda.synchronize()
+        ref_acc.resetAccumulation(0)
+        rs = torch.cuda.ExternalStream(ref_acc.get_stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(rs)
+        for j in range(n_cmp):
+            ref_acc.accumulate(dev_M[j], configs[j], signs[j])
+        e1.record(rs)
+        torch.cuda.synchronize()
+        fp64_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        fp64 = world * n_cmp / (fp64_ms / 1e3)
+        ref_acc.finalize()
+        mixed_acc = TpAccumulator(g0, params)
+        mixed_acc.resetAccumulation(0)
+        for j in range(n_cmp):
+            mixed_acc.accumulate(dev_M[j], configs[j], signs[j])
+        mixed_acc.finalize()
+        err = [float(np.linalg.norm(a - b) / np.linalg.norm(b))
+               for a, b in zip(mixed_acc.get_G4(), ref_acc.get_G4())]
+        del mixed_acc, ref_acc
+
+    # Roofline of the dominant stage.
+    hbm_gbs, bf16_tf, peak_src = peaks()
+    dom = max(stages, key=lambda k: stages[k][0])
+    dom_ms, dom_launches = stages[dom]
+    per_launch_ms = dom_ms / max(dom_launches, 1)
+    nc, nb, nw = cl.nc, w.nb, 2 * w.nw_half
+    nwe = nw + 2 * w.ext()
+    D = nb * nc * nwe
+    n_g4 = nb ** 4 * nc ** 2 * nw ** 2 * len(w.exchange_momenta(nc)) * len(w.exchange_frequencies())
+    if dom == "update_g4":
+        alg_bytes = len(w.channels) * n_g4 * 32 + B * 2 * D * D * 8
+        roof = {"kernel": "updateG4Kernel<float2,float>", "bound": "hbm",
+                "achieved": alg_bytes / (per_launch_ms / 1e3) / 1e9, "peak": hbm_gbs, "unit": "GB/s",
+                "traffic": None, "peak_source": peak_src}
+    else:
+        # Front-end stages are dominated by their global traffic (M / X' / G, FP32 complex).
+        mean_n = float(np.mean([s.n for m in pool[:B] for s in m.sectors]))
+        if dom == "col_transform":
+            alg_bytes = 2 * B * (D * mean_n * 8 + D * D * 8)
+            kern = "colTransformKernel<float>"
+        elif dom == "row_transform":
+            alg_bytes = 2 * B * (mean_n * mean_n * 8 + D * mean_n * 8)
+            kern = "rowTransformKernel<float,8,8>"
+        else:
+            alg_bytes = 2 * B * mean_n * nwe * 16
+            kern = "twiddleKernel"
+        roof = {"kernel": kern, "bound": "hbm", "achieved": alg_bytes / (per_launch_ms / 1e3) / 1e9,
+                "peak": hbm_gbs, "unit": "GB/s", "traffic": None, "peak_source": peak_src}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["ms_per_launch"] = per_launch_ms
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (G, G4 partials) + fp64 (running G4)",
+        "data": "synthetic (seeded; dca_b200.workloads)",
+        "config": {"workload": f"{w.name}: single-band Hubbard 4x4 (Nc=16), Nw=64, 16 q x 1 wq, "
+                               f"PH-magnetic + PH-charge, n~U[{w.n_range[0]},{w.n_range[1]}], batch {B}",
+                   "measurements_per_step": B, "precision": "mixed", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (G4 537 MB, G 1 GB per batch)"},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
+        "fp64_unbatched_meas_per_s": fp64,
+        "speedup_vs_fp64": (value / fp64) if fp64 else None,
+        "rel_err_vs_fp64": err,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        val, P, kind, t, timed = run_cpu_reference(w, 2, 1)
+        result["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": P, "kind": kind,
+                                  "sample": f"{P} single-threaded processes x {timed} timed c3 measurement "
+                                            f"(after 1 warm-up), FP64 TpAccumulator<CPU>, {t:.1f} s"}
+    return result
+
+
+def run_reference_arm(args, world, rank):
+    from dca_b200 import workloads as W
+    w = W.WORKLOADS[args.workload]
+    if rank != 0:
+        return None
+    per_worker = min(args.warmup + args.steps, 12)
+    warm = min(args.warmup, max(per_worker - 1, 0))
+    val, P, kind, t, timed = run_cpu_reference(w, per_worker, warm)
+    return {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / max(timed, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic (seeded; dca_b200.workloads)",
+            "config": {"workload": f"{w.name}: single-band Hubbard 4x4 (Nc=16), Nw=64, 16 q x 1 wq, "
+                                   f"PH-magnetic + PH-charge, n~U[{w.n_range[0]},{w.n_range[1]}]",
+                       "parallelism": f"{P} CPU processes"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": P, "kind": kind,
+                             "sample": f"{P} processes x {timed} measurements (after {warm} warm-up), "
+                                       f"one step = one measurement per process"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            res = run_reference_arm(args, world, rank)
+        else:
+            res = run_ours(args, world, rank, local)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,332 @@
+"""Python mirror of the reference's accumulator interface, over libdcaacc.so.
+
+Method names, argument meaning and error behaviour follow the classes the CT-AUX / CT-INT
+solvers call:
+
+* ``TpAccumulator`` -- ``TpAccumulator<Parameters, DistType::NONE, linalg::GPU>``
+  (tp_accumulator_gpu.hpp:59-263): ``resetAccumulation``, ``accumulate(M, configs, sign)``,
+  ``finalize``, ``sumTo``, ``get_G4``, ``synchronizeCopy``, ``get_stream``, ``deviceFingerprint``.
+* ``SpAccumulator`` -- ``SpAccumulator<Parameters, linalg::GPU>`` (sp_accumulator_gpu.hpp:42-130):
+  ``resetAccumulation``, ``accumulate``, ``finalize``, ``sumTo``, ``get_sign_times_M_r_w``,
+  ``get_sign_times_M_r_w_sqr``, ``synchronizeCopy``, ``deviceFingerprint``.
+
+Misuse raises ``LogicError`` (the reference's ``std::logic_error``), CUDA failures raise
+``RuntimeError`` (``std::runtime_error``), allocation failures ``MemoryError`` (``std::bad_alloc``).
+
+Inputs: ``M_pair`` is two column-major ``(n, n)`` float64 matrices, either numpy arrays (host) or
+CUDA tensors (device, on the accumulator's device); ``configs`` is two objects with numpy
+attributes ``tau``, ``left_band``, ``right_band``, ``left_site``, ``right_site``
+(``workloads.Sector`` has them).  G4 is returned per channel as complex128 in the reference layout
+(b1, b2, b3, b4, k1, w1, k2, w2, q, wq), first index fastest.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from . import workloads as W
+
+
+class LogicError(ValueError):
+    """Misuse of an accumulator (the reference throws std::logic_error)."""
+
+
+def _raise(status: int):
+    msg = N.lib.dcaacc_last_error().decode(errors="replace")
+    if status in (1, 2, 6):
+        raise LogicError(f"{N.STATUS_NAMES[status]}: {msg}")
+    if status == 3:
+        raise MemoryError(msg)
+    raise RuntimeError(f"{N.STATUS_NAMES.get(status, status)}: {msg}")
+
+
+def _check(status: int):
+    if status != N.OK:
+        _raise(status)
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@dataclasses.dataclass
+class TpParameters:
+    """What TpAccumulatorBase reads from Parameters and the static domains
+    (tp_accumulator_base.hpp:184-208, g4_helper.cu:34-87)."""
+
+    n_bands: int
+    n_sites: int
+    n_w_half: int
+    n_sp_freq: int
+    beta: float
+    channels: Sequence[int]
+    k_ex: Sequence[int]
+    w_ex: Sequence[int]
+    r_vecs: np.ndarray
+    k_vecs: np.ndarray
+    a_vecs: np.ndarray
+    k_add: np.ndarray  # [i, j] = index of k_i + k_j
+    k_sub: np.ndarray  # [i, j] = index of k_j - k_i
+    r_sub: Optional[np.ndarray] = None
+    precision: int = N.PRECISION_FP64
+    max_batch: int = 1
+    max_order: int = 512
+    accumulators: int = 1
+    non_density: bool = False
+
+    @classmethod
+    def from_workload(cls, w: W.Workload, cluster: Optional[W.Cluster] = None, **kw) -> "TpParameters":
+        cl = cluster if cluster is not None else w.cluster()
+        args = dict(
+            n_bands=w.nb, n_sites=cl.nc, n_w_half=w.nw_half, n_sp_freq=w.n_sp, beta=w.beta,
+            channels=list(w.channels), k_ex=w.exchange_momenta(cl.nc), w_ex=w.exchange_frequencies(),
+            r_vecs=cl.r_vecs, k_vecs=cl.k_vecs, a_vecs=w.model.a_vecs(), k_add=cl.k_add,
+            k_sub=cl.k_sub, r_sub=cl.r_sub, max_order=w.n_range[1], max_batch=w.batch)
+        args.update(kw)
+        return cls(**args)
+
+    def g4_shape(self):
+        nb, nc, nw = self.n_bands, self.n_sites, 2 * self.n_w_half
+        # Fortran-order shape of (b1, b2, b3, b4, k1, w1, k2, w2, q, wq).
+        return (nb, nb, nb, nb, nc, nw, nc, nw, len(self.k_ex), len(self.w_ex))
+
+
+def _make_sectors(M_pair, configs, keep: list):
+    secs = (N.Sector * 2)()
+    for s in range(2):
+        c = configs[s]
+        n = int(np.asarray(c.tau).shape[0])
+        arrs = [np.ascontiguousarray(c.tau, np.float64)]
+        for name in ("left_band", "right_band", "left_site", "right_site"):
+            arrs.append(np.ascontiguousarray(getattr(c, name), np.int32))
+        keep.extend(arrs)
+        M = M_pair[s]
+        sec = secs[s]
+        sec.n = n
+        sec.tau = _dptr(arrs[0])
+        sec.left_band, sec.right_band, sec.left_site, sec.right_site = (_iptr(a) for a in arrs[1:])
+        if hasattr(M, "is_cuda") and M.is_cuda:
+            import torch
+
+            if M.dtype != torch.float64:
+                raise LogicError("device M must be float64")
+            if n and not (M.stride(0) == 1 and M.stride(1) >= max(n, 1)):
+                M = M.t().contiguous().t()  # column major
+            keep.append(M)
+            sec.M = ctypes.c_void_p(M.data_ptr())
+            sec.ldm = max(M.stride(1), 1) if n else 1
+            sec.m_on_device = 1
+        else:
+            Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
+            keep.append(Mh)
+            sec.M = ctypes.c_void_p(Mh.ctypes.data)
+            sec.ldm = max(n, 1)
+            sec.m_on_device = 0
+    return secs
+
+
+class TpAccumulator:
+    """Two-particle accumulator (see module docstring)."""
+
+    def __init__(self, G0: np.ndarray, parameters: TpParameters, thread_id: int = 0):
+        p = parameters
+        self.parameters = p
+        self.thread_id = thread_id
+        self._keep = [
+            np.ascontiguousarray(p.k_ex, np.int32), np.ascontiguousarray(p.w_ex, np.int32),
+            np.ascontiguousarray(p.channels, np.int32),
+            np.ascontiguousarray(p.r_vecs, np.float64), np.ascontiguousarray(p.k_vecs, np.float64),
+            np.ascontiguousarray(p.a_vecs, np.float64),
+            # Tables are column major: element (i, j) at i + Nc j.
+            np.ascontiguousarray(np.asarray(p.k_add, np.int32).T),
+            np.ascontiguousarray(np.asarray(p.k_sub, np.int32).T),
+        ]
+        k_ex, w_ex, ch, rv, kv, av, kadd, ksub = self._keep
+        cfg = N.TpConfig(
+            p.n_bands, p.n_sites, p.n_w_half, p.n_sp_freq, len(k_ex), _iptr(k_ex), len(w_ex),
+            _iptr(w_ex), len(ch), _iptr(ch), p.beta, _dptr(rv), _dptr(kv), _dptr(av), _iptr(kadd),
+            _iptr(ksub), int(p.non_density), p.precision, p.max_batch, p.max_order, p.accumulators)
+        g0 = np.ascontiguousarray(G0, np.complex128).reshape(-1)
+        expect = (2 * p.n_bands) ** 2 * p.n_sites * 2 * p.n_sp_freq
+        if g0.size != expect:
+            raise LogicError(f"G0 has {g0.size} entries, expected {expect}")
+        self._h = ctypes.c_void_p()
+        _check(N.lib.dcaacc_tp_create(ctypes.byref(cfg), g0.view(np.float64).ctypes.data_as(
+            ctypes.POINTER(ctypes.c_double)), ctypes.byref(self._h)))
+        self._g4: Optional[List[np.ndarray]] = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib.dcaacc_tp_destroy(h)
+            self._h = None
+
+    # -- reference method set ----------------------------------------------------------------
+    def resetAccumulation(self, dca_loop: int = 0):
+        _check(N.lib.dcaacc_tp_reset(self._h))
+        self._g4 = None
+
+    def accumulate(self, M_pair, configs, sign: int) -> float:
+        keep: list = []
+        secs = _make_sectors(M_pair, configs, keep)
+        flops = ctypes.c_double(0)
+        _check(N.lib.dcaacc_tp_accumulate(self._h, secs, int(sign), ctypes.byref(flops)))
+        self._last_inputs = keep  # device M must outlive the queued work
+        return flops.value
+
+    def flush(self):
+        _check(N.lib.dcaacc_tp_flush(self._h))
+
+    def finalize(self):
+        _check(N.lib.dcaacc_tp_finalize(self._h))
+        size = N.lib.dcaacc_tp_g4_size(self._h)
+        out = []
+        for c in range(len(self.parameters.channels)):
+            g = np.empty(size, np.complex128)
+            _check(N.lib.dcaacc_tp_get_g4(self._h, c, g.view(np.float64).ctypes.data_as(
+                ctypes.POINTER(ctypes.c_double)), size))
+            out.append(g)
+        self._g4 = out
+
+    def get_G4(self) -> List[np.ndarray]:
+        if self._g4 is None:
+            raise LogicError("There is no G4 stored in this class.")
+        return self._g4
+
+    def sumTo(self, other: "TpAccumulator"):
+        _check(N.lib.dcaacc_tp_sum_to(self._h, other._h))
+        self._g4 = None
+
+    def get_G(self, spin: int) -> np.ndarray:
+        """G of the last processed measurement (FP64 mode), layout (b1, b2, k1, k2, w1, w2)."""
+        p = self.parameters
+        ext = max(abs(w) for w in p.w_ex)
+        nwe = 2 * p.n_w_half + 2 * ext
+        size = (p.n_bands * p.n_sites * nwe) ** 2
+        g = np.empty(size, np.complex128)
+        _check(N.lib.dcaacc_tp_get_g(self._h, spin, g.view(np.float64).ctypes.data_as(
+            ctypes.POINTER(ctypes.c_double)), size))
+        return g
+
+    def synchronizeCopy(self):
+        _check(N.lib.dcaacc_tp_synchronize(self._h))
+
+    def syncStreams(self, event=None):
+        self.synchronizeCopy()
+
+    def get_stream(self) -> int:
+        return N.lib.dcaacc_tp_get_stream(self._h) or 0
+
+    def set_stream(self, stream_handle: int):
+        _check(N.lib.dcaacc_tp_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+    def deviceFingerprint(self) -> int:
+        return N.lib.dcaacc_tp_device_fingerprint(self._h)
+
+    def kernel_launches(self) -> int:
+        return N.lib.dcaacc_tp_kernel_launches(self._h)
+
+    STAGES = ("twiddle", "row_transform", "col_transform", "update_g4")
+
+    def enable_timing(self, on: bool = True):
+        _check(N.lib.dcaacc_tp_enable_timing(self._h, int(on)))
+
+    def stage_times(self):
+        """{stage: (cumulative ms, launches)} since enable_timing."""
+        ms = (ctypes.c_double * 4)()
+        cnt = (ctypes.c_uint64 * 4)()
+        _check(N.lib.dcaacc_tp_stage_times(self._h, ms, cnt, 4))
+        return {name: (ms[i], cnt[i]) for i, name in enumerate(self.STAGES)}
+
+    def peek_G4(self, channel: int, offset: int, count: int) -> np.ndarray:
+        out = np.empty(count, np.complex128)
+        _check(N.lib.dcaacc_tp_peek_g4(self._h, channel, offset, count, _dptr(out.view(np.float64))))
+        return out
+
+    def num_channels(self) -> int:
+        return len(self.parameters.channels)
+
+
+@dataclasses.dataclass
+class SpParameters:
+    n_bands: int
+    n_sites: int
+    n_sp_freq: int
+    beta: float
+    r_sub: np.ndarray  # [i, j] = index of r_j - r_i
+    max_order: int = 512
+
+    @classmethod
+    def from_workload(cls, w: W.Workload, cluster: Optional[W.Cluster] = None, **kw):
+        cl = cluster if cluster is not None else w.cluster()
+        args = dict(n_bands=w.nb, n_sites=cl.nc, n_sp_freq=w.n_sp, beta=w.beta, r_sub=cl.r_sub,
+                    max_order=w.n_range[1])
+        args.update(kw)
+        return cls(**args)
+
+
+class SpAccumulator:
+    """Single-particle accumulator (see module docstring)."""
+
+    def __init__(self, parameters: SpParameters, accumulate_m_squared: bool = False):
+        p = parameters
+        self.parameters = p
+        self._rsub = np.ascontiguousarray(np.asarray(p.r_sub, np.int32).T)
+        cfg = N.SpConfig(p.n_bands, p.n_sites, p.n_sp_freq, p.beta, _iptr(self._rsub),
+                         int(accumulate_m_squared), p.max_order)
+        self._sqr = bool(accumulate_m_squared)
+        self._h = ctypes.c_void_p()
+        _check(N.lib.dcaacc_sp_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            N.lib.dcaacc_sp_destroy(h)
+            self._h = None
+
+    def resetAccumulation(self):
+        _check(N.lib.dcaacc_sp_reset(self._h))
+
+    def accumulate(self, M_pair, configs, factor: float):
+        keep: list = []
+        secs = _make_sectors(M_pair, configs, keep)
+        _check(N.lib.dcaacc_sp_accumulate(self._h, secs, float(factor)))
+        self._last_inputs = keep
+
+    def finalize(self):
+        _check(N.lib.dcaacc_sp_finalize(self._h))
+
+    def _get(self, sqr: bool) -> np.ndarray:
+        p = self.parameters
+        size = (2 * p.n_bands) ** 2 * p.n_sites * 2 * p.n_sp_freq
+        out = np.empty(size, np.complex128)
+        fn = N.lib.dcaacc_sp_get_m_r_w_sqr if sqr else N.lib.dcaacc_sp_get_m_r_w
+        _check(fn(self._h, out.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)), size))
+        return out
+
+    def get_sign_times_M_r_w(self) -> np.ndarray:
+        return self._get(False)
+
+    def get_sign_times_M_r_w_sqr(self) -> np.ndarray:
+        return self._get(True)
+
+    def sumTo(self, other: "SpAccumulator"):
+        _check(N.lib.dcaacc_sp_sum_to(self._h, other._h))
+
+    def synchronizeCopy(self):
+        _check(N.lib.dcaacc_sp_synchronize(self._h))
+
+    def deviceFingerprint(self) -> int:
+        return N.lib.dcaacc_sp_device_fingerprint(self._h)
+
+    def kernel_launches(self) -> int:
+        return N.lib.dcaacc_sp_kernel_launches(self._h)

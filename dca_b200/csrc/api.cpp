@@ -1,0 +1,241 @@
+// The C ABI (include/dcaacc.h): status codes around the accumulator objects.
+#include <cuda_runtime.h>
+
+#include <new>
+#include <string>
+
+#include "../../include/dcaacc.h"
+#include "common.cuh"
+#include "sp_accumulator.hpp"
+#include "tp_accumulator.hpp"
+
+struct dcaacc_tp {
+  dcaacc::TpAccumulator impl;
+  dcaacc_tp(const dcaacc_tp_config& c, const double* g0) : impl(c, g0) {}
+};
+struct dcaacc_sp {
+  dcaacc::SpAccumulator impl;
+  explicit dcaacc_sp(const dcaacc_sp_config& c) : impl(c) {}
+};
+
+namespace {
+thread_local std::string g_last_error;
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return DCAACC_OK;
+  }
+  catch (const dcaacc::Error& e) {
+    g_last_error = e.what();
+    return e.status;
+  }
+  catch (const std::bad_alloc& e) {
+    g_last_error = "host allocation failed";
+    return DCAACC_OOM;
+  }
+  catch (const std::exception& e) {
+    g_last_error = e.what();
+    return DCAACC_INVALID_ARG;
+  }
+}
+
+int null_handle() {
+  g_last_error = "null handle";
+  return DCAACC_INVALID_ARG;
+}
+}  // namespace
+
+extern "C" {
+
+const char* dcaacc_last_error(void) {
+  return g_last_error.c_str();
+}
+
+int dcaacc_tp_create(const dcaacc_tp_config* cfg, const double* G0, dcaacc_tp** out) {
+  if (!cfg || !out)
+    return null_handle();
+  *out = nullptr;
+  return guard([&] { *out = new dcaacc_tp(*cfg, G0); });
+}
+
+void dcaacc_tp_destroy(dcaacc_tp* acc) {
+  delete acc;
+}
+
+int dcaacc_tp_reset(dcaacc_tp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.reset(); });
+}
+
+int dcaacc_tp_accumulate(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t sign, double* flops_out) {
+  if (!acc)
+    return null_handle();
+  return guard([&] {
+    const double f = acc->impl.accumulate(sectors, sign);
+    if (flops_out)
+      *flops_out = f;
+  });
+}
+
+int dcaacc_tp_accumulate_batch(dcaacc_tp* acc, int32_t n_meas, const dcaacc_sector* sectors,
+                               const int32_t* signs, double* flops_out) {
+  if (!acc)
+    return null_handle();
+  return guard([&] {
+    if (n_meas < 0 || (n_meas && (!sectors || !signs)))
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "invalid batch");
+    double f = 0;
+    for (int m = 0; m < n_meas; ++m)
+      f += acc->impl.accumulate(sectors + 2 * m, signs[m]);
+    if (flops_out)
+      *flops_out = f;
+  });
+}
+
+int dcaacc_tp_flush(dcaacc_tp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.flush(); });
+}
+
+int dcaacc_tp_finalize(dcaacc_tp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.finalize(); });
+}
+
+int dcaacc_tp_get_g4(const dcaacc_tp* acc, int32_t channel, double* out, size_t count) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.getG4(channel, out, count); });
+}
+
+size_t dcaacc_tp_g4_size(const dcaacc_tp* acc) {
+  return acc ? acc->impl.g4Size() : 0;
+}
+
+int dcaacc_tp_sum_to(dcaacc_tp* acc, dcaacc_tp* other) {
+  if (!acc || !other)
+    return null_handle();
+  return guard([&] { acc->impl.sumTo(other->impl); });
+}
+
+int dcaacc_tp_get_g(const dcaacc_tp* acc, int32_t spin, double* out, size_t count) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.getG(spin, out, count); });
+}
+
+int dcaacc_tp_set_stream(dcaacc_tp* acc, void* stream) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.setStream(static_cast<cudaStream_t>(stream)); });
+}
+
+void* dcaacc_tp_get_stream(const dcaacc_tp* acc) {
+  return acc ? static_cast<void*>(acc->impl.stream()) : nullptr;
+}
+
+int dcaacc_tp_synchronize(dcaacc_tp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.synchronize(); });
+}
+
+size_t dcaacc_tp_device_fingerprint(const dcaacc_tp* acc) {
+  return acc ? acc->impl.deviceFingerprint() : 0;
+}
+
+uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc) {
+  return acc ? acc->impl.kernelLaunches() : 0;
+}
+
+int dcaacc_tp_enable_timing(dcaacc_tp* acc, int32_t on) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.enableTiming(on != 0); });
+}
+
+int dcaacc_tp_stage_times(dcaacc_tp* acc, double* ms, uint64_t* launches, int32_t n_stages) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.stageTimes(ms, launches, n_stages); });
+}
+
+int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.peekG4(channel, offset, count, out); });
+}
+
+int dcaacc_sp_create(const dcaacc_sp_config* cfg, dcaacc_sp** out) {
+  if (!cfg || !out)
+    return null_handle();
+  *out = nullptr;
+  return guard([&] { *out = new dcaacc_sp(*cfg); });
+}
+
+void dcaacc_sp_destroy(dcaacc_sp* acc) {
+  delete acc;
+}
+
+int dcaacc_sp_reset(dcaacc_sp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.reset(); });
+}
+
+int dcaacc_sp_accumulate(dcaacc_sp* acc, const dcaacc_sector* sectors, double sign) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.accumulate(sectors, sign); });
+}
+
+int dcaacc_sp_finalize(dcaacc_sp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.finalize(); });
+}
+
+int dcaacc_sp_get_m_r_w(const dcaacc_sp* acc, double* out, size_t count) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.get(false, out, count); });
+}
+
+int dcaacc_sp_get_m_r_w_sqr(const dcaacc_sp* acc, double* out, size_t count) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.get(true, out, count); });
+}
+
+int dcaacc_sp_sum_to(const dcaacc_sp* acc, dcaacc_sp* other) {
+  if (!acc || !other)
+    return null_handle();
+  return guard([&] { acc->impl.sumTo(other->impl); });
+}
+
+int dcaacc_sp_set_stream(dcaacc_sp* acc, void* stream) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.setStream(static_cast<cudaStream_t>(stream)); });
+}
+
+int dcaacc_sp_synchronize(dcaacc_sp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.synchronize(); });
+}
+
+size_t dcaacc_sp_device_fingerprint(const dcaacc_sp* acc) {
+  return acc ? acc->impl.deviceFingerprint() : 0;
+}
+
+uint64_t dcaacc_sp_kernel_launches(const dcaacc_sp* acc) {
+  return acc ? acc->impl.kernelLaunches() : 0;
+}
+
+}  // extern "C"

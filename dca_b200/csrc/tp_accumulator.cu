@@ -1,0 +1,576 @@
+// Host side of the two-particle accumulator (see tp_accumulator.hpp).
+#include "tp_accumulator.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "tp_frontend.hpp"
+#include "tp_g4.hpp"
+
+namespace dcaacc {
+
+namespace {
+[[noreturn]] void invalid(const std::string& msg) {
+  throw Error(DCAACC_INVALID_ARG, msg);
+}
+}  // namespace
+
+TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
+  // ---- validation (the reference's logic_error cases, tp_accumulator_base.hpp:197-198,
+  // tp_accumulator_gpu.hpp:456-468, plus the index tables G4Helper::set trusts) ----
+  if (c.n_bands < 1 || c.n_sites < 1 || c.n_w_half < 1 || c.n_sp_freq < 1)
+    invalid("band, site and frequency counts must be positive");
+  if (c.n_k_ex < 1 || !c.k_ex || c.n_w_ex < 1 || !c.w_ex)
+    invalid("at least one momentum and one frequency transfer are required");
+  if (c.n_channels < 1 || c.n_channels > kMaxChannels || !c.channels)
+    invalid("between 1 and 4 channels are supported");
+  if (!(c.beta > 0) || !std::isfinite(c.beta))
+    invalid("beta must be positive");
+  if (!c.r_vecs || !c.k_vecs || !c.a_vecs || !c.k_add || !c.k_sub || !G0)
+    invalid("null table pointer");
+  if (c.precision != DCAACC_PRECISION_FP64 && c.precision != DCAACC_PRECISION_MIXED)
+    invalid("unknown precision mode");
+  if (c.max_batch < 1 || c.max_order < 1)
+    invalid("max_batch and max_order must be positive");
+  const int nc = c.n_sites, nb = c.n_bands;
+  if (nb * nc > 1024)
+    invalid("nb * Nc must not exceed 1024");
+  for (int i = 0; i < nc * nc; ++i)
+    if (c.k_add[i] < 0 || c.k_add[i] >= nc || c.k_sub[i] < 0 || c.k_sub[i] >= nc)
+      invalid("momentum add/subtract table entry out of range");
+  for (int i = 0; i < c.n_k_ex; ++i)
+    if (c.k_ex[i] < 0 || c.k_ex[i] >= nc)
+      invalid("momentum transfer index out of range");
+  int ext = 0;
+  for (int i = 0; i < c.n_w_ex; ++i)
+    ext = std::max(ext, std::abs(c.w_ex[i]));
+  for (int i = 0; i < c.n_channels; ++i)
+    if (c.channels[i] < DCAACC_PH_TRANSVERSE || c.channels[i] > DCAACC_PP_UP_DOWN)
+      throw Error(DCAACC_UNSUPPORTED, "Specified four point type not implemented.");
+  const int nw = 2 * c.n_w_half, nw_ext = nw + 2 * ext;
+  if (2 * c.n_sp_freq < nw_ext)
+    invalid("The number of single particle frequencies is too small.");
+
+  dims_.nb = nb;
+  dims_.nc = nc;
+  dims_.nw = nw;
+  dims_.ext = ext;
+  dims_.nw_ext = nw_ext;
+  dims_.n_orb = nb * nc;
+  dims_.R = nb * nc;
+  dims_.nq = c.n_k_ex;
+  dims_.nwq = c.n_w_ex;
+  dims_.n_channels = c.n_channels;
+  for (int i = 0; i < kMaxChannels; ++i)
+    dims_.channels[i] = i < c.n_channels ? c.channels[i] : 0;
+  dims_.beta = c.beta;
+  mixed_ = c.precision == DCAACC_PRECISION_MIXED;
+  non_density_ = c.non_density != 0;
+  atomic_ = c.accumulators > 1;
+  max_batch_ = c.max_batch;
+  max_order_ = c.max_order;
+  n_sp_ = c.n_sp_freq;
+  k_add_.assign(c.k_add, c.k_add + nc * nc);
+  k_sub_.assign(c.k_sub, c.k_sub + nc * nc);
+  q_list_.assign(c.k_ex, c.k_ex + c.n_k_ex);
+  wex_list_.assign(c.w_ex, c.w_ex + c.n_w_ex);
+  g4_size_ = size_t(nb) * nb * nb * nb * nc * nc * nw * nw * c.n_k_ex * c.n_w_ex;
+  const long R = dims_.R;
+  g_sector_stride_ = long(nw_ext) * nw_ext * R * R;
+
+  DCAACC_CUDA_CHECK(cudaGetDevice(&device_));
+  DCAACC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  own_stream_ = true;
+  DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&upload_done_, cudaEventDisableTiming));
+
+  // ---- G0 slice over the extended mesh (tp_accumulator_base.hpp:210-221) ----
+  {
+    const int sp_offset = (2 * c.n_sp_freq - nw_ext) / 2;
+    std::vector<double2> g0(size_t(nb) * nb * nc * nw_ext * 2);
+    for (int s = 0; s < 2; ++s)
+      for (int w = 0; w < nw_ext; ++w)
+        for (int k = 0; k < nc; ++k)
+          for (int b2 = 0; b2 < nb; ++b2)
+            for (int b1 = 0; b1 < nb; ++b1) {
+              const size_t in =
+                  b1 + nb * (s + 2 * (b2 + nb * (s + 2 * (k + size_t(nc) * (w + sp_offset)))));
+              g0[b1 + nb * (b2 + nb * (k + size_t(nc) * (w + size_t(nw_ext) * s)))] =
+                  make_double2(G0[2 * in], G0[2 * in + 1]);
+            }
+    G0_.alloc(g0.size());
+    DCAACC_CUDA_CHECK(cudaMemcpy(G0_.get(), g0.data(), G0_.bytes(), cudaMemcpyHostToDevice));
+  }
+  // ---- cluster transform with band phases: Fb(r, k, b) = e^{i k.r} e^{i k.a_b}
+  // (space_transform_2D.hpp:93-140) ----
+  {
+    std::vector<double2> fb(size_t(nb) * nc * nc);
+    for (int b = 0; b < nb; ++b)
+      for (int k = 0; k < nc; ++k) {
+        const double kx = c.k_vecs[2 * k], ky = c.k_vecs[2 * k + 1];
+        const std::complex<double> ph =
+            std::exp(std::complex<double>(0, kx * c.a_vecs[2 * b] + ky * c.a_vecs[2 * b + 1]));
+        for (int r = 0; r < nc; ++r) {
+          const std::complex<double> t =
+              std::exp(std::complex<double>(0, kx * c.r_vecs[2 * r] + ky * c.r_vecs[2 * r + 1]));
+          const std::complex<double> v = t * ph;
+          fb[(size_t(b) * nc + k) * nc + r] = make_double2(v.real(), v.imag());
+        }
+      }
+    Fb_.alloc(fb.size());
+    DCAACC_CUDA_CHECK(cudaMemcpy(Fb_.get(), fb.data(), Fb_.bytes(), cudaMemcpyHostToDevice));
+  }
+  auto upload_ints = [](DevBuf<int>& d, const std::vector<int>& h) {
+    d.alloc(h.size());
+    DCAACC_CUDA_CHECK(cudaMemcpy(d.get(), h.data(), d.bytes(), cudaMemcpyHostToDevice));
+  };
+  upload_ints(k_add_d_, k_add_);
+  upload_ints(k_sub_d_, k_sub_);
+  upload_ints(q_d_, q_list_);
+  upload_ints(wex_d_, wex_list_);
+
+  // ---- G4 per channel ----
+  G4_ = std::vector<DevBuf<double2>>(c.n_channels);
+  std::vector<double2*> ptrs;
+  for (auto& g : G4_) {
+    g.alloc(g4_size_);
+    DCAACC_CUDA_CHECK(cudaMemset(g.get(), 0, g.bytes()));
+    ptrs.push_back(g.get());
+  }
+  G4_ptrs_.alloc(ptrs.size());
+  DCAACC_CUDA_CHECK(cudaMemcpy(G4_ptrs_.get(), ptrs.data(), G4_ptrs_.bytes(), cudaMemcpyHostToDevice));
+
+  // ---- batch workspace ----
+  const size_t n_sec = 2 * size_t(max_batch_);
+  const size_t n_vtx = n_sec * max_order_;
+  const size_t n_orb1 = dims_.n_orb + 1;
+  sectors_d_.alloc(n_sec);
+  tau_d_.alloc(n_vtx);
+  perm_r_d_.alloc(n_vtx);
+  perm_c_d_.alloc(n_vtx);
+  rstart_d_.alloc(n_sec * n_orb1);
+  cstart_d_.alloc(n_sec * n_orb1);
+  signs_d_.alloc(max_batch_);
+  Tr_d_.alloc(n_vtx * nw_ext);
+  if (non_density_)
+    Tc_d_.alloc(n_vtx * nw_ext);
+  M_d_.alloc(n_sec * size_t(max_order_) * max_order_);
+  const size_t x_elems = n_sec * size_t(R) * max_order_ * nw_ext;
+  const size_t g_elems = n_sec * size_t(g_sector_stride_);
+  if (mixed_) {
+    X32_.alloc(x_elems);
+    G32_.alloc(g_elems);
+  }
+  else {
+    X64_.alloc(x_elems);
+    G64_.alloc(g_elems);
+  }
+  sectors_h_.alloc(n_sec);
+  tau_h_.alloc(n_vtx);
+  perm_r_h_.alloc(n_vtx);
+  perm_c_h_.alloc(n_vtx);
+  rstart_h_.alloc(n_sec * n_orb1);
+  cstart_h_.alloc(n_sec * n_orb1);
+  signs_h_.alloc(max_batch_);
+  DCAACC_CUDA_CHECK(cudaEventRecord(upload_done_, stream_));
+
+  if (frontendSmemRequirement(dims_, max_order_, !mixed_) > 227 * 1024)
+    invalid("max_order too large for the front-end's shared-memory tiles");
+  G4_host_.assign(c.n_channels, {});
+}
+
+TpAccumulator::~TpAccumulator() {
+  if (stream_)
+    cudaStreamSynchronize(stream_);
+  for (auto& t : timed_) {
+    cudaEventDestroy(t.begin);
+    cudaEventDestroy(t.end);
+  }
+  if (upload_done_)
+    cudaEventDestroy(upload_done_);
+  if (own_stream_ && stream_)
+    cudaStreamDestroy(stream_);
+}
+
+void TpAccumulator::reset() {
+  // resetAccumulation: zero G4 and arm accumulate (tp_accumulator_gpu.hpp:285-296).
+  DCAACC_CUDA_CHECK(cudaEventSynchronize(upload_done_));
+  slots_ = 0;
+  vtx_used_ = 0;
+  x_used_ = 0;
+  n_max_batch_ = 0;
+  for (auto& g : G4_)
+    DCAACC_CUDA_CHECK(cudaMemsetAsync(g.get(), 0, g.bytes(), stream_));
+  ready_ = true;
+  finalized_ = false;
+  have_g_ = false;
+}
+
+void TpAccumulator::validateSector(const dcaacc_sector& s) const {
+  if (s.n < 0)
+    invalid("negative expansion order");
+  if (s.n > max_order_)
+    invalid("expansion order " + std::to_string(s.n) + " exceeds max_order " +
+            std::to_string(max_order_));
+  if (s.n == 0)
+    return;
+  if (!s.tau || !s.left_band || !s.right_band || !s.left_site || !s.right_site || !s.M)
+    invalid("null sector pointer");
+  if (s.ldm < s.n)
+    invalid("leading dimension of M smaller than n");
+  for (int i = 0; i < s.n; ++i) {
+    if (s.left_band[i] < 0 || s.left_band[i] >= dims_.nb || s.right_band[i] < 0 ||
+        s.right_band[i] >= dims_.nb)
+      invalid("vertex band out of range");
+    if (s.left_site[i] < 0 || s.left_site[i] >= dims_.nc || s.right_site[i] < 0 ||
+        s.right_site[i] >= dims_.nc)
+      invalid("vertex site out of range");
+    if (!std::isfinite(s.tau[i]))
+      invalid("vertex time is not finite");
+  }
+}
+
+double TpAccumulator::flopEstimate(const dcaacc_sector* sec) const {
+  // Algorithmic flops of this implementation for one measurement: NDFT rows + columns,
+  // both cluster transforms, the G0 epilogue, and the G4 update (18 / 26 flops per entry and
+  // channel, the reference's convention in tp_accumulator_kernels.cu:704-723).
+  const double nwe = dims_.nw_ext, R = dims_.R, D = R * nwe, nc = dims_.nc, nb = dims_.nb;
+  double f = 0;
+  for (int s = 0; s < 2; ++s) {
+    const double n = sec[s].n;
+    f += 8 * nwe * n * n / (nb * nc) * nb + 8 * D * n * nc;  // row NDFT per orbital + row transform
+    f += 8 * D * nwe * n + 8 * D * D * nc;                    // column NDFT + column transform
+    f += (nb == 1 ? 12 : 16 * nb) * D * D;                   // G0 epilogue
+  }
+  for (int c = 0; c < dims_.n_channels; ++c)
+    f += (dims_.channels[c] == DCAACC_PH_MAGNETIC || dims_.channels[c] == DCAACC_PH_CHARGE ? 26.0 : 18.0) *
+         double(g4_size_);
+  return f;
+}
+
+void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
+  if (slots_ == 0)
+    DCAACC_CUDA_CHECK(cudaEventSynchronize(upload_done_));  // staging buffers free again
+  const int slot = slots_;
+  const int n_orb = dims_.n_orb;
+  for (int s = 0; s < 2; ++s) {
+    const dcaacc_sector& x = sec[s];
+    const int n = x.n;
+    const int vtx_off = vtx_used_;
+    const int sidx = 2 * slot + s;
+    const int orb_off = sidx * (n_orb + 1);
+    // Orbital of each vertex on the row side (right band / site) and the column side
+    // (left band / site for non-density-density models), cached_ndft_base.hpp:97-103.
+    // A counting sort keeps vertex order inside an orbital, i.e. the reference's
+    // (orbital, idx) ordering.
+    auto sort_side = [&](bool left, int* perm, int* start) {
+      std::fill(start, start + n_orb + 1, 0);
+      for (int v = 0; v < n; ++v) {
+        const int o = left ? x.left_band[v] + dims_.nb * x.left_site[v]
+                           : x.right_band[v] + dims_.nb * x.right_site[v];
+        start[o + 1]++;
+      }
+      for (int o = 0; o < n_orb; ++o)
+        start[o + 1] += start[o];
+      std::vector<int> fill(start, start + n_orb);
+      for (int v = 0; v < n; ++v) {
+        const int o = left ? x.left_band[v] + dims_.nb * x.left_site[v]
+                           : x.right_band[v] + dims_.nb * x.right_site[v];
+        perm[fill[o]++] = v;
+      }
+    };
+    sort_side(false, perm_r_h_.get() + vtx_off, rstart_h_.get() + orb_off);
+    if (non_density_)
+      sort_side(true, perm_c_h_.get() + vtx_off, cstart_h_.get() + orb_off);
+    else {
+      std::copy_n(perm_r_h_.get() + vtx_off, n, perm_c_h_.get() + vtx_off);
+      std::copy_n(rstart_h_.get() + orb_off, n_orb + 1, cstart_h_.get() + orb_off);
+    }
+    std::copy_n(x.tau, n, tau_h_.get() + vtx_off);
+
+    const double* Mptr = x.M;
+    int ldm = std::max(x.ldm, 1);
+    if (n && !x.m_on_device) {
+      double* dst = M_d_.get() + size_t(sidx) * max_order_ * max_order_;
+      DCAACC_CUDA_CHECK(cudaMemcpy2DAsync(dst, sizeof(double) * n, x.M, sizeof(double) * x.ldm,
+                                          sizeof(double) * n, n, cudaMemcpyHostToDevice, stream_));
+      Mptr = dst;
+      ldm = n;
+    }
+    SectorDesc d{};
+    d.M = Mptr;
+    d.ldm = ldm;
+    d.n = n;
+    d.vtx_off = vtx_off;
+    d.orb_off = orb_off;
+    d.spin = s;
+    d.slot = slot;
+    d.x_off = x_used_;
+    sectors_h_[sidx] = d;
+    x_used_ += long(dims_.R) * n * dims_.nw_ext;
+    vtx_used_ += n;
+    n_max_batch_ = std::max(n_max_batch_, n);
+  }
+  signs_h_[slot] = sign;
+  ++slots_;
+}
+
+void TpAccumulator::process() {
+  if (slots_ == 0)
+    return;
+  const int n_sec = 2 * slots_;
+  const int n_orb1 = dims_.n_orb + 1;
+  auto h2d = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes)
+      DCAACC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
+  };
+  h2d(sectors_d_.get(), sectors_h_.get(), sizeof(SectorDesc) * n_sec);
+  h2d(tau_d_.get(), tau_h_.get(), sizeof(double) * vtx_used_);
+  h2d(perm_r_d_.get(), perm_r_h_.get(), sizeof(int) * vtx_used_);
+  h2d(perm_c_d_.get(), perm_c_h_.get(), sizeof(int) * vtx_used_);
+  h2d(rstart_d_.get(), rstart_h_.get(), sizeof(int) * n_sec * n_orb1);
+  h2d(cstart_d_.get(), cstart_h_.get(), sizeof(int) * n_sec * n_orb1);
+  h2d(signs_d_.get(), signs_h_.get(), sizeof(int) * slots_);
+  DCAACC_CUDA_CHECK(cudaEventRecord(upload_done_, stream_));
+
+  FrontendArgs fa{};
+  fa.dims = dims_;
+  fa.sectors = sectors_d_.get();
+  fa.n_sectors = n_sec;
+  fa.n_max = n_max_batch_;
+  fa.tau = tau_d_.get();
+  fa.perm_r = perm_r_d_.get();
+  fa.perm_c = non_density_ ? perm_c_d_.get() : perm_r_d_.get();
+  fa.row_start = rstart_d_.get();
+  fa.col_start = non_density_ ? cstart_d_.get() : rstart_d_.get();
+  fa.Tr = Tr_d_.get();
+  fa.Tc = non_density_ ? Tc_d_.get() : Tr_d_.get();
+  fa.Fb = Fb_.get();
+  fa.G0 = G0_.get();
+  if (n_max_batch_ > 0) {
+    cudaEvent_t b = nullptr;
+    timeBegin(DCAACC_STAGE_TWIDDLE, &b);
+    launchTwiddles(fa, stream_);
+    launches_ += non_density_ ? 2 : 1;
+    timeEnd(DCAACC_STAGE_TWIDDLE, b, non_density_ ? 2 : 1);
+  }
+  G4Args ga{};
+  ga.dims = dims_;
+  ga.signs = signs_d_.get();
+  ga.n_slots = slots_;
+  ga.k_add = k_add_d_.get();
+  ga.k_sub = k_sub_d_.get();
+  ga.q_list = q_d_.get();
+  ga.wex_list = wex_d_.get();
+  ga.G4 = G4_ptrs_.get();
+  ga.atomic = atomic_;
+  cudaEvent_t b = nullptr;
+  timeBegin(DCAACC_STAGE_ROW, &b);
+  if (mixed_)
+    launchRowTransform<float>(fa, X32_.get(), stream_);
+  else
+    launchRowTransform<double>(fa, X64_.get(), stream_);
+  timeEnd(DCAACC_STAGE_ROW, b, 1);
+  timeBegin(DCAACC_STAGE_COL, &b);
+  if (mixed_)
+    launchColTransform<float>(fa, X32_.get(), G32_.get(), g_sector_stride_, stream_);
+  else
+    launchColTransform<double>(fa, X64_.get(), G64_.get(), g_sector_stride_, stream_);
+  timeEnd(DCAACC_STAGE_COL, b, 1);
+  timeBegin(DCAACC_STAGE_G4, &b);
+  if (mixed_)
+    launchUpdateG4<float2>(ga, G32_.get(), g_sector_stride_, stream_);
+  else
+    launchUpdateG4<double2>(ga, G64_.get(), g_sector_stride_, stream_);
+  timeEnd(DCAACC_STAGE_G4, b, 1);
+  launches_ += 3;
+  have_g_ = !mixed_;
+  slots_ = 0;
+  vtx_used_ = 0;
+  x_used_ = 0;
+  n_max_batch_ = 0;
+}
+
+double TpAccumulator::accumulate(const dcaacc_sector* sectors, int sign) {
+  if (!ready_)
+    throw Error(DCAACC_NOT_READY, "The accumulator is not ready to measure.");
+  if (!sectors)
+    invalid("null sectors");
+  if (sign != 1 && sign != -1)
+    invalid("sign must be +1 or -1");
+  validateSector(sectors[0]);
+  validateSector(sectors[1]);
+  if (sectors[0].n + sectors[1].n == 0)  // empty configuration (tp_accumulator_cpu.hpp:238-239)
+    return 0.;
+  if (slots_ == max_batch_)
+    process();
+  stage(sectors, sign);
+  if (slots_ == max_batch_)
+    process();
+  return flopEstimate(sectors);
+}
+
+void TpAccumulator::flush() {
+  process();
+}
+
+void TpAccumulator::finalize() {
+  if (finalized_)
+    return;
+  process();
+  for (size_t c = 0; c < G4_.size(); ++c) {
+    G4_host_[c].resize(g4_size_);
+    DCAACC_CUDA_CHECK(cudaMemcpyAsync(G4_host_[c].data(), G4_[c].get(), G4_[c].bytes(),
+                                      cudaMemcpyDeviceToHost, stream_));
+  }
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  finalized_ = true;
+  ready_ = false;
+}
+
+void TpAccumulator::getG4(int channel, double* out, size_t count) const {
+  if (!finalized_)
+    throw Error(DCAACC_NOT_READY, "G4 is available after finalize().");
+  if (channel < 0 || channel >= static_cast<int>(G4_host_.size()))
+    invalid("channel index out of range");
+  if (count != g4_size_)
+    invalid("output size does not match the G4 size");
+  std::memcpy(out, G4_host_[channel].data(), 16 * count);
+}
+
+void TpAccumulator::sumTo(TpAccumulator& other) {
+  if (other.G4_.size() != G4_.size() || other.g4_size_ != g4_size_)
+    invalid("Objects accumulate different number of channels.");
+  if (other.device_ != device_)
+    invalid("sumTo requires both accumulators on the same device");
+  process();
+  other.process();
+  cudaEvent_t ev;
+  DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  DCAACC_CUDA_CHECK(cudaEventRecord(ev, other.stream_));
+  DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, ev, 0));
+  for (size_t c = 0; c < G4_.size(); ++c) {
+    launchAddAndClear(other.G4_[c].get(), G4_[c].get(), g4_size_, stream_);
+    ++launches_;
+  }
+  DCAACC_CUDA_CHECK(cudaEventRecord(ev, stream_));
+  DCAACC_CUDA_CHECK(cudaStreamWaitEvent(other.stream_, ev, 0));
+  DCAACC_CUDA_CHECK(cudaEventDestroy(ev));
+  other.finalized_ = false;
+}
+
+void TpAccumulator::getG(int spin, double* out, size_t count) const {
+  if (mixed_)
+    throw Error(DCAACC_UNSUPPORTED, "G is kept for inspection in FP64 mode only");
+  if (!have_g_)
+    throw Error(DCAACC_NOT_READY, "no measurement has been processed");
+  if (spin < 0 || spin > 1)
+    invalid("spin must be 0 or 1");
+  const int nb = dims_.nb, nc = dims_.nc, nwe = dims_.nw_ext, R = dims_.R;
+  const size_t total = size_t(g_sector_stride_);
+  if (count != total)
+    invalid("output size does not match the G size");
+  std::vector<double2> blk(total);
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  DCAACC_CUDA_CHECK(cudaMemcpy(blk.data(), G64_.get() + size_t(spin) * g_sector_stride_,
+                               sizeof(double2) * total, cudaMemcpyDeviceToHost));
+  // Block layout ((wr nwe + wc) R + r) R + c  ->  (b1, b2, k1, k2, w1, w2).
+  for (int wc = 0; wc < nwe; ++wc)
+    for (int wr = 0; wr < nwe; ++wr)
+      for (int r = 0; r < R; ++r)
+        for (int cc = 0; cc < R; ++cc) {
+          const int b1 = r % nb, k1 = r / nb, b2 = cc % nb, k2 = cc / nb;
+          const size_t o = b1 + nb * (b2 + nb * (k1 + nc * (k2 + size_t(nc) * (wr + size_t(nwe) * wc))));
+          const double2 v = blk[((size_t(wr) * nwe + wc) * R + r) * R + cc];
+          out[2 * o] = v.x;
+          out[2 * o + 1] = v.y;
+        }
+}
+
+void TpAccumulator::timeBegin(int, cudaEvent_t* b) {
+  *b = nullptr;
+  if (!timing_)
+    return;
+  DCAACC_CUDA_CHECK(cudaEventCreate(b));
+  DCAACC_CUDA_CHECK(cudaEventRecord(*b, stream_));
+}
+
+void TpAccumulator::timeEnd(int stage, cudaEvent_t b, int launches) {
+  if (!timing_ || !b)
+    return;
+  cudaEvent_t e;
+  DCAACC_CUDA_CHECK(cudaEventCreate(&e));
+  DCAACC_CUDA_CHECK(cudaEventRecord(e, stream_));
+  timed_.push_back(Timed{stage, b, e});
+  stage_launches_[stage] += launches;
+}
+
+void TpAccumulator::collectTimes() {
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  for (auto& t : timed_) {
+    float ms = 0;
+    DCAACC_CUDA_CHECK(cudaEventElapsedTime(&ms, t.begin, t.end));
+    stage_ms_[t.stage] += ms;
+    cudaEventDestroy(t.begin);
+    cudaEventDestroy(t.end);
+  }
+  timed_.clear();
+}
+
+void TpAccumulator::enableTiming(bool on) {
+  collectTimes();
+  timing_ = on;
+  for (int i = 0; i < DCAACC_N_STAGES; ++i) {
+    stage_ms_[i] = 0;
+    stage_launches_[i] = 0;
+  }
+}
+
+void TpAccumulator::stageTimes(double* ms, uint64_t* launches, int n) {
+  if (n < 0 || n > DCAACC_N_STAGES)
+    invalid("n_stages out of range");
+  collectTimes();
+  for (int i = 0; i < n; ++i) {
+    if (ms)
+      ms[i] = stage_ms_[i];
+    if (launches)
+      launches[i] = stage_launches_[i];
+  }
+}
+
+void TpAccumulator::peekG4(int channel, size_t offset, size_t count, double* out) {
+  if (channel < 0 || channel >= static_cast<int>(G4_.size()))
+    invalid("channel index out of range");
+  if (offset > g4_size_ || count > g4_size_ - offset)
+    invalid("window outside G4");
+  process();
+  DCAACC_CUDA_CHECK(cudaMemcpyAsync(out, G4_[channel].get() + offset, 16 * count,
+                                    cudaMemcpyDeviceToHost, stream_));
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+void TpAccumulator::setStream(cudaStream_t s) {
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  if (own_stream_)
+    DCAACC_CUDA_CHECK(cudaStreamDestroy(stream_));
+  own_stream_ = false;
+  stream_ = s;
+}
+
+void TpAccumulator::synchronize() {
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+size_t TpAccumulator::deviceFingerprint() const {
+  size_t b = G0_.bytes() + Fb_.bytes() + k_add_d_.bytes() + k_sub_d_.bytes() + q_d_.bytes() +
+             wex_d_.bytes() + G4_ptrs_.bytes() + sectors_d_.bytes() + tau_d_.bytes() +
+             M_d_.bytes() + perm_r_d_.bytes() + perm_c_d_.bytes() + rstart_d_.bytes() +
+             cstart_d_.bytes() + signs_d_.bytes() + Tr_d_.bytes() + Tc_d_.bytes() + X64_.bytes() +
+             G64_.bytes() + X32_.bytes() + G32_.bytes();
+  for (const auto& g : G4_)
+    b += g.bytes();
+  return b;
+}
+
+}  // namespace dcaacc

@@ -1,0 +1,182 @@
+// Host side of the two-particle accumulator: the object behind a dcaacc_tp handle.
+//
+// Mirrors TpAccumulator<Parameters, DistType::NONE, linalg::GPU>
+// (tp_accumulator_gpu.hpp:59-263): resetAccumulation, accumulate, finalize, sumTo, get_G4,
+// get_stream / synchronizeCopy / deviceFingerprint.  Differences by design:
+//   * each handle owns its G4 (the reference keeps one process-wide static device G4,
+//     tp_accumulator_gpu.hpp:493-497); several accumulator threads combine with sumTo;
+//   * in mixed precision, measurements are queued and processed in batches of max_batch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/dcaacc.h"
+#include "common.cuh"
+#include "tp_layout.hpp"
+
+namespace dcaacc {
+
+// Owning device buffer.
+template <typename T>
+class DevBuf {
+public:
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p_)
+      cudaFree(p_);
+  }
+  void alloc(size_t n) {
+    if (p_)
+      cudaFree(p_);
+    p_ = nullptr;
+    n_ = n;
+    if (n)
+      DCAACC_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+  }
+  T* get() const {
+    return p_;
+  }
+  size_t size() const {
+    return n_;
+  }
+  size_t bytes() const {
+    return n_ * sizeof(T);
+  }
+
+private:
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+// Owning pinned host buffer.
+template <typename T>
+class PinBuf {
+public:
+  PinBuf() = default;
+  PinBuf(const PinBuf&) = delete;
+  PinBuf& operator=(const PinBuf&) = delete;
+  ~PinBuf() {
+    if (p_)
+      cudaFreeHost(p_);
+  }
+  void alloc(size_t n) {
+    if (p_)
+      cudaFreeHost(p_);
+    p_ = nullptr;
+    n_ = n;
+    if (n)
+      DCAACC_CUDA_CHECK(cudaMallocHost(&p_, n * sizeof(T)));
+  }
+  T* get() const {
+    return p_;
+  }
+  T& operator[](size_t i) {
+    return p_[i];
+  }
+  size_t size() const {
+    return n_;
+  }
+
+private:
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+class TpAccumulator {
+public:
+  TpAccumulator(const dcaacc_tp_config& cfg, const double* G0);
+  ~TpAccumulator();
+
+  void reset();
+  double accumulate(const dcaacc_sector* sectors, int sign);
+  void flush();
+  void finalize();
+  void getG4(int channel, double* out, size_t count) const;
+  void sumTo(TpAccumulator& other);
+  void getG(int spin, double* out, size_t count) const;
+  void setStream(cudaStream_t s);
+  cudaStream_t stream() const {
+    return stream_;
+  }
+  void synchronize();
+  size_t deviceFingerprint() const;
+  uint64_t kernelLaunches() const {
+    return launches_;
+  }
+  size_t g4Size() const {
+    return g4_size_;
+  }
+  void enableTiming(bool on);
+  void stageTimes(double* ms, uint64_t* launches, int n);
+  void peekG4(int channel, size_t offset, size_t count, double* out);
+
+private:
+  void validateSector(const dcaacc_sector& s) const;
+  void stage(const dcaacc_sector* sectors, int sign);
+  void process();
+  double flopEstimate(const dcaacc_sector* sectors) const;
+
+  // Configuration.
+  TpDims dims_{};
+  bool mixed_ = false;
+  bool non_density_ = false;
+  bool atomic_ = false;
+  int max_batch_ = 1, max_order_ = 1;
+  int n_sp_ = 0;
+  std::vector<int> k_add_, k_sub_, q_list_, wex_list_;
+  size_t g4_size_ = 0;
+  long g_sector_stride_ = 0;  // complex elements of one (slot, spin) G
+
+  // Device state.
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  bool own_stream_ = false;
+  cudaEvent_t upload_done_ = nullptr;
+  DevBuf<double2> G0_, Fb_;
+  DevBuf<int> k_add_d_, k_sub_d_, q_d_, wex_d_;
+  std::vector<DevBuf<double2>> G4_;
+  DevBuf<double2*> G4_ptrs_;
+  // Batch workspace.
+  DevBuf<SectorDesc> sectors_d_;
+  DevBuf<double> tau_d_, M_d_;
+  DevBuf<int> perm_r_d_, perm_c_d_, rstart_d_, cstart_d_, signs_d_;
+  DevBuf<double2> Tr_d_, Tc_d_;
+  DevBuf<double2> X64_, G64_;  // FP64 mode
+  DevBuf<float2> X32_, G32_;   // mixed mode
+  // Pinned staging of the batch being assembled.
+  PinBuf<SectorDesc> sectors_h_;
+  PinBuf<double> tau_h_;
+  PinBuf<int> perm_r_h_, perm_c_h_, rstart_h_, cstart_h_, signs_h_;
+
+  // Batch bookkeeping.
+  int slots_ = 0;         // measurements staged
+  int vtx_used_ = 0;      // packed vertices staged
+  long x_used_ = 0;       // X' elements reserved
+  int n_max_batch_ = 0;   // largest order staged
+  bool ready_ = false;    // reset() called since the last finalize
+  bool finalized_ = false;
+  bool have_g_ = false;   // FP64 mode: G of the last measurement is in G64_
+  uint64_t launches_ = 0;
+  std::vector<std::vector<std::complex<double>>> G4_host_;
+
+  // Stage timing: pairs of events per recorded launch group.
+  struct Timed {
+    int stage;
+    cudaEvent_t begin, end;
+  };
+  bool timing_ = false;
+  std::vector<Timed> timed_;
+  double stage_ms_[4] = {0, 0, 0, 0};
+  uint64_t stage_launches_[4] = {0, 0, 0, 0};
+  void timeBegin(int stage, cudaEvent_t* b);
+  void timeEnd(int stage, cudaEvent_t b, int launches);
+  void collectTimes();
+};
+
+}  // namespace dcaacc

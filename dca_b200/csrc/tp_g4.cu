@@ -1,0 +1,227 @@
+// G4 update: G4(b1,b2,b3,b4,k1,w1,k2,w2,q,wq) += sum over a batch of measurements.
+//
+// Replaces the reference's updateG4Kernel (tp_accumulator_kernels.cu:255-681, one thread per G4
+// entry with a 10-level div/mod unroll of its linear index and one launch per channel per
+// measurement) by one kernel that:
+//   * assigns a CTA to a (w1, w2, wq) tile and lets its threads walk the tile's entries in G4's
+//     memory order (b1..b4, k1 contiguous; k2, q strided), so every G4 load and store is coalesced
+//     and each G4 entry is read and written exactly once per launch;
+//   * updates every configured channel in the same pass (the channels share the G blocks);
+//   * loops over all measurements of a batch with the partial sums in registers, then adds them
+//     to the FP64 running G4 once (the FP32-partials mode of the mixed path); with a batch of one
+//     and FP64 G and partials it is the plain FP64 update.
+//
+// Channel formulas (spin-symmetric branch of TpAccumulator<CPU>::updateG4,
+// tp_accumulator_cpu.hpp:452-666), written with Gd_s(r, wr; c, wc) = G_(b_r, b_c, s, k_r, k_c, wr, wc),
+// r = b + nb k, the band transpose of getGMultiband (tp_accumulator_cpu.hpp:389-405) applied:
+//   PH_MAGNETIC  s/2 [ dG(b1 k1, w1; b2 k1+q, w1+x) dG(b4 k2+q, w2+x; b3 k2, w2)
+//                      - sum_s Gd_s(b1 k1, w1; b3 k2, w2) Gd_s(b4 k2+q, w2+x; b2 k1+q, w1+x) ],
+//                dG = Gd_0 - Gd_1
+//   PH_CHARGE    s/2 [ sG(b1 k1, w1; b2 k1+q, w1+x) sG(b4 k2+q, w2+x; b3 k2, w2)
+//                      - sum_s Gd_s(b4 k1, w1; b1 k2, w2) Gd_s(b3 k2+q, w2+x; b2 k1+q, w1+x) ],
+//                sG = Gd_0 + Gd_1
+//   PH_TRANSVERSE  -s/2 sum_s Gd_s(b4 k1, w1; b2 k2, w2) Gd_{!s}(b1 k2+q, w2+x; b3 k1+q, w1+x)
+//   PP_UP_DOWN      s/2 sum_s Gd_s(b3 k1, w1; b1 k2, w2) Gd_{!s}(b4 q-k1, m1; b2 q-k2, m2),
+//                m = x + Nw - 1 - w
+// with s the measurement sign, x the frequency transfer, compact w shifted by ext onto the
+// extended mesh of G.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "tp_g4.hpp"
+
+namespace dcaacc {
+
+namespace {
+
+template <typename GT, typename AT>
+__device__ inline cplx_t<AT> ldG(const GT* p) {
+  const GT v = __ldg(p);
+  return mk(static_cast<AT>(v.x), static_cast<AT>(v.y));
+}
+
+template <typename GT, typename AT, int EPT>
+__global__ void __launch_bounds__(256)
+updateG4Kernel(const TpDims dims, const GT* __restrict__ G, long g_sector_stride,
+               const int* __restrict__ signs, int n_slots, const int* __restrict__ k_add,
+               const int* __restrict__ k_sub, const int* __restrict__ q_list,
+               const int* __restrict__ wex_list, double2* const* __restrict__ G4, bool atomic) {
+  using C = cplx_t<AT>;
+  const int nb = dims.nb, nc = dims.nc, nw = dims.nw, nw_ext = dims.nw_ext, R = dims.R;
+  const int w1 = blockIdx.x, w2 = blockIdx.y, iwq = blockIdx.z;
+  const int wex = wex_list[iwq];
+  const int ext = dims.ext;
+  const int nb2 = nb * nb, nb4 = nb2 * nb2;
+  const int inner = nb4 * nc;                 // (b1, b2, b3, b4, k1)
+  const long per_tile = static_cast<long>(inner) * nc * dims.nq;
+  const long blk_stride = static_cast<long>(R) * R;
+
+  // Extended frequency indices of the blocks this tile reads.
+  const int w1e = w1 + ext, w2e = w2 + ext;
+  const int w1x = w1e + wex, w2x = w2e + wex;
+  const int m1 = wex + nw - 1 - w1 + ext, m2 = wex + nw - 1 - w2 + ext;
+  auto blk = [&](int wr, int wc) { return (static_cast<long>(wr) * nw_ext + wc) * blk_stride; };
+  const long bA = blk(w1e, w2e), bB = blk(w2x, w1x), bC = blk(w1e, w1x), bE = blk(w2x, w2e),
+             bP = blk(m1, m2);
+
+  // G4 offset of (b=0, k1=0, w1, k2=0, w2, q=0, wq): strides of the (k2, q) part follow.
+  const long s_w1 = inner;
+  const long s_k2 = s_w1 * nw;
+  const long s_w2 = s_k2 * nc;
+  const long s_q = s_w2 * nw;
+  const long s_wq = s_q * dims.nq;
+  const long tile_base = w1 * s_w1 + w2 * s_w2 + iwq * s_wq;
+
+  for (long chunk = 0; chunk < per_tile; chunk += static_cast<long>(EPT) * blockDim.x) {
+    C acc[EPT][kMaxChannels];
+#pragma unroll
+    for (int e = 0; e < EPT; ++e)
+#pragma unroll
+      for (int c = 0; c < kMaxChannels; ++c)
+        acc[e][c] = mk(AT(0), AT(0));
+
+    for (int slot = 0; slot < n_slots; ++slot) {
+      const AT half_sign = AT(0.5) * static_cast<AT>(signs[slot]);
+      const GT* G0s = G + g_sector_stride * (2 * slot);
+      const GT* G1s = G0s + g_sector_stride;
+#pragma unroll
+      for (int e = 0; e < EPT; ++e) {
+        const long idx = chunk + threadIdx.x + static_cast<long>(e) * blockDim.x;
+        if (idx >= per_tile)
+          break;
+        const int in = static_cast<int>(idx % inner);
+        const int outer = static_cast<int>(idx / inner);  // k2 + nc * q
+        const int b1 = in % nb, b2 = (in / nb) % nb, b3 = (in / nb2) % nb, b4 = (in / (nb2 * nb)) % nb;
+        const int k1 = in / nb4;
+        const int k2 = outer % nc, iq = outer / nc;
+        const int q = q_list[iq];
+        const int k1q = k_add[k1 + nc * q], k2q = k_add[k2 + nc * q];
+        auto rc = [&](int b, int k) { return b + nb * k; };
+#pragma unroll
+        for (int c = 0; c < kMaxChannels; ++c) {
+          if (c >= dims.n_channels)
+            break;
+          const int ch = dims.channels[c];
+          C v = mk(AT(0), AT(0));
+          if (ch == 2 || ch == 3) {  // PH_MAGNETIC / PH_CHARGE
+            const long ia = bC + rc(b1, k1) * R + rc(b2, k1q);
+            const long ib = bE + rc(b4, k2q) * R + rc(b3, k2);
+            const C a0 = ldG<GT, AT>(G0s + ia), a1 = ldG<GT, AT>(G1s + ia);
+            const C e0 = ldG<GT, AT>(G0s + ib), e1 = ldG<GT, AT>(G1s + ib);
+            const AT sg = ch == 2 ? AT(-1) : AT(1);
+            const C u = mk(a0.x + sg * a1.x, a0.y + sg * a1.y);
+            const C w = mk(e0.x + sg * e1.x, e0.y + sg * e1.y);
+            v = cmul(u, w);
+            long id, ie;
+            if (ch == 2) {
+              id = bA + rc(b1, k1) * R + rc(b3, k2);
+              ie = bB + rc(b4, k2q) * R + rc(b2, k1q);
+            }
+            else {
+              id = bA + rc(b4, k1) * R + rc(b1, k2);
+              ie = bB + rc(b3, k2q) * R + rc(b2, k1q);
+            }
+            C d = cmul(ldG<GT, AT>(G0s + id), ldG<GT, AT>(G0s + ie));
+            cfma(d, ldG<GT, AT>(G1s + id), ldG<GT, AT>(G1s + ie));
+            v = csub(v, d);
+          }
+          else if (ch == 1) {  // PH_TRANSVERSE
+            const long id = bA + rc(b4, k1) * R + rc(b2, k2);
+            const long ie = bB + rc(b1, k2q) * R + rc(b3, k1q);
+            C d = cmul(ldG<GT, AT>(G0s + id), ldG<GT, AT>(G1s + ie));
+            cfma(d, ldG<GT, AT>(G1s + id), ldG<GT, AT>(G0s + ie));
+            v = mk(-d.x, -d.y);
+          }
+          else if (ch == 4) {  // PP_UP_DOWN
+            const int qk1 = k_sub[k1 + nc * q], qk2 = k_sub[k2 + nc * q];
+            const long id = bA + rc(b3, k1) * R + rc(b1, k2);
+            const long ie = bP + rc(b4, qk1) * R + rc(b2, qk2);
+            v = cmul(ldG<GT, AT>(G0s + id), ldG<GT, AT>(G1s + ie));
+            cfma(v, ldG<GT, AT>(G1s + id), ldG<GT, AT>(G0s + ie));
+          }
+          acc[e][c].x = fma(half_sign, v.x, acc[e][c].x);
+          acc[e][c].y = fma(half_sign, v.y, acc[e][c].y);
+        }
+      }
+    }
+
+    // One read-modify-write of the FP64 running sum per entry and channel.
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      const long idx = chunk + threadIdx.x + static_cast<long>(e) * blockDim.x;
+      if (idx >= per_tile)
+        break;
+      const int in = static_cast<int>(idx % inner);
+      const int outer = static_cast<int>(idx / inner);
+      const int k2 = outer % nc, iq = outer / nc;
+      const long g4i = tile_base + in + k2 * s_k2 + iq * s_q;
+#pragma unroll
+      for (int c = 0; c < kMaxChannels; ++c) {
+        if (c >= dims.n_channels)
+          break;
+        double2* p = G4[c] + g4i;
+        if (atomic) {
+          atomicAdd(&p->x, static_cast<double>(acc[e][c].x));
+          atomicAdd(&p->y, static_cast<double>(acc[e][c].y));
+        }
+        else {
+          double2 old = *p;
+          old.x += static_cast<double>(acc[e][c].x);
+          old.y += static_cast<double>(acc[e][c].y);
+          *p = old;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+template <typename GT>
+void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
+  const dim3 grid(a.dims.nw, a.dims.nw, a.dims.nwq);
+  if constexpr (std::is_same_v<GT, double2>) {
+    updateG4Kernel<double2, double, 4><<<grid, 256, 0, stream>>>(
+        a.dims, G, g_sector_stride, a.signs, a.n_slots, a.k_add, a.k_sub, a.q_list, a.wex_list,
+        a.G4, a.atomic);
+  }
+  else {
+    updateG4Kernel<float2, float, 8><<<grid, 256, 0, stream>>>(
+        a.dims, G, g_sector_stride, a.signs, a.n_slots, a.k_add, a.k_sub, a.q_list, a.wex_list,
+        a.G4, a.atomic);
+  }
+  DCAACC_LAUNCH_CHECK();
+}
+
+template void launchUpdateG4<double2>(const G4Args&, const double2*, long, cudaStream_t);
+template void launchUpdateG4<float2>(const G4Args&, const float2*, long, cudaStream_t);
+
+}  // namespace dcaacc
+
+namespace dcaacc {
+
+namespace {
+__global__ void addAndClearKernel(double2* __restrict__ dst, double2* __restrict__ src, size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const double2 a = src[i];
+    double2 b = dst[i];
+    b.x += a.x;
+    b.y += a.y;
+    dst[i] = b;
+    src[i] = make_double2(0.0, 0.0);
+  }
+}
+}  // namespace
+
+void launchAddAndClear(double2* dst, double2* src, size_t n, cudaStream_t stream) {
+  if (!n)
+    return;
+  const int blocks = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16));
+  addAndClearKernel<<<blocks, 256, 0, stream>>>(dst, src, n);
+  DCAACC_LAUNCH_CHECK();
+}
+
+}  // namespace dcaacc

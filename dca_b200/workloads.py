@@ -255,7 +255,7 @@ def make_g0(model: Model, cluster: Cluster, beta: float, mu: float, n_sp: int) -
 class Workload:
     name: str
     model: Model
-    cluster_kind: Tuple  # ("square", L) or ("betts8",)
+    cluster_kind: Tuple  # ("square", L), ("rect", R1, R2) or ("betts8",)
     beta: float
     nw_half: int  # four-point fermionic frequencies (Nw = 2 nw_half)
     n_sp: int  # single-particle fermionic frequencies (positive)
@@ -269,8 +269,11 @@ class Workload:
     mu: Optional[float] = None
 
     def cluster(self) -> Cluster:
-        if self.cluster_kind[0] == "square":
+        kind = self.cluster_kind[0]
+        if kind == "square":
             return square_cluster(self.cluster_kind[1])
+        if kind == "rect":
+            return make_cluster(self.cluster_kind[1], self.cluster_kind[2])
         return betts8_cluster()
 
     @property

@@ -164,6 +164,22 @@ size_t dcaacc_tp_device_fingerprint(const dcaacc_tp* acc);
 /* Number of this library's kernels launched by the handle since creation. */
 uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc);
 
+/* Stage timers, the counterpart of the reference's Profiler scopes in the accumulator
+ * ("Frequency FT", "Space FT", "ComputeG", "updateG4": tp_accumulator_cpu.hpp:236-280,
+ * tp_accumulator_gpu_base.hpp:214-219).  When enabled, CUDA events bracket each launch on the
+ * handle's stream.  stage_times writes the cumulative milliseconds and launch counts of
+ * DCAACC_N_STAGES stages (twiddles, row transform, column transform + G, G4 update) since the
+ * last enable, synchronizing the stream first. */
+enum { DCAACC_STAGE_TWIDDLE = 0, DCAACC_STAGE_ROW = 1, DCAACC_STAGE_COL = 2, DCAACC_STAGE_G4 = 3,
+       DCAACC_N_STAGES = 4 };
+int dcaacc_tp_enable_timing(dcaacc_tp* acc, int32_t on);
+int dcaacc_tp_stage_times(dcaacc_tp* acc, double* ms, uint64_t* launches, int32_t n_stages);
+
+/* Reads count complex entries of one channel's running G4 starting at offset, without finalizing
+ * (processes queued measurements first, then a synchronous device-to-host copy).  For monitoring
+ * an accumulation in progress. */
+int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out);
+
 /* ---------------------------------------------------------------------------------------------
  * Single-particle accumulator (delayed NFFT): SpAccumulator / Dnfft1DGpu.
  * ------------------------------------------------------------------------------------------- */

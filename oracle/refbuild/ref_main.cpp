@@ -11,10 +11,12 @@
 // the reference's parameter setup does, with mock cluster domains that carry the case's
 // lattice vectors and add/subtract tables.
 //
-// Usage: tp_ref <case.bin> <out.bin> [--no-tp] [--no-sp] [--time]
-//   --time prints "tp_seconds=<s> sp_seconds=<s> n_meas=<m>" on stderr.
+// Usage: tp_ref <case.bin> <out.bin> [--no-tp] [--no-sp] [--time] [--warmup W]
+//   --time prints "tp_seconds=<s> sp_seconds=<s> n_meas=<m>" on stderr, the seconds covering the
+//   measurements after the first W.
 #include <array>
 #include <chrono>
+#include <cstdlib>
 #include <complex>
 #include <cstdint>
 #include <iostream>
@@ -224,7 +226,8 @@ public:
 namespace harness {
 
 template <int NB>
-int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool do_sp, bool timing) {
+int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool do_sp, bool timing,
+        int warmup) {
   using namespace dca;
   using P = Params<NB>;
   P pars;
@@ -284,9 +287,12 @@ int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool d
 
     phys::solver::accumulator::TpAccumulator<P, DistType::NONE, linalg::CPU> acc(G0, pars);
     acc.resetAccumulation();
-    const auto t0 = std::chrono::steady_clock::now();
-    for (int m = 0; m < n_meas; ++m)
+    auto t0 = std::chrono::steady_clock::now();
+    for (int m = 0; m < n_meas; ++m) {
+      if (m == warmup)
+        t0 = std::chrono::steady_clock::now();
       acc.accumulate(Ms[m], confs[m], static_cast<std::int8_t>(c.meas[m].sign));
+    }
     tp_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     for (const auto& g4 : acc.get_G4()) {
       res.G4.emplace_back(g4.size());
@@ -299,9 +305,12 @@ int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool d
     const bool sqr = c.flags & 1;
     phys::solver::accumulator::SpAccumulator<P, linalg::CPU> sp(pars, sqr);
     sp.resetAccumulation();
-    const auto t0 = std::chrono::steady_clock::now();
-    for (int m = 0; m < n_meas; ++m)
+    auto t0 = std::chrono::steady_clock::now();
+    for (int m = 0; m < n_meas; ++m) {
+      if (m == warmup)
+        t0 = std::chrono::steady_clock::now();
       sp.accumulate(Ms[m], confs[m], static_cast<double>(c.meas[m].sign));
+    }
     sp_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     sp.finalize();
     const auto& mrw = sp.get_sign_times_M_r_w();
@@ -329,12 +338,15 @@ int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool d
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    std::cerr << "usage: tp_ref <case.bin> <out.bin> [--no-tp] [--no-sp] [--time]\n";
+    std::cerr << "usage: tp_ref <case.bin> <out.bin> [--no-tp] [--no-sp] [--time] [--warmup W]\n";
     return 2;
   }
   bool do_tp = true, do_sp = true, timing = false;
+  int warmup = 0;
   for (int i = 3; i < argc; ++i) {
     const std::string a = argv[i];
+    if (a == "--warmup" && i + 1 < argc)
+      warmup = std::atoi(argv[++i]);
     if (a == "--no-tp")
       do_tp = false;
     else if (a == "--no-sp")
@@ -346,11 +358,11 @@ int main(int argc, char** argv) {
     const auto c = casefile::readCase(argv[1]);
     switch (c.nb) {
       case 1:
-        return harness::run<1>(c, argv[2], do_tp, do_sp, timing);
+        return harness::run<1>(c, argv[2], do_tp, do_sp, timing, warmup);
       case 2:
-        return harness::run<2>(c, argv[2], do_tp, do_sp, timing);
+        return harness::run<2>(c, argv[2], do_tp, do_sp, timing, warmup);
       case 3:
-        return harness::run<3>(c, argv[2], do_tp, do_sp, timing);
+        return harness::run<3>(c, argv[2], do_tp, do_sp, timing, warmup);
       default:
         std::cerr << "unsupported band count " << c.nb << "\n";
         return 2;

@@ -1,0 +1,55 @@
+"""The C ABI library loads and exports what include/dcaacc.h declares; host-side validation."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "dcaacc.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dcaacc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from dca_b200 import _native
+    syms = declared_symbols()
+    assert len(syms) >= 29
+    for s in syms:
+        assert hasattr(_native.lib, s), s
+
+
+def test_invalid_configuration_rejected_before_any_device_work():
+    from dca_b200 import _native as N
+    from dca_b200 import workloads as W
+    w = W.WORKLOADS["c1"]
+    cl = w.cluster()
+    k_ex = np.array([0], np.int32)
+    w_ex = np.array([0], np.int32)
+    ch = np.array([9], np.int32)  # not a FourPointType
+    rv = np.ascontiguousarray(cl.r_vecs)
+    kv = np.ascontiguousarray(cl.k_vecs)
+    av = np.zeros((1, 2))
+    kadd = np.ascontiguousarray(cl.k_add.T.astype(np.int32))
+    ksub = np.ascontiguousarray(cl.k_sub.T.astype(np.int32))
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    cfg = N.TpConfig(1, cl.nc, 8, 64, 1, ip(k_ex), 1, ip(w_ex), 1, ip(ch), 10.0, dp(rv), dp(kv),
+                     dp(av), ip(kadd), ip(ksub), 0, 0, 1, 64, 1)
+    g0 = np.zeros(4 * cl.nc * 128 * 2)
+    h = ctypes.c_void_p()
+    assert N.lib.dcaacc_tp_create(ctypes.byref(cfg), dp(g0), ctypes.byref(h)) == 6  # UNSUPPORTED
+    ch[0] = N.PRECISION_FP64 + 2
+    kadd[0, 0] = 99  # corrupt table
+    assert N.lib.dcaacc_tp_create(ctypes.byref(cfg), dp(g0), ctypes.byref(h)) == 1  # INVALID_ARG
+    assert b"out of range" in N.lib.dcaacc_last_error()
+    kadd[0, 0] = 0
+    cfg.n_sp_freq = 2  # too few single-particle frequencies for the extended mesh
+    assert N.lib.dcaacc_tp_create(ctypes.byref(cfg), dp(g0), ctypes.byref(h)) == 1
+    assert b"too small" in N.lib.dcaacc_last_error()
+    assert N.lib.dcaacc_tp_reset(None) == 1

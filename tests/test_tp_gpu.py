@@ -1,0 +1,154 @@
+"""Two-particle accumulator on the GPU, through the C ABI, against the oracle / reference outputs."""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES
+from helpers import case_from_workload, golden, rel_err
+from dca_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12   # plain FP64 path vs the FP64 reference
+MIXED_TOL = 1e-6   # mixed-precision path vs FP64 (relative Frobenius error per channel)
+
+
+def run_gpu(case, measurements=None, **kw):
+    from dca_b200.accumulators import TpAccumulator
+    acc = TpAccumulator(case.G0, case.tp_params(**kw))
+    acc.resetAccumulation(0)
+    for m in (measurements if measurements is not None else case.measurements):
+        acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    acc.finalize()
+    return acc
+
+
+def run_oracle(oracle_lib, case, measurements=None, **kw):
+    acc = oracle_lib.OracleTp(case.G0, case.tp_params(**kw))
+    for m in (measurements if measurements is not None else case.measurements):
+        acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    return acc
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_fp64_matches_reference_golden(name):
+    case, ref = golden(name)
+    acc = run_gpu(case)
+    for got, want in zip(acc.get_G4(), ref.g4):
+        assert rel_err(got, want) <= FP64_TOL
+
+
+@pytest.mark.parametrize("name", ["sq2_all", "mb3_all", "sq4_q5"])
+def test_fp64_g_matches_oracle(oracle_lib, name):
+    case, _ = golden(name)
+    m = case.measurements[-1]
+    acc = run_gpu(case, [m])
+    ora = run_oracle(oracle_lib, case, [m])
+    for spin in range(2):
+        assert rel_err(acc.get_G(spin), ora.get_G(spin)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_mixed_matches_reference_golden(name):
+    case, ref = golden(name)
+    acc = run_gpu(case, precision=1, max_batch=2)
+    for got, want in zip(acc.get_G4(), ref.g4):
+        assert rel_err(got, want) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("wname", ["c2", "c4"])
+def test_fp64_full_size_matches_oracle(oracle_lib, wname):
+    case = case_from_workload(W.WORKLOADS[wname], 1)
+    acc = run_gpu(case)
+    ora = run_oracle(oracle_lib, case)
+    for got, want in zip(acc.get_G4(), ora.get_G4()):
+        assert rel_err(got, want) <= FP64_TOL
+
+
+def test_mixed_c3_batched_matches_oracle(oracle_lib):
+    """Uneven orders in one batch, a partial last batch flushed by finalize."""
+    w = W.WORKLOADS["c3"]
+    case = case_from_workload(w, 5)
+    acc = run_gpu(case, precision=1, max_batch=4)
+    ora = run_oracle(oracle_lib, case)
+    errs = [rel_err(g, o) for g, o in zip(acc.get_G4(), ora.get_G4())]
+    print("mixed c3 relative errors per channel:", errs)
+    assert max(errs) <= MIXED_TOL
+
+
+def test_mixed_equals_fp64_gpu_at_full_batch():
+    """Full c3 batch (64 measurements): mixed vs the FP64 GPU path (itself pinned above)."""
+    w = W.WORKLOADS["c3"]
+    case = case_from_workload(w, 64)
+    mixed = run_gpu(case, precision=1, max_batch=64)
+    fp64 = run_gpu(case, precision=0, max_batch=1)
+    errs = [rel_err(a, b) for a, b in zip(mixed.get_G4(), fp64.get_G4())]
+    print("mixed vs FP64, 64 measurements:", errs)
+    assert max(errs) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_sum_to_equals_single_accumulator(precision):
+    case, _ = golden("sq2_all")
+    from dca_b200.accumulators import TpAccumulator
+    a = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=2))
+    b = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=2))
+    for acc in (a, b):
+        acc.resetAccumulation(0)
+    ms = case.measurements
+    for m in ms[:1]:
+        a.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    for m in ms[1:]:
+        b.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    a.sumTo(b)
+    b.finalize()
+    a.finalize()
+    whole = run_gpu(case, precision=precision, max_batch=2)
+    for got, want, zero in zip(b.get_G4(), whole.get_G4(), a.get_G4()):
+        assert rel_err(got, want) <= 1e-13
+        assert np.all(zero == 0)
+
+
+def test_device_resident_m_matches_host_m():
+    import torch
+    case, _ = golden("mb3_all")
+    from dca_b200.accumulators import TpAccumulator
+    host = run_gpu(case)
+    acc = TpAccumulator(case.G0, case.tp_params())
+    acc.resetAccumulation(0)
+    for m in case.measurements:
+        Md = [torch.from_numpy(np.ascontiguousarray(s.M.T)).cuda().t() for s in m.sectors]
+        acc.accumulate(Md, list(m.sectors), m.sign)
+        acc.synchronizeCopy()
+    acc.finalize()
+    for got, want in zip(acc.get_G4(), host.get_G4()):
+        assert rel_err(got, want) <= 1e-14
+
+
+def test_lifecycle_and_errors():
+    from dca_b200.accumulators import LogicError, TpAccumulator
+    case, _ = golden("c1_mag")
+    acc = TpAccumulator(case.G0, case.tp_params())
+    m = case.measurements[0]
+    args = ([s.M for s in m.sectors], list(m.sectors), m.sign)
+    with pytest.raises(LogicError):          # not ready to measure
+        acc.accumulate(*args)
+    acc.resetAccumulation(0)
+    acc.accumulate(*args)
+    with pytest.raises(LogicError):          # bad sign
+        acc.accumulate(args[0], args[1], 3)
+    bad = W.Sector(m.sectors[0].tau, m.sectors[0].left_band, m.sectors[0].right_band + 1,
+                   m.sectors[0].left_site, m.sectors[0].right_site, m.sectors[0].M)
+    with pytest.raises(LogicError):          # band out of range
+        acc.accumulate([bad.M, m.sectors[1].M], [bad, m.sectors[1]], 1)
+    empty = W.Sector(np.zeros(0), *(np.zeros(0, np.int32) for _ in range(4)), np.zeros((0, 0)))
+    assert acc.accumulate([empty.M, empty.M], [empty, empty], 1) == 0.0
+    acc.finalize()
+    one = acc.get_G4()[0].copy()
+    with pytest.raises(LogicError):          # finalized: needs resetAccumulation
+        acc.accumulate(*args)
+    acc.resetAccumulation(1)
+    acc.accumulate(*args)
+    acc.finalize()
+    assert rel_err(acc.get_G4()[0], one) <= 1e-15
+    assert acc.kernel_launches() > 0 and acc.deviceFingerprint() > 0
