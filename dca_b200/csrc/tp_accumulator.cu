@@ -138,6 +138,8 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
     DCAACC_CUDA_CHECK(cudaMemset(g.get(), 0, g.bytes()));
     ptrs.push_back(g.get());
   }
+  err_d_.alloc(1);
+  DCAACC_CUDA_CHECK(cudaMemset(err_d_.get(), 0, sizeof(int)));
   G4_ptrs_.alloc(ptrs.size());
   DCAACC_CUDA_CHECK(cudaMemcpy(G4_ptrs_.get(), ptrs.data(), G4_ptrs_.bytes(), cudaMemcpyHostToDevice));
 
@@ -365,6 +367,7 @@ void TpAccumulator::process() {
   ga.wex_list = wex_d_.get();
   ga.G4 = G4_ptrs_.get();
   ga.atomic = atomic_;
+  ga.err = err_d_.get();
   cudaEvent_t b = nullptr;
   timeBegin(DCAACC_STAGE_ROW, &b);
   if (mixed_)
@@ -425,8 +428,19 @@ void TpAccumulator::finalize() {
                                       cudaMemcpyDeviceToHost, stream_));
   }
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  checkDeviceError();
   finalized_ = true;
   ready_ = false;
+}
+
+void TpAccumulator::checkDeviceError() {
+  int e = 0;
+  DCAACC_CUDA_CHECK(cudaMemcpy(&e, err_d_.get(), sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    DCAACC_CUDA_CHECK(cudaMemset(err_d_.get(), 0, sizeof(int)));
+    throw Error(DCAACC_DEVICE_INDEX_ERR, e & 1 ? "a device-side wait timed out; G4 is incomplete"
+                                               : "a device-side index check failed; G4 is incomplete");
+  }
 }
 
 void TpAccumulator::getG4(int channel, double* out, size_t count) const {
@@ -560,6 +574,7 @@ void TpAccumulator::setStream(cudaStream_t s) {
 
 void TpAccumulator::synchronize() {
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  checkDeviceError();
 }
 
 size_t TpAccumulator::deviceFingerprint() const {
@@ -567,7 +582,7 @@ size_t TpAccumulator::deviceFingerprint() const {
              wex_d_.bytes() + G4_ptrs_.bytes() + sectors_d_.bytes() + tau_d_.bytes() +
              M_d_.bytes() + perm_r_d_.bytes() + perm_c_d_.bytes() + rstart_d_.bytes() +
              cstart_d_.bytes() + signs_d_.bytes() + Tr_d_.bytes() + Tc_d_.bytes() + X64_.bytes() +
-             G64_.bytes() + X32_.bytes() + G32_.bytes();
+             G64_.bytes() + X32_.bytes() + G32_.bytes() + err_d_.bytes();
   for (const auto& g : G4_)
     b += g.bytes();
   return b;

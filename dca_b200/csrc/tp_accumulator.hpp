@@ -142,6 +142,7 @@ private:
   DevBuf<int> k_add_d_, k_sub_d_, q_d_, wex_d_;
   std::vector<DevBuf<double2>> G4_;
   DevBuf<double2*> G4_ptrs_;
+  DevBuf<int> err_d_;  // kernels' error word (async_copy.cuh kErr* bits)
   // Batch workspace.
   DevBuf<SectorDesc> sectors_d_;
   DevBuf<double> tau_d_, M_d_;
@@ -177,6 +178,7 @@ private:
   void timeBegin(int stage, cudaEvent_t* b);
   void timeEnd(int stage, cudaEvent_t b, int launches);
   void collectTimes();
+  void checkDeviceError();
 };
 
 }  // namespace dcaacc

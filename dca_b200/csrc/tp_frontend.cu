@@ -65,14 +65,18 @@ __device__ inline cplx_t<Real> loadC(const double2* p) {
   return mk(static_cast<Real>(v.x), static_cast<Real>(v.y));
 }
 
-// Row transform.  grid (ceil(n_max / JC), ceil(NwExt / WC), n_sectors), 256 threads.
-template <typename Real, int JC, int WC>
-__global__ void __launch_bounds__(256)
+// Row transform.  grid (ceil(n_max / JC), ceil(NwExt / WC), n_sectors), WC * JC threads.
+// Thread (w, jc) walks the row-sorted vertices once; the vertices of one orbital are contiguous,
+// so its running sum is flushed to shared memory at each orbital boundary (the same boundaries
+// for every thread, so no divergence).  M columns and twiddles are staged through shared memory
+// in chunks of IB vertices.
+template <typename Real, int JC, int WC, int IB>
+__global__ void __launch_bounds__(JC * WC)
 rowTransformKernel(const TpDims dims, const SectorDesc* __restrict__ sectors,
                    const int* __restrict__ perm_r, const int* __restrict__ perm_c,
                    const int* __restrict__ row_start, const double2* __restrict__ Tr,
                    const double2* __restrict__ Fb,  // (r, k, b): e^{i k (r + a_b)}
-                   cplx_t<Real>* __restrict__ Xp, int n_max) {
+                   cplx_t<Real>* __restrict__ Xp) {
   using C = cplx_t<Real>;
   const SectorDesc sd = sectors[blockIdx.z];
   const int n = sd.n;
@@ -81,67 +85,90 @@ rowTransformKernel(const TpDims dims, const SectorDesc* __restrict__ sectors,
   if (jj0 >= n)
     return;
   const int nw_ext = dims.nw_ext, n_orb = dims.n_orb, R = dims.R, nb = dims.nb, nc = dims.nc;
+  const int t = threadIdx.x;
+  const int w = t % WC, jc = t / WC;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Xs = reinterpret_cast<C*>(smem_raw);                      // [JC][WC][n_orb]
-  C* Fs = Xs + JC * WC * n_orb;                                // [nb][nc][nc]
-  Real* Ms = reinterpret_cast<Real*>(Fs + nb * nc * nc);       // [JC][n]
+  constexpr int MS = IB + 1;               // padded row of Ms (no bank conflicts across jc)
+  C* Xs = reinterpret_cast<C*>(smem_raw);   // [n_orb][JC][WC]
+  C* Fs = Xs + JC * WC * n_orb;             // [nb][nc][nc]
+  C* Ts = Fs + nb * nc * nc;                // [IB][WC]
+  Real* Ms = reinterpret_cast<Real*>(Ts + IB * WC);  // [JC][MS]
+  int* rs = reinterpret_cast<int*>(Ms + JC * MS);    // [n_orb + 1]
 
   const int* pr = perm_r + sd.vtx_off;
   const int* pc = perm_c + sd.vtx_off;
-  const int* rs = row_start + sd.orb_off;
-
-  for (int idx = threadIdx.x; idx < nb * nc * nc; idx += blockDim.x)
+  for (int idx = t; idx < nb * nc * nc; idx += blockDim.x)
     Fs[idx] = loadC<Real>(Fb + idx);
+  for (int idx = t; idx <= n_orb; idx += blockDim.x)
+    rs[idx] = row_start[sd.orb_off + idx];
   const int jc_count = min(JC, n - jj0);
-  for (int jc = 0; jc < jc_count; ++jc) {
-    const double* col = sd.M + static_cast<long>(sd.ldm) * pc[jj0 + jc];
-    for (int ii = threadIdx.x; ii < n; ii += blockDim.x)
-      Ms[jc * n_max + ii] = static_cast<Real>(col[pr[ii]]);
-  }
-  __syncthreads();
 
   // Row NDFT per orbital: X(o1, w; jc) = sum_{ii in seg(o1)} T(w, ii) M(ii, jc).
-  for (int p = threadIdx.x; p < WC * n_orb; p += blockDim.x) {
-    const int w = p % WC, o1 = p / WC, we = w0 + w;
-    C acc[JC];
-#pragma unroll
-    for (int jc = 0; jc < JC; ++jc)
-      acc[jc] = mk(Real(0), Real(0));
-    if (we < nw_ext) {
-      for (int ii = rs[o1]; ii < rs[o1 + 1]; ++ii) {
-        const C t = loadC<Real>(Tr + static_cast<long>(sd.vtx_off + ii) * nw_ext + we);
-#pragma unroll
-        for (int jc = 0; jc < JC; ++jc) {
-          const Real m = Ms[jc * n_max + ii];
-          acc[jc].x = fma(t.x, m, acc[jc].x);
-          acc[jc].y = fma(t.y, m, acc[jc].y);
-        }
-      }
+  C acc = mk(Real(0), Real(0));
+  int o1 = 0;
+  __syncthreads();
+  int seg_end = rs[1];
+  while (o1 < n_orb && seg_end == 0) {  // leading empty orbitals
+    Xs[o1 * JC * WC + t] = acc;
+    ++o1;
+    seg_end = o1 < n_orb ? rs[o1 + 1] : n;
+  }
+  for (int i0 = 0; i0 < n; i0 += IB) {
+    const int ib_count = min(IB, n - i0);
+    for (int idx = t; idx < ib_count * WC; idx += blockDim.x) {
+      const int ib = idx / WC, ww = idx % WC;
+      Ts[ib * WC + ww] = (w0 + ww < nw_ext) ? loadC<Real>(Tr + static_cast<long>(sd.vtx_off + i0 + ib) * nw_ext + w0 + ww)
+                                           : mk(Real(0), Real(0));
     }
-#pragma unroll
-    for (int jc = 0; jc < JC; ++jc)
-      Xs[(jc * WC + w) * n_orb + o1] = acc[jc];
+    for (int idx = t; idx < JC * ib_count; idx += blockDim.x) {
+      const int c = idx / ib_count, ib = idx % ib_count;
+      Ms[c * MS + ib] = c < jc_count
+                            ? static_cast<Real>(sd.M[static_cast<long>(sd.ldm) * pc[jj0 + c] + pr[i0 + ib]])
+                            : Real(0);
+    }
+    __syncthreads();
+    for (int ib = 0; ib < ib_count; ++ib) {
+      const int ii = i0 + ib;
+      while (ii >= seg_end) {  // orbital boundary: uniform across the CTA
+        Xs[o1 * JC * WC + t] = acc;
+        acc = mk(Real(0), Real(0));
+        ++o1;
+        seg_end = o1 < n_orb ? rs[o1 + 1] : n;
+      }
+      const C tv = Ts[ib * WC + w];
+      const Real m = Ms[jc * MS + ib];
+      acc.x = fma(tv.x, m, acc.x);
+      acc.y = fma(tv.y, m, acc.y);
+    }
+    __syncthreads();
+  }
+  for (; o1 < n_orb; ++o1) {
+    Xs[o1 * JC * WC + t] = acc;
+    acc = mk(Real(0), Real(0));
   }
   __syncthreads();
 
   // Row cluster transform with band phases: X'(b1 + nb k1) = sum_r1 Fb(b1, k1, r1) X(b1 + nb r1).
-  for (int q = threadIdx.x; q < jc_count * WC * R; q += blockDim.x) {
-    const int row = q % R, w = (q / R) % WC, jc = q / (R * WC), we = w0 + w;
+  for (int q = t; q < jc_count * WC * R; q += blockDim.x) {
+    const int row = q % R, ww = (q / R) % WC, c = q / (R * WC), we = w0 + ww;
     if (we >= nw_ext)
       continue;
     const int b1 = row % nb, k1 = row / nb;
-    const C* x = Xs + (jc * WC + w) * n_orb + b1;
+    const C* x = Xs + b1 * JC * WC + c * WC + ww;
     const C* f = Fs + (b1 * nc + k1) * nc;
-    C acc = mk(Real(0), Real(0));
+    C a = mk(Real(0), Real(0));
     for (int r1 = 0; r1 < nc; ++r1)
-      cfma(acc, f[r1], x[nb * r1]);
-    Xp[sd.x_off + (static_cast<long>(we) * n + jj0 + jc) * R + row] = acc;
+      cfma(a, f[r1], x[nb * r1 * JC * WC]);
+    Xp[sd.x_off + (static_cast<long>(we) * n + jj0 + c) * R + row] = a;
   }
 }
 
 // Column transform + G epilogue.  grid (NwExt, ceil(NwExt / WC2), n_sectors), R * WC2 threads.
-template <typename Real>
+// X' rows of frequency w1 and the twiddles of the CTA's w2 chunk are staged through shared
+// memory in chunks of JB vertices; thread (row, w2) walks the column-sorted vertices once and
+// flushes its running sum at each column-orbital boundary.
+template <typename Real, int JB>
 __global__ void colTransformKernel(const TpDims dims, const SectorDesc* __restrict__ sectors,
                                    const int* __restrict__ col_start,
                                    const double2* __restrict__ Tc, const double2* __restrict__ Fb,
@@ -153,32 +180,66 @@ __global__ void colTransformKernel(const TpDims dims, const SectorDesc* __restri
   const int n = sd.n;
   const int w1 = blockIdx.x;
   const int nw_ext = dims.nw_ext, n_orb = dims.n_orb, R = dims.R, nb = dims.nb, nc = dims.nc;
-  const int row = threadIdx.x % R, w2l = threadIdx.x / R;
-  const int w2 = blockIdx.y * WC2 + w2l;
+  const int t = threadIdx.x;
+  const int row = t % R, w2l = t / R;
+  const int w2c0 = blockIdx.y * WC2;
+  const int w2 = w2c0 + w2l;
   const bool active = w2 < nw_ext;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Zs = reinterpret_cast<C*>(smem_raw);  // [R][WC2][n_orb]
-  C* Gs = Zs + R * WC2 * n_orb;            // [R][WC2][R]
+  C* Zs = reinterpret_cast<C*>(smem_raw);  // [n_orb][WC2][R]; reused as the output tile
+  C* Gs = Zs + WC2 * R * (R + 1);          // [R cols][WC2][R rows]; Zs space holds the padded tile
   C* Fs = Gs + R * WC2 * R;                // [nb][nc][nc]
-  for (int idx = threadIdx.x; idx < nb * nc * nc; idx += blockDim.x)
+  C* Xst = Fs + nb * nc * nc;              // [JB][R]
+  C* Tst = Xst + JB * R;                   // [JB][WC2]
+  int* cs = reinterpret_cast<int*>(Tst + JB * WC2);  // [n_orb + 1]
+  for (int idx = t; idx < nb * nc * nc; idx += blockDim.x)
     Fs[idx] = loadC<Real>(Fb + idx);
+  for (int idx = t; idx <= n_orb; idx += blockDim.x)
+    cs[idx] = col_start[sd.orb_off + idx];
+  __syncthreads();
 
-  const int* cs = col_start + sd.orb_off;
-  C* z = Zs + (row * WC2 + w2l) * n_orb;
-  if (active) {
-    // Column NDFT per orbital: Z(o2) = sum_{jj in seg(o2)} X'(row, w1; jj) conj(T(w2, jj)).
-    const C* xrow = Xp + sd.x_off + static_cast<long>(w1) * n * R + row;
-    const double2* tcol = Tc + static_cast<long>(sd.vtx_off) * nw_ext + w2;
-    for (int o2 = 0; o2 < n_orb; ++o2) {
-      C acc = mk(Real(0), Real(0));
-      for (int jj = cs[o2]; jj < cs[o2 + 1]; ++jj)
-        cfmac(acc, xrow[static_cast<long>(jj) * R], loadC<Real>(tcol + static_cast<long>(jj) * nw_ext));
-      z[o2] = acc;
+  // Column NDFT per orbital: Z(o2) = sum_{jj in seg(o2)} X'(row, w1; jj) conj(T(w2, jj)).
+  const int zs = WC2 * R;  // stride between orbitals of one thread's Z
+  C* z = Zs + t;
+  C acc = mk(Real(0), Real(0));
+  int o2 = 0;
+  int seg_end = cs[1];
+  while (o2 < n_orb && seg_end == 0) {
+    z[o2 * zs] = acc;
+    ++o2;
+    seg_end = o2 < n_orb ? cs[o2 + 1] : n;
+  }
+  const C* xrow = Xp + sd.x_off + static_cast<long>(w1) * n * R;
+  for (int j0 = 0; j0 < n; j0 += JB) {
+    const int jb_count = min(JB, n - j0);
+    for (int idx = t; idx < jb_count * R; idx += blockDim.x)
+      Xst[idx] = xrow[static_cast<long>(j0) * R + idx];
+    for (int idx = t; idx < jb_count * WC2; idx += blockDim.x) {
+      const int jb = idx / WC2, ww = idx % WC2;
+      Tst[idx] = (w2c0 + ww < nw_ext)
+                     ? loadC<Real>(Tc + static_cast<long>(sd.vtx_off + j0 + jb) * nw_ext + w2c0 + ww)
+                     : mk(Real(0), Real(0));
     }
+    __syncthreads();
+    for (int jb = 0; jb < jb_count; ++jb) {
+      const int jj = j0 + jb;
+      while (jj >= seg_end) {
+        z[o2 * zs] = acc;
+        acc = mk(Real(0), Real(0));
+        ++o2;
+        seg_end = o2 < n_orb ? cs[o2 + 1] : n;
+      }
+      cfmac(acc, Xst[jb * R + row], Tst[jb * WC2 + w2l]);
+    }
+    __syncthreads();
+  }
+  for (; o2 < n_orb; ++o2) {
+    z[o2 * zs] = acc;
+    acc = mk(Real(0), Real(0));
   }
   __syncthreads();
-  C* g = Gs + (row * WC2 + w2l) * R;
+  C* g = Gs + t;  // column col of this thread's row at g[col * zs]
   if (active) {
     // Column cluster transform with band phases and the 1/Nc normalisation
     // (space_transform_2D.hpp:79-89).
@@ -186,50 +247,58 @@ __global__ void colTransformKernel(const TpDims dims, const SectorDesc* __restri
     for (int col = 0; col < R; ++col) {
       const int b2 = col % nb, k2 = col / nb;
       const C* f = Fs + (b2 * nc + k2) * nc;
-      C acc = mk(Real(0), Real(0));
+      C a = mk(Real(0), Real(0));
       for (int r2 = 0; r2 < nc; ++r2)
-        cfmac(acc, z[b2 + nb * r2], f[r2]);
-      g[col] = cscale(acc, norm);
+        cfmac(a, z[(b2 + nb * r2) * zs], f[r2]);
+      g[col * zs] = cscale(a, norm);
     }
   }
   __syncthreads();
-  if (!active)
-    return;
-
-  // Epilogue: G = -G0(k1, w1) G~ G0(k2, w2) + beta G0(k1, w1) delta (tp_accumulator_cpu.hpp:309-375).
-  const int s = sd.spin;
-  const int b1 = row % nb, k1 = row / nb;
-  const double2* g0s = G0 + static_cast<long>(s) * nw_ext * nc * nb * nb;
-  auto g0 = [&](int ba, int bb, int k, int w) {
-    return loadC<Real>(g0s + ba + nb * (bb + nb * (k + nc * w)));
-  };
-  C* out = G + g_sector_stride * (2 * sd.slot + s) +
-             (static_cast<long>(w1) * nw_ext + w2) * R * R + static_cast<long>(row) * R;
-  const Real beta = static_cast<Real>(dims.beta);
-  for (int col = 0; col < R; ++col) {
-    const int b2 = col % nb, k2 = col / nb;
-    C v;
-    if (nb == 1) {
-      v = cmul(cmul(g0(0, 0, k1, w1), g[col]), g0(0, 0, k2, w2));
-      v = mk(-v.x, -v.y);
-    }
-    else {
-      v = mk(Real(0), Real(0));
-      const C* gs_k1 = Gs + (static_cast<long>(k1 * nb) * WC2 + w2l) * R;  // row (c1 = 0, k1)
-      for (int c2 = 0; c2 < nb; ++c2) {
-        C t = mk(Real(0), Real(0));  // (G0_w1 G~)(b1, c2) at (k1, k2)
-        for (int c1 = 0; c1 < nb; ++c1)
-          cfma(t, g0(b1, c1, k1, w1), gs_k1[c1 * WC2 * R + c2 + nb * k2]);
-        cfma(v, t, g0(c2, b2, k2, w2));
+  // Epilogue: G = -G0(k1, w1) G~ G0(k2, w2) + beta G0(k1, w1) delta (tp_accumulator_cpu.hpp:309-375),
+  // staged as row-major blocks (row stride R + 1 against bank conflicts) in the Zs space.
+  C* Os = Zs;  // [WC2][R][R + 1]
+  if (active) {
+    const int s = sd.spin;
+    const int b1 = row % nb, k1 = row / nb;
+    const double2* g0s = G0 + static_cast<long>(s) * nw_ext * nc * nb * nb;
+    auto g0 = [&](int ba, int bb, int k, int w) {
+      return loadC<Real>(g0s + ba + nb * (bb + nb * (k + nc * w)));
+    };
+    const Real beta = static_cast<Real>(dims.beta);
+    C* o = Os + (w2l * R + row) * (R + 1);
+    for (int col = 0; col < R; ++col) {
+      const int b2 = col % nb, k2 = col / nb;
+      C v;
+      if (nb == 1) {
+        v = cmul(cmul(g0(0, 0, k1, w1), g[col * zs]), g0(0, 0, k2, w2));
+        v = mk(-v.x, -v.y);
       }
-      v = mk(-v.x, -v.y);
+      else {
+        v = mk(Real(0), Real(0));
+        for (int c2 = 0; c2 < nb; ++c2) {
+          C tt = mk(Real(0), Real(0));  // (G0_w1 G~)(b1, c2) at (k1, k2)
+          for (int c1 = 0; c1 < nb; ++c1)
+            cfma(tt, g0(b1, c1, k1, w1), Gs[((c2 + nb * k2) * WC2 + w2l) * R + c1 + nb * k1]);
+          cfma(v, tt, g0(c2, b2, k2, w2));
+        }
+        v = mk(-v.x, -v.y);
+      }
+      if (k1 == k2 && w1 == w2) {
+        const C d = g0(b1, b2, k1, w1);
+        v.x += d.x * beta;
+        v.y += d.y * beta;
+      }
+      o[col] = v;
     }
-    if (k1 == k2 && w1 == w2) {
-      const C d = g0(b1, b2, k1, w1);
-      v.x += d.x * beta;
-      v.y += d.y * beta;
-    }
-    out[col] = v;
+  }
+  __syncthreads();
+  // Coalesced store of the CTA's blocks (w1, w2c0 .. w2c0 + WC2 - 1), each R x R contiguous.
+  const int n_w2 = min(WC2, nw_ext - w2c0);
+  C* out = G + g_sector_stride * (2 * sd.slot + sd.spin) +
+           (static_cast<long>(w1) * nw_ext + w2c0) * R * R;
+  for (int idx = t; idx < n_w2 * R * R; idx += blockDim.x) {
+    const int wl = idx / (R * R), rem = idx % (R * R);
+    out[idx] = Os[(wl * R + rem / R) * (R + 1) + rem % R];
   }
 }
 
@@ -248,37 +317,42 @@ void launchTwiddles(const FrontendArgs& a, cudaStream_t stream) {
   }
 }
 
+constexpr int kRowJC = 32, kRowWC = 8, kRowIB = 64, kColJB = 64;
+
 template <typename Real>
-static size_t rowSmem(const TpDims& d, int n_max, int JC, int WC) {
-  return sizeof(cplx_t<Real>) * (JC * WC * d.n_orb + d.nb * d.nc * d.nc) + sizeof(Real) * JC * n_max;
+static size_t rowSmem(const TpDims& d) {
+  return sizeof(cplx_t<Real>) * (kRowJC * kRowWC * d.n_orb + d.nb * d.nc * d.nc + kRowIB * kRowWC) +
+         sizeof(Real) * kRowJC * (kRowIB + 1) + sizeof(int) * (d.n_orb + 1);
 }
 
 template <typename Real>
 static int pickWC2(const TpDims& d) {
   // Largest power of two <= 16 with R * WC2 <= 1024 threads and Zs + Gs <= 96 KB.
   int wc2 = 16;
-  while (wc2 > 1 && (d.R * wc2 > 1024 || 2 * sizeof(cplx_t<Real>) * d.R * d.R * wc2 > 96 * 1024))
+  while (wc2 > 1 && (d.R * wc2 > 1024 || sizeof(cplx_t<Real>) * (d.R * d.R * wc2 + d.R * (d.R + 1) * wc2) > 96 * 1024))
     wc2 /= 2;
   return wc2;
 }
 
 template <typename Real>
 static size_t colSmem(const TpDims& d, int wc2) {
-  return sizeof(cplx_t<Real>) * (2 * d.R * wc2 * d.R + d.nb * d.nc * d.nc);
+  // Zs (also the padded output tile) + Gs + Fs + staging + column starts.
+  const size_t zs = std::max(size_t(d.R) * wc2 * d.n_orb, size_t(wc2) * d.R * (d.R + 1));
+  return sizeof(cplx_t<Real>) * (zs + size_t(d.R) * wc2 * d.R + d.nb * d.nc * d.nc + kColJB * (d.R + wc2)) +
+         sizeof(int) * (d.n_orb + 1);
 }
 
 template <typename Real>
 void launchRowTransform(const FrontendArgs& a, cplx_t<Real>* Xp, cudaStream_t stream) {
-  constexpr int JC = 8, WC = 8;
   const TpDims& d = a.dims;
   if (a.n_max == 0)
     return;
-  const size_t smem = rowSmem<Real>(d, a.n_max, JC, WC);
-  auto k = rowTransformKernel<Real, JC, WC>;
+  const size_t smem = rowSmem<Real>(d);
+  auto k = rowTransformKernel<Real, kRowJC, kRowWC, kRowIB>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const dim3 grid(ceil_div(a.n_max, JC), ceil_div(d.nw_ext, WC), a.n_sectors);
-  k<<<grid, 256, smem, stream>>>(d, a.sectors, a.perm_r, a.perm_c, a.row_start, a.Tr, a.Fb, Xp,
-                                 a.n_max);
+  const dim3 grid(ceil_div(a.n_max, kRowJC), ceil_div(d.nw_ext, kRowWC), a.n_sectors);
+  k<<<grid, kRowJC * kRowWC, smem, stream>>>(d, a.sectors, a.perm_r, a.perm_c, a.row_start, a.Tr, a.Fb,
+                                             Xp);
   DCAACC_LAUNCH_CHECK();
 }
 
@@ -288,7 +362,7 @@ void launchColTransform(const FrontendArgs& a, const cplx_t<Real>* Xp, cplx_t<Re
   const TpDims& d = a.dims;
   const int wc2 = pickWC2<Real>(d);
   const size_t smem = colSmem<Real>(d, wc2);
-  auto k = colTransformKernel<Real>;
+  auto k = colTransformKernel<Real, kColJB>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const dim3 grid(d.nw_ext, ceil_div(d.nw_ext, wc2), a.n_sectors);
   k<<<grid, d.R * wc2, smem, stream>>>(d, a.sectors, a.col_start, a.Tc, a.Fb, a.G0, Xp, G,
@@ -296,10 +370,10 @@ void launchColTransform(const FrontendArgs& a, const cplx_t<Real>* Xp, cplx_t<Re
   DCAACC_LAUNCH_CHECK();
 }
 
-size_t frontendSmemRequirement(const TpDims& d, int n_max, bool fp64) {
+size_t frontendSmemRequirement(const TpDims& d, int /*n_max*/, bool fp64) {
   if (fp64)
-    return std::max(rowSmem<double>(d, n_max, 8, 8), colSmem<double>(d, pickWC2<double>(d)));
-  return std::max(rowSmem<float>(d, n_max, 8, 8), colSmem<float>(d, pickWC2<float>(d)));
+    return std::max(rowSmem<double>(d), colSmem<double>(d, pickWC2<double>(d)));
+  return std::max(rowSmem<float>(d), colSmem<float>(d, pickWC2<float>(d)));
 }
 
 template void launchRowTransform<double>(const FrontendArgs&, double2*, cudaStream_t);

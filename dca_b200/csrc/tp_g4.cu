@@ -29,6 +29,7 @@
 
 #include <algorithm>
 
+#include "async_copy.cuh"
 #include "common.cuh"
 #include "tp_g4.hpp"
 
@@ -177,10 +178,242 @@ updateG4Kernel(const TpDims dims, const GT* __restrict__ G, long g_sector_stride
   }
 }
 
+
+// Single-band PH-magnetic / PH-charge update with the G blocks staged in shared memory.
+//
+// CTA = one (w1, w2, wq) tile and a chunk of momentum transfers q; thread = (k1, q, k2-chunk),
+// holding the partial sums of its KT entries (k1, k2, q) for both channels in registers across
+// the whole batch.  Per measurement the CTA needs four R x R blocks per spin,
+//   A = G(., w1; ., w2)   B = G(., w2+x; ., w1+x)   C = G(., w1; ., w1+x)   E = G(., w2+x; ., w2),
+// fetched by the bulk-copy engine (cp.async.bulk, one copy per block) into a two-stage ring while
+// the previous measurement is being consumed.  With u_s(k1) = C_s(k1, k1+q), v_s(k2) = E_s(k2+q, k2):
+//   magnetic += s/2 [(u_0 - u_1)(v_0 - v_1) - D],  charge += s/2 [(u_0 + u_1)(v_0 + v_1) - D],
+//   D = sum_s A_s(k1, k2) B_s(k2+q, k1+q)
+// (for one band the two channels share D).
+// QFAST: consecutive threads take consecutive q (the A-block reads of a warp are broadcasts and
+// the B-block reads fall in distinct banks) -- used for long batches.  Otherwise consecutive
+// threads take consecutive k1 (coalesced G4 read-modify-write) and the running sums are read
+// before the G blocks arrive (PREFETCH) -- used for the bandwidth-bound single-measurement case.
+template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH>
+__global__ void __launch_bounds__(512)
+updateG4SinglebandPH(const TpDims dims, const GT* __restrict__ G, long g_sector_stride,
+                     const int* __restrict__ signs, int n_slots, const int* __restrict__ k_add,
+                     const int* __restrict__ q_list, const int* __restrict__ wex_list,
+                     double2* const* __restrict__ G4, bool atomic, int q_chunk, int n_kc,
+                     int* __restrict__ err) {
+  using C = cplx_t<AT>;
+  const int nc = dims.nc, nw = dims.nw, nw_ext = dims.nw_ext, R = dims.R, nq = dims.nq;
+  const int w1 = blockIdx.x, w2 = blockIdx.y;
+  const int n_qchunks = (nq + q_chunk - 1) / q_chunk;
+  const int iwq = blockIdx.z / n_qchunks, q0 = (blockIdx.z % n_qchunks) * q_chunk;
+  const int wex = wex_list[iwq];
+  const int ext = dims.ext;
+  const int t = threadIdx.x;
+  const int k1 = QFAST ? (t / q_chunk) % nc : t % nc;
+  const int ql = QFAST ? t % q_chunk : (t / nc) % q_chunk;
+  const int kc = t / (nc * q_chunk);
+  const int iq = q0 + ql;
+  const bool active = iq < nq && kc < n_kc;
+  const int q = active ? q_list[iq] : 0;
+
+  bool has_mag = false, has_charge = false;
+  for (int c = 0; c < dims.n_channels; ++c) {
+    has_mag |= dims.channels[c] == 2;
+    has_charge |= dims.channels[c] == 3;
+  }
+
+  const long blk_elems = static_cast<long>(R) * R;
+  const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
+  const long boff[4] = {(static_cast<long>(w1e) * nw_ext + w2e) * blk_elems,
+                        (static_cast<long>(w2x) * nw_ext + w1x) * blk_elems,
+                        (static_cast<long>(w1e) * nw_ext + w1x) * blk_elems,
+                        (static_cast<long>(w2x) * nw_ext + w2e) * blk_elems};
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);                   // [2]
+  GT* stage = reinterpret_cast<GT*>(smem_raw + 16);                        // [2][2 spins][4][R*R]
+  C* Um = reinterpret_cast<C*>(stage + 2 * 8 * blk_elems);                 // [nc][q_chunk]
+  C* Uc = Um + q_chunk * nc;
+  C* Vm = Uc + q_chunk * nc;
+  C* Vc = Vm + q_chunk * nc;
+  int* kadd = reinterpret_cast<int*>(Vc + q_chunk * nc);                  // [nc][nc]
+
+  for (int i = t; i < nc * nc; i += blockDim.x)
+    kadd[i] = k_add[i];
+  const uint32_t blk_bytes = static_cast<uint32_t>(blk_elems * sizeof(GT));
+  auto issue = [&](int slot, int st) {
+    GT* dst = stage + static_cast<long>(st) * 8 * blk_elems;
+    mbarArriveExpectTx(&bar[st], 8 * blk_bytes);
+    for (int s = 0; s < 2; ++s) {
+      const GT* src = G + g_sector_stride * (2 * slot + s);
+      for (int b = 0; b < 4; ++b)
+        bulkCopyG2S(dst + (s * 4 + b) * blk_elems, src + boff[b], blk_bytes, &bar[st]);
+    }
+  };
+  if (t == 0) {
+    mbarInit(&bar[0], 1);
+    mbarInit(&bar[1], 1);
+    fenceBarrierInit();
+  }
+  __syncthreads();
+  if (t == 0) {
+    issue(0, 0);
+    if (n_slots > 1)
+      issue(1, 1);
+  }
+
+  C acc_m[KT], acc_c[KT];
+#pragma unroll
+  for (int j = 0; j < KT; ++j) {
+    acc_m[j] = mk(AT(0), AT(0));
+    acc_c[j] = mk(AT(0), AT(0));
+  }
+  const long s_w1 = nc, s_k2 = s_w1 * nw, s_w2 = s_k2 * nc, s_q = s_w2 * nw, s_wq = s_q * nq;
+  const long g4_base = k1 + w1 * s_w1 + w2 * s_w2 + iq * s_q + iwq * s_wq;
+  double2 old[PREFETCH ? 2 * KT : 1];
+  if constexpr (PREFETCH) {
+    // Running sums of (at most) two channels, loaded while the G blocks are in flight.
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int j = 0; j < KT; ++j) {
+        const int k2 = kc * KT + j;
+        old[c * KT + j] = (active && c < dims.n_channels && k2 < nc) ? G4[c][g4_base + k2 * s_k2]
+                                                                     : make_double2(0, 0);
+      }
+  }
+
+  for (int m = 0; m < n_slots; ++m) {
+    const int st = m & 1;
+    const bool ok = mbarWait(&bar[st], (m >> 1) & 1, err);
+    if (!__syncthreads_and(ok))
+      return;  // uniform bail-out; the host reports the error word
+    const GT* S = stage + static_cast<long>(st) * 8 * blk_elems;
+    const GT *A0 = S, *B0 = S + blk_elems, *C0 = S + 2 * blk_elems, *E0 = S + 3 * blk_elems;
+    const GT *A1 = S + 4 * blk_elems, *B1 = S + 5 * blk_elems, *C1 = S + 6 * blk_elems,
+             *E1 = S + 7 * blk_elems;
+    const AT hs = AT(0.5) * static_cast<AT>(signs[m]);
+    auto ld = [](const GT* p) { return mk(static_cast<AT>(p->x), static_cast<AT>(p->y)); };
+    if (active && kc == 0) {
+      const int k1q = kadd[k1 + nc * q];
+      const C c0 = ld(C0 + k1 * R + k1q), c1 = ld(C1 + k1 * R + k1q);
+      const C e0 = ld(E0 + k1q * R + k1), e1 = ld(E1 + k1q * R + k1);  // v(k2 = k1)
+      Um[k1 * q_chunk + ql] = mk(hs * (c0.x - c1.x), hs * (c0.y - c1.y));
+      Uc[k1 * q_chunk + ql] = mk(hs * (c0.x + c1.x), hs * (c0.y + c1.y));
+      Vm[k1 * q_chunk + ql] = mk(e0.x - e1.x, e0.y - e1.y);
+      Vc[k1 * q_chunk + ql] = mk(e0.x + e1.x, e0.y + e1.y);
+    }
+    __syncthreads();
+    if (active) {
+      const int k1q = kadd[k1 + nc * q];
+      const C um = Um[k1 * q_chunk + ql], uc = Uc[k1 * q_chunk + ql];
+#pragma unroll
+      for (int j = 0; j < KT; ++j) {
+        const int k2 = kc * KT + j;
+        if (k2 < nc) {
+          const int k2q = kadd[k2 + nc * q];
+          C d = cmul(ld(A0 + k1 * R + k2), ld(B0 + k2q * R + k1q));
+          cfma(d, ld(A1 + k1 * R + k2), ld(B1 + k2q * R + k1q));
+          d = cscale(d, hs);
+          if (has_mag) {
+            C v = cmul(um, Vm[k2 * q_chunk + ql]);
+            acc_m[j] = cadd(acc_m[j], csub(v, d));
+          }
+          if (has_charge) {
+            C v = cmul(uc, Vc[k2 * q_chunk + ql]);
+            acc_c[j] = cadd(acc_c[j], csub(v, d));
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage st and U/V free again
+    if (t == 0 && m + 2 < n_slots) {
+      fenceProxyAsync();
+      issue(m + 2, st);
+    }
+  }
+
+  if (!active)
+    return;
+  // One read-modify-write of the FP64 running sums.
+#pragma unroll
+  for (int c = 0; c < kMaxChannels; ++c) {
+    if (c >= dims.n_channels)
+      break;
+    const bool mag = dims.channels[c] == 2;
+    double2* g4 = G4[c] + g4_base;
+#pragma unroll
+    for (int j = 0; j < KT; ++j) {
+      const int k2 = kc * KT + j;
+      if (k2 >= nc)
+        break;
+      const C v = mag ? acc_m[j] : acc_c[j];
+      double2* p = g4 + k2 * s_k2;
+      if (atomic) {
+        atomicAdd(&p->x, static_cast<double>(v.x));
+        atomicAdd(&p->y, static_cast<double>(v.y));
+      }
+      else {
+        double2 o;
+        if constexpr (PREFETCH)
+          o = (c < 2) ? old[c * KT + j] : *p;
+        else
+          o = *p;
+        o.x += static_cast<double>(v.x);
+        o.y += static_cast<double>(v.y);
+        *p = o;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 template <typename GT>
+static bool singlebandPHApplies(const TpDims& d) {
+  if (d.nb != 1)
+    return false;
+  for (int c = 0; c < d.n_channels; ++c)
+    if (d.channels[c] != 2 && d.channels[c] != 3)
+      return false;
+  return (size_t(d.R) * d.R * sizeof(GT)) % 16 == 0;
+}
+
+template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH>
+static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_stride, int target_threads,
+                               cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  const int n_kc = (d.nc + KT - 1) / KT;
+  const int per_q = d.nc * n_kc;
+  if (per_q > 1024)
+    return false;
+  const int q_chunk = std::max(1, std::min(d.nq, target_threads / per_q));
+  const int threads = per_q * q_chunk;
+  const size_t smem = 16 + sizeof(GT) * 2 * 8 * size_t(d.R) * d.R +
+                      sizeof(cplx_t<AT>) * 4 * q_chunk * d.nc + sizeof(int) * d.nc * d.nc;
+  if (smem > 220 * 1024)
+    return false;
+  auto k = updateG4SinglebandPH<GT, AT, KT, QFAST, PREFETCH>;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int n_qchunks = (d.nq + q_chunk - 1) / q_chunk;
+  const dim3 grid(d.nw, d.nw, d.nwq * n_qchunks);
+  k<<<grid, threads, smem, stream>>>(d, G, g_sector_stride, a.signs, a.n_slots, a.k_add, a.q_list,
+                                     a.wex_list, a.G4, a.atomic, q_chunk, n_kc, a.err);
+  DCAACC_LAUNCH_CHECK();
+  return true;
+}
+
+template <typename GT>
 void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
+  if (singlebandPHApplies<GT>(a.dims)) {
+    bool done;
+    if constexpr (std::is_same_v<GT, double2>)
+      done = launchSinglebandPH<double2, double, 4, false, true>(a, G, g_sector_stride, 512, stream);
+    else
+      done = launchSinglebandPH<float2, float, 16, true, false>(a, G, g_sector_stride, 256, stream);
+    if (done)
+      return;
+  }
   const dim3 grid(a.dims.nw, a.dims.nw, a.dims.nwq);
   if constexpr (std::is_same_v<GT, double2>) {
     updateG4Kernel<double2, double, 4><<<grid, 256, 0, stream>>>(

@@ -20,6 +20,7 @@ struct G4Args {
   const int* wex_list;  // [nwq] frequency transfers (device)
   double2* const* G4;   // [n_channels] device pointers to each channel's running sum (device array)
   bool atomic;          // several accumulators share G4
+  int* err;             // device error word (async_copy.cuh kErr* bits)
 };
 
 // dst += src; src = 0 (sumTo of two accumulators on the same device).

@@ -104,8 +104,10 @@ def test_sum_to_equals_single_accumulator(precision):
     b.finalize()
     a.finalize()
     whole = run_gpu(case, precision=precision, max_batch=2)
+    # FP32 batch partial sums depend on how measurements are grouped into batches.
+    tol = 1e-13 if precision == 0 else MIXED_TOL
     for got, want, zero in zip(b.get_G4(), whole.get_G4(), a.get_G4()):
-        assert rel_err(got, want) <= 1e-13
+        assert rel_err(got, want) <= tol
         assert np.all(zero == 0)
 
 
