@@ -284,6 +284,7 @@ def run_ours(args, world, rank, local):
 
     # Plain FP64, unbatched (the path the mixed one is compared with) and the error between them.
     fp64 = None
+    fp64_stages = None
     err = None
     if not args.no_fp64:
         n_cmp = B
@@ -293,6 +294,7 @@ def run_ours(args, world, rank, local):
             ref_acc.accumulate(dev_M[j], configs[j], signs[j])
         torch.cuda.synchronize()
         ref_acc.resetAccumulation(0)
+        ref_acc.enable_timing(True)
         rs = torch.cuda.ExternalStream(ref_acc.get_stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(rs)
@@ -302,6 +304,7 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         fp64_ms = max_over_ranks(e0.elapsed_time(e1), world)
         fp64 = world * n_cmp / (fp64_ms / 1e3)
+        fp64_stages = {k: v[0] / n_cmp for k, v in ref_acc.stage_times().items()}
         ref_acc.finalize()
         mixed_acc = TpAccumulator(g0, params)
         mixed_acc.resetAccumulation(0)
@@ -357,6 +360,7 @@ def run_ours(args, world, rank, local):
         "roofline": roof,
         "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
         "fp64_unbatched_meas_per_s": fp64,
+        "fp64_stages_ms_per_meas": fp64_stages,
         "speedup_vs_fp64": (value / fp64) if fp64 else None,
         "rel_err_vs_fp64": err,
         "clocks": clk,

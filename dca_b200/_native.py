@@ -114,6 +114,7 @@ def _load():
         "dcaacc_tp_enable_timing": (i, [p, i]),
         "dcaacc_tp_stage_times": (i, [p, POINTER(c_double), POINTER(c_uint64), i]),
         "dcaacc_tp_peek_g4": (i, [p, i, sz, sz, POINTER(c_double)]),
+        "dcaacc_tp_compute_g_noalloc": (i, [POINTER(TpConfig), p, POINTER(Sector), p, p]),
         "dcaacc_sp_create": (i, [POINTER(SpConfig), POINTER(p)]),
         "dcaacc_sp_destroy": (None, [p]),
         "dcaacc_sp_reset": (i, [p]),

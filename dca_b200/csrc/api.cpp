@@ -9,6 +9,11 @@
 #include "sp_accumulator.hpp"
 #include "tp_accumulator.hpp"
 
+namespace dcaacc {
+void computeGNoAlloc(const dcaacc_tp_config& c, const double* G0_dev, const dcaacc_sector* sec,
+                     double* G_out, cudaStream_t stream);
+}
+
 struct dcaacc_tp {
   dcaacc::TpAccumulator impl;
   dcaacc_tp(const dcaacc_tp_config& c, const double* g0) : impl(c, g0) {}
@@ -169,6 +174,13 @@ int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t cou
   if (!acc || !out)
     return null_handle();
   return guard([&] { acc->impl.peekG4(channel, offset, count, out); });
+}
+
+int dcaacc_tp_compute_g_noalloc(const dcaacc_tp_config* cfg, const double* G0,
+                                const dcaacc_sector* sectors, double* G_out, void* stream) {
+  if (!cfg)
+    return null_handle();
+  return guard([&] { dcaacc::computeGNoAlloc(*cfg, G0, sectors, G_out, static_cast<cudaStream_t>(stream)); });
 }
 
 int dcaacc_sp_create(const dcaacc_sp_config* cfg, dcaacc_sp** out) {

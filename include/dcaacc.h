@@ -180,6 +180,33 @@ int dcaacc_tp_stage_times(dcaacc_tp* acc, double* ms, uint64_t* launches, int32_
  * an accumulation in progress. */
 int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out);
 
+/* Allocation-free G of one measurement.  No counterpart in the reference: it exists for callers
+ * that cannot allocate device memory while they run -- applications whose device memory is fully
+ * reserved by their own pool allocator, and per-measurement loops that must not pay the
+ * device-wide synchronisation of cudaMalloc / cudaFree.  It runs the same three front-end kernels
+ * as a handle in FP64 mode (twiddles, row NDFT + cluster transform, column NDFT + cluster
+ * transform + G0 epilogue) but takes its scratch from a 48 MiB array compiled into the library,
+ * which every GPU that loads the library keeps until the process exits; it calls no cudaMalloc,
+ * cudaFree or other allocating routine.
+ *
+ *   cfg       sizes, transfers (only their extent matters here), beta, vectors as for
+ *             dcaacc_tp_create; precision, max_batch, max_order and channels are ignored
+ *   G0        DEVICE pointer, complex FP64 G0(b1, s1, b2, s2, k, w) over the full single-particle mesh
+ *   sectors   [2]; vertex arrays in host memory, M in device memory (m_on_device must be 1)
+ *   G_out     DEVICE pointer to 2 * D * D complex FP64 (D = nb Nc NwExt): spin s at offset s D^2,
+ *             frequency-block layout -- block (w_r, w_c) of R x R entries (R = nb Nc, row-major,
+ *             index b + nb k) at ((w_r NwExt + w_c) R^2); entry (r, c) of block (w_r, w_c) is the
+ *             reference's G_(b_r, b_c, s, k_r, k_c, w_r, w_c)
+ *   stream    cudaStream_t (as void*), may be null
+ * Limits: n <= 512 per spin sector, nb Nc <= 64, and all scratch (about 16 R NwExt (n_0 + n_1)
+ * bytes plus small tables) within 48 MiB; larger problems return DCAACC_INVALID_ARG.
+ * The scratch's device address is looked up on the first call made on each device (with that
+ * device current); make that first call before any stream capture.  All calls share the one
+ * scratch array: calls whose GPU work overlaps (different streams, or host threads without
+ * ordering) race on it.  Work is enqueued on the stream; synchronise it before reading G_out. */
+int dcaacc_tp_compute_g_noalloc(const dcaacc_tp_config* cfg, const double* G0,
+                                const dcaacc_sector* sectors, double* G_out, void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Single-particle accumulator (delayed NFFT): SpAccumulator / Dnfft1DGpu.
  * ------------------------------------------------------------------------------------------- */
