@@ -194,8 +194,8 @@ updateG4Kernel(const TpDims dims, const GT* __restrict__ G, long g_sector_stride
 // the B-block reads fall in distinct banks) -- used for long batches.  Otherwise consecutive
 // threads take consecutive k1 (coalesced G4 read-modify-write) and the running sums are read
 // before the G blocks arrive (PREFETCH) -- used for the bandwidth-bound single-measurement case.
-template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH>
-__global__ void __launch_bounds__(512)
+template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
 updateG4SinglebandPH(const TpDims dims, const GT* __restrict__ G, long g_sector_stride,
                      const int* __restrict__ signs, int n_slots, const int* __restrict__ k_add,
                      const int* __restrict__ q_list, const int* __restrict__ wex_list,
@@ -232,7 +232,8 @@ updateG4SinglebandPH(const TpDims dims, const GT* __restrict__ G, long g_sector_
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);                   // [2]
   GT* stage = reinterpret_cast<GT*>(smem_raw + 16);                        // [2][2 spins][4][R*R]
-  C* Um = reinterpret_cast<C*>(stage + 2 * 8 * blk_elems);                 // [nc][q_chunk]
+  const int n_stages = n_slots > 1 ? 2 : 1;
+  C* Um = reinterpret_cast<C*>(stage + n_stages * 8 * blk_elems);          // [nc][q_chunk]
   C* Uc = Um + q_chunk * nc;
   C* Vm = Uc + q_chunk * nc;
   C* Vc = Vm + q_chunk * nc;
@@ -240,6 +241,15 @@ updateG4SinglebandPH(const TpDims dims, const GT* __restrict__ G, long g_sector_
 
   for (int i = t; i < nc * nc; i += blockDim.x)
     kadd[i] = k_add[i];
+  // Slot-independent shared-memory offsets of this thread's A and B elements.
+  const int k1q_t = k_add[k1 + nc * q];
+  const int a_off = k1 * R + kc * KT;
+  int b_off[KT];
+#pragma unroll
+  for (int j = 0; j < KT; ++j) {
+    const int k2 = min(kc * KT + j, nc - 1);
+    b_off[j] = k_add[k2 + nc * q] * R + k1q_t;
+  }
   const uint32_t blk_bytes = static_cast<uint32_t>(blk_elems * sizeof(GT));
   auto issue = [&](int slot, int st) {
     GT* dst = stage + static_cast<long>(st) * 8 * blk_elems;
@@ -305,15 +315,14 @@ updateG4SinglebandPH(const TpDims dims, const GT* __restrict__ G, long g_sector_
     }
     __syncthreads();
     if (active) {
-      const int k1q = kadd[k1 + nc * q];
       const C um = Um[k1 * q_chunk + ql], uc = Uc[k1 * q_chunk + ql];
 #pragma unroll
       for (int j = 0; j < KT; ++j) {
         const int k2 = kc * KT + j;
         if (k2 < nc) {
-          const int k2q = kadd[k2 + nc * q];
-          C d = cmul(ld(A0 + k1 * R + k2), ld(B0 + k2q * R + k1q));
-          cfma(d, ld(A1 + k1 * R + k2), ld(B1 + k2q * R + k1q));
+          const int ob = b_off[j];
+          C d = cmul(ld(A0 + a_off + j), ld(B0 + ob));
+          cfma(d, ld(A1 + a_off + j), ld(B1 + ob));
           d = cscale(d, hs);
           if (has_mag) {
             C v = cmul(um, Vm[k2 * q_chunk + ql]);
@@ -379,7 +388,7 @@ static bool singlebandPHApplies(const TpDims& d) {
   return (size_t(d.R) * d.R * sizeof(GT)) % 16 == 0;
 }
 
-template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH>
+template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH, int MAXT, int MINB>
 static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_stride, int target_threads,
                                cudaStream_t stream) {
   const TpDims& d = a.dims;
@@ -387,13 +396,14 @@ static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_strid
   const int per_q = d.nc * n_kc;
   if (per_q > 1024)
     return false;
-  const int q_chunk = std::max(1, std::min(d.nq, target_threads / per_q));
+  const int q_chunk = std::max(1, std::min(d.nq, std::min(target_threads, MAXT) / per_q));
   const int threads = per_q * q_chunk;
-  const size_t smem = 16 + sizeof(GT) * 2 * 8 * size_t(d.R) * d.R +
+  const int n_stages = a.n_slots > 1 ? 2 : 1;
+  const size_t smem = 16 + sizeof(GT) * n_stages * 8 * size_t(d.R) * d.R +
                       sizeof(cplx_t<AT>) * 4 * q_chunk * d.nc + sizeof(int) * d.nc * d.nc;
   if (smem > 220 * 1024)
     return false;
-  auto k = updateG4SinglebandPH<GT, AT, KT, QFAST, PREFETCH>;
+  auto k = updateG4SinglebandPH<GT, AT, KT, QFAST, PREFETCH, MAXT, MINB>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int n_qchunks = (d.nq + q_chunk - 1) / q_chunk;
   const dim3 grid(d.nw, d.nw, d.nwq * n_qchunks);
@@ -405,12 +415,16 @@ static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_strid
 
 template <typename GT>
 void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
+  if constexpr (std::is_same_v<GT, float2>) {
+    if (launchUpdateG4SinglebandBatched(a, G, g_sector_stride, stream))
+      return;
+  }
   if (singlebandPHApplies<GT>(a.dims)) {
     bool done;
     if constexpr (std::is_same_v<GT, double2>)
-      done = launchSinglebandPH<double2, double, 4, false, true>(a, G, g_sector_stride, 512, stream);
+      done = launchSinglebandPH<double2, double, 2, false, true, 256, 4>(a, G, g_sector_stride, 256, stream);
     else
-      done = launchSinglebandPH<float2, float, 16, true, false>(a, G, g_sector_stride, 256, stream);
+      done = launchSinglebandPH<float2, float, 16, true, false, 256, 2>(a, G, g_sector_stride, 256, stream);
     if (done)
       return;
   }

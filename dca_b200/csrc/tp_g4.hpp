@@ -26,6 +26,11 @@ struct G4Args {
 // dst += src; src = 0 (sumTo of two accumulators on the same device).
 void launchAddAndClear(double2* dst, double2* src, size_t n, cudaStream_t stream);
 
+// Batched FP32 single-band PH update (tp_g4_batched.cu); false when the configuration is not
+// covered (then launchUpdateG4 uses the general kernels).
+bool launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
+                                     cudaStream_t stream);
+
 // G: block-layout G of n_slots measurements, sector (slot, spin) at g_sector_stride * (2 slot + spin).
 template <typename GT>
 void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream);

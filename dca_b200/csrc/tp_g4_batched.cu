@@ -1,0 +1,291 @@
+// Batched single-band G4 update (the mixed path's PH-magnetic / PH-charge kernel).
+//
+// Same mathematics as updateG4SinglebandPH in tp_g4.cu (see the channel formulas there), tuned
+// for long batches with FP32 G and FP32 partial sums:
+//   * the cluster size is a compile-time constant, so the per-thread loop over k2 is fully
+//     unrolled and all shared-memory offsets that do not depend on the measurement are computed
+//     once, before the batch loop;
+//   * per measurement, the A blocks are pre-scaled by sign/2 in shared memory, so the direct term
+//     D = sum_s A_s B_s arrives scaled;
+//   * consecutive threads take consecutive q: a warp's A reads are broadcasts, its B reads fall in
+//     distinct banks, and the U/V rows are padded so their writes and reads are conflict free;
+//   * tiles (w1, w2) and (w2, w1), which read the same two G blocks A and B (swapped), are launched
+//     next to each other so the second read of each block comes from L2.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "async_copy.cuh"
+#include "common.cuh"
+#include "tp_g4.hpp"
+
+namespace dcaacc {
+
+namespace {
+
+// Tile order: the Nw diagonal tiles first, then the off-diagonal pairs (a, b), (b, a) next to each
+// other.
+__device__ inline void tileOfIndex(int idx, int nw, int& w1, int& w2) {
+  if (idx < nw) {
+    w1 = w2 = idx;
+    return;
+  }
+  const int j = idx - nw;
+  const int p = j >> 1;
+  int b = static_cast<int>((1.0 + sqrt(1.0 + 8.0 * p)) * 0.5);
+  while (b * (b - 1) / 2 > p)
+    --b;
+  while ((b + 1) * b / 2 <= p)
+    ++b;
+  const int a = p - b * (b - 1) / 2;
+  if (j & 1) {
+    w1 = b;
+    w2 = a;
+  }
+  else {
+    w1 = a;
+    w2 = b;
+  }
+}
+
+template <int NC, bool MAG, bool CHARGE>
+__global__ void __launch_bounds__(256, 2)
+updateG4SinglebandBatched(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
+                          const int* __restrict__ signs, int n_slots, const int* __restrict__ k_add,
+                          const int* __restrict__ q_list, const int* __restrict__ wex_list,
+                          double2* const* __restrict__ G4, bool atomic, int q_chunk, int* __restrict__ err) {
+  constexpr int R = NC;
+  constexpr int BLK = R * R;
+  const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq;
+  const int tiles = nw * nw;
+  const int n_qchunks = (nq + q_chunk - 1) / q_chunk;
+  int w1, w2;
+  tileOfIndex(blockIdx.x % tiles, nw, w1, w2);
+  const int rest = blockIdx.x / tiles;
+  const int iwq = rest / n_qchunks, q0 = (rest % n_qchunks) * q_chunk;
+  const int wex = wex_list[iwq];
+  const int ext = dims.ext;
+  const int t = threadIdx.x;
+  const int qp = q_chunk + 1;  // padded row of the U / V tables
+  // Main-phase mapping: q fastest.
+  const int ql = t % q_chunk, k1 = t / q_chunk;
+  const int iq = q0 + ql;
+  const bool active = iq < nq && k1 < NC;
+  const int q = active ? q_list[iq] : 0;
+  // U/V-phase mapping: k fastest.
+  const int kv = t % NC, qv = t / NC;
+  const bool active_v = qv < q_chunk && q0 + qv < nq;
+  const int q_v = active_v ? q_list[q0 + qv] : 0;
+
+  const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
+  const long b_A = (static_cast<long>(w1e) * nw_ext + w2e) * BLK;
+  const long b_B = (static_cast<long>(w2x) * nw_ext + w1x) * BLK;
+  const long b_C = (static_cast<long>(w1e) * nw_ext + w1x) * BLK;
+  const long b_E = (static_cast<long>(w2x) * nw_ext + w2e) * BLK;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);       // [2]
+  float2* stage = reinterpret_cast<float2*>(smem_raw + 16);    // [2][spin][A B C E][BLK]
+  float2* Um = stage + 2 * 8 * BLK;                            // [NC][qp]
+  float2* Uc = Um + NC * qp;
+  float2* Vm = Uc + NC * qp;
+  float2* Vc = Vm + NC * qp;
+
+  int b_off[NC];
+  const int k1q = k_add[k1 % NC + NC * q];
+#pragma unroll
+  for (int j = 0; j < NC; ++j)
+    b_off[j] = k_add[j + NC * q] * R + k1q;
+  const int a_off = (k1 % NC) * R;
+  const int v_c = k_add[kv + NC * q_v];  // k + q for the U/V phase
+
+  constexpr uint32_t blk_bytes = BLK * sizeof(float2);
+  auto issue = [&](int slot, int st) {
+    float2* dst = stage + st * 8 * BLK;
+    mbarArriveExpectTx(&bar[st], 8 * blk_bytes);
+    const float2* src0 = G + g_sector_stride * (2 * slot);
+    const float2* src1 = src0 + g_sector_stride;
+    bulkCopyG2S(dst + 0 * BLK, src0 + b_A, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 1 * BLK, src0 + b_B, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 2 * BLK, src0 + b_C, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 3 * BLK, src0 + b_E, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 4 * BLK, src1 + b_A, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 5 * BLK, src1 + b_B, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 6 * BLK, src1 + b_C, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 7 * BLK, src1 + b_E, blk_bytes, &bar[st]);
+  };
+  if (t == 0) {
+    mbarInit(&bar[0], 1);
+    mbarInit(&bar[1], 1);
+    fenceBarrierInit();
+  }
+  __syncthreads();
+  if (t == 0) {
+    issue(0, 0);
+    if (n_slots > 1)
+      issue(1, 1);
+  }
+
+  float2 acc_m[NC], acc_c[NC];
+#pragma unroll
+  for (int j = 0; j < NC; ++j) {
+    acc_m[j] = make_float2(0.f, 0.f);
+    acc_c[j] = make_float2(0.f, 0.f);
+  }
+
+  for (int m = 0; m < n_slots; ++m) {
+    const int st = m & 1;
+    const bool ok = mbarWait(&bar[st], (m >> 1) & 1, err);
+    if (!__syncthreads_and(ok))
+      return;  // uniform bail-out; the host reports the error word
+    float2* S = stage + st * 8 * BLK;
+    const float hs = 0.5f * static_cast<float>(signs[m]);
+    // Phase 1: scale A_0, A_1 by s/2; U = s/2 (C_0 -+ C_1)(k, k+q), V = (E_0 -+ E_1)(k+q, k).
+    for (int e = t; e < BLK; e += blockDim.x) {
+      float2 a = S[e];
+      S[e] = make_float2(hs * a.x, hs * a.y);
+      a = S[4 * BLK + e];
+      S[4 * BLK + e] = make_float2(hs * a.x, hs * a.y);
+    }
+    if (active_v) {
+      const float2 c0 = S[2 * BLK + kv * R + v_c], c1 = S[6 * BLK + kv * R + v_c];
+      const float2 e0 = S[3 * BLK + v_c * R + kv], e1 = S[7 * BLK + v_c * R + kv];
+      const int o = kv * qp + qv;
+      if (MAG) {
+        Um[o] = make_float2(hs * (c0.x - c1.x), hs * (c0.y - c1.y));
+        Vm[o] = make_float2(e0.x - e1.x, e0.y - e1.y);
+      }
+      if (CHARGE) {
+        Uc[o] = make_float2(hs * (c0.x + c1.x), hs * (c0.y + c1.y));
+        Vc[o] = make_float2(e0.x + e1.x, e0.y + e1.y);
+      }
+    }
+    __syncthreads();
+    // Phase 2: the tile's entries (k1, k2 = 0..NC-1, q).
+    if (active) {
+      const float2* A0 = S + a_off;
+      const float2* A1 = S + 4 * BLK + a_off;
+      const float2* B0 = S + 1 * BLK;
+      const float2* B1 = S + 5 * BLK;
+      const int o = k1 * qp + ql;
+      const float2 um = MAG ? Um[o] : make_float2(0.f, 0.f);
+      const float2 uc = CHARGE ? Uc[o] : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < NC; ++j) {
+        const float2 a0 = A0[j], a1 = A1[j], b0 = B0[b_off[j]], b1 = B1[b_off[j]];
+        float2 d = cmul(a0, b0);
+        cfma(d, a1, b1);
+        if (MAG) {
+          const float2 v = Vm[j * qp + ql];
+          float2& ac = acc_m[j];
+          ac.x = fma(um.x, v.x, ac.x);
+          ac.x = fma(-um.y, v.y, ac.x);
+          ac.y = fma(um.x, v.y, ac.y);
+          ac.y = fma(um.y, v.x, ac.y);
+          ac.x -= d.x;
+          ac.y -= d.y;
+        }
+        if (CHARGE) {
+          const float2 v = Vc[j * qp + ql];
+          float2& ac = acc_c[j];
+          ac.x = fma(uc.x, v.x, ac.x);
+          ac.x = fma(-uc.y, v.y, ac.x);
+          ac.y = fma(uc.x, v.y, ac.y);
+          ac.y = fma(uc.y, v.x, ac.y);
+          ac.x -= d.x;
+          ac.y -= d.y;
+        }
+      }
+    }
+    fenceProxyAsync();  // this thread's generic writes to the stage precede the next bulk copy
+    __syncthreads();    // stage st and the U/V tables are free again
+    if (t == 0 && m + 2 < n_slots)
+      issue(m + 2, st);
+  }
+
+  if (!active)
+    return;
+  const long s_w1 = NC, s_k2 = s_w1 * nw, s_w2 = s_k2 * NC, s_q = s_w2 * nw, s_wq = s_q * nq;
+  const long base = k1 + w1 * s_w1 + w2 * s_w2 + iq * s_q + iwq * s_wq;
+#pragma unroll
+  for (int c = 0; c < kMaxChannels; ++c) {
+    if (c >= dims.n_channels)
+      break;
+    const bool mag = dims.channels[c] == 2;
+    double2* g4 = G4[c] + base;
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+      const float2 v = mag ? acc_m[j] : acc_c[j];
+      double2* p = g4 + j * s_k2;
+      if (atomic) {
+        atomicAdd(&p->x, static_cast<double>(v.x));
+        atomicAdd(&p->y, static_cast<double>(v.y));
+      }
+      else {
+        double2 o = *p;
+        o.x += static_cast<double>(v.x);
+        o.y += static_cast<double>(v.y);
+        *p = o;
+      }
+    }
+  }
+}
+
+template <int NC, bool MAG, bool CHARGE>
+void launchBatched(const G4Args& a, const float2* G, long stride, cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  const int q_chunk = std::max(1, std::min(d.nq, 256 / NC));
+  const int threads = NC * q_chunk;
+  const int qp = q_chunk + 1;
+  const size_t smem = 16 + sizeof(float2) * (2 * 8 * NC * NC + 4 * NC * qp);
+  auto k = updateG4SinglebandBatched<NC, MAG, CHARGE>;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int n_qchunks = (d.nq + q_chunk - 1) / q_chunk;
+  const long blocks = long(d.nw) * d.nw * d.nwq * n_qchunks;
+  k<<<static_cast<unsigned>(blocks), threads, smem, stream>>>(d, G, stride, a.signs, a.n_slots, a.k_add,
+                                                              a.q_list, a.wex_list, a.G4, a.atomic, q_chunk,
+                                                              a.err);
+  DCAACC_LAUNCH_CHECK();
+}
+
+template <int NC>
+bool launchForNc(const G4Args& a, const float2* G, long stride, bool mag, bool charge, cudaStream_t s) {
+  if (mag && charge)
+    launchBatched<NC, true, true>(a, G, stride, s);
+  else if (mag)
+    launchBatched<NC, true, false>(a, G, stride, s);
+  else
+    launchBatched<NC, false, true>(a, G, stride, s);
+  return true;
+}
+
+}  // namespace
+
+bool launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
+                                     cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  if (d.nb != 1)
+    return false;
+  bool mag = false, charge = false;
+  for (int c = 0; c < d.n_channels; ++c) {
+    if (d.channels[c] == 2)
+      mag = true;
+    else if (d.channels[c] == 3)
+      charge = true;
+    else
+      return false;
+  }
+  switch (d.nc) {
+    case 4:
+      return launchForNc<4>(a, G, g_sector_stride, mag, charge, stream);
+    case 8:
+      return launchForNc<8>(a, G, g_sector_stride, mag, charge, stream);
+    case 16:
+      return launchForNc<16>(a, G, g_sector_stride, mag, charge, stream);
+    default:
+      return false;
+  }
+}
+
+}  // namespace dcaacc
