@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -163,6 +164,11 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   if (mixed_) {
     X32_.alloc(x_elems);
     G32_.alloc(g_elems);
+    // The disconnected terms of the one-band PH channels run on the tensor cores unless
+    // DCAACC_TP_SIMT_ONLY=1 (kept to compare both paths).
+    const char* simt_only = std::getenv("DCAACC_TP_SIMT_ONLY");
+    if (singlebandBatchedApplies(dims_) && !(simt_only && std::strcmp(simt_only, "1") == 0))
+      disc_.alloc(discScratchBytes(dims_, max_batch_));
   }
   else {
     X64_.alloc(x_elems);
@@ -368,6 +374,8 @@ void TpAccumulator::process() {
   ga.G4 = G4_ptrs_.get();
   ga.atomic = atomic_;
   ga.err = err_d_.get();
+  ga.disc_scratch = disc_.get();
+  ga.disc_scratch_bytes = disc_.bytes();
   cudaEvent_t b = nullptr;
   timeBegin(DCAACC_STAGE_ROW, &b);
   if (mixed_)
@@ -382,12 +390,10 @@ void TpAccumulator::process() {
     launchColTransform<double>(fa, X64_.get(), G64_.get(), g_sector_stride_, stream_);
   timeEnd(DCAACC_STAGE_COL, b, 1);
   timeBegin(DCAACC_STAGE_G4, &b);
-  if (mixed_)
-    launchUpdateG4<float2>(ga, G32_.get(), g_sector_stride_, stream_);
-  else
-    launchUpdateG4<double2>(ga, G64_.get(), g_sector_stride_, stream_);
-  timeEnd(DCAACC_STAGE_G4, b, 1);
-  launches_ += 3;
+  const int g4_launches = mixed_ ? launchUpdateG4<float2>(ga, G32_.get(), g_sector_stride_, stream_)
+                                 : launchUpdateG4<double2>(ga, G64_.get(), g_sector_stride_, stream_);
+  timeEnd(DCAACC_STAGE_G4, b, g4_launches);
+  launches_ += 2 + g4_launches;
   have_g_ = !mixed_;
   slots_ = 0;
   vtx_used_ = 0;

@@ -150,6 +150,7 @@ private:
   DevBuf<double2> Tr_d_, Tc_d_;
   DevBuf<double2> X64_, G64_;  // FP64 mode
   DevBuf<float2> X32_, G32_;   // mixed mode
+  DevBuf<unsigned char> disc_;  // mixed mode, one band: tensor-core disconnected-term workspace
   // Pinned staging of the batch being assembled.
   PinBuf<SectorDesc> sectors_h_;
   PinBuf<double> tau_h_;

@@ -414,10 +414,10 @@ static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_strid
 }
 
 template <typename GT>
-void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
+int launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
   if constexpr (std::is_same_v<GT, float2>) {
-    if (launchUpdateG4SinglebandBatched(a, G, g_sector_stride, stream))
-      return;
+    if (const int n = launchUpdateG4SinglebandBatched(a, G, g_sector_stride, stream))
+      return n;
   }
   if (singlebandPHApplies<GT>(a.dims)) {
     bool done;
@@ -426,7 +426,7 @@ void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStre
     else
       done = launchSinglebandPH<float2, float, 16, true, false, 256, 2>(a, G, g_sector_stride, 256, stream);
     if (done)
-      return;
+      return 1;
   }
   const dim3 grid(a.dims.nw, a.dims.nw, a.dims.nwq);
   if constexpr (std::is_same_v<GT, double2>) {
@@ -440,10 +440,11 @@ void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStre
         a.G4, a.atomic);
   }
   DCAACC_LAUNCH_CHECK();
+  return 1;
 }
 
-template void launchUpdateG4<double2>(const G4Args&, const double2*, long, cudaStream_t);
-template void launchUpdateG4<float2>(const G4Args&, const float2*, long, cudaStream_t);
+template int launchUpdateG4<double2>(const G4Args&, const double2*, long, cudaStream_t);
+template int launchUpdateG4<float2>(const G4Args&, const float2*, long, cudaStream_t);
 
 }  // namespace dcaacc
 

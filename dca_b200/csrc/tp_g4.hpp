@@ -21,18 +21,31 @@ struct G4Args {
   double2* const* G4;   // [n_channels] device pointers to each channel's running sum (device array)
   bool atomic;          // several accumulators share G4
   int* err;             // device error word (async_copy.cuh kErr* bits)
+  void* disc_scratch = nullptr;   // workspace of the tensor-core disconnected-term GEMM (or null)
+  size_t disc_scratch_bytes = 0;
 };
 
 // dst += src; src = 0 (sumTo of two accumulators on the same device).
 void launchAddAndClear(double2* dst, double2* src, size_t n, cudaStream_t stream);
 
-// Batched FP32 single-band PH update (tp_g4_batched.cu); false when the configuration is not
-// covered (then launchUpdateG4 uses the general kernels).
-bool launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
-                                     cudaStream_t stream);
+// Batched FP32 single-band PH update (tp_g4_batched.cu): one band, Nc in {4, 8, 16}, channels
+// PH-magnetic / PH-charge only.
+bool singlebandBatchedApplies(const TpDims& d);
+// Returns the number of kernels launched, 0 when the configuration is not covered (then
+// launchUpdateG4 uses the general kernels).  With a.disc_scratch large enough, the disconnected
+// terms run on the tensor cores (launchDiscGemm) and the update kernel only adds the direct term.
+int launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
+                                    cudaStream_t stream);
+
+// Tensor-core disconnected terms (tp_g4_disc.cu).  Workspace for batches of up to max_batch
+// measurements; launchDiscGemm returns the device result (per problem an M x M FP32 matrix), or
+// null when a.disc_scratch is missing or too small.
+size_t discScratchBytes(const TpDims& d, int max_batch);
+const float2* launchDiscGemm(const G4Args& a, const float2* G, long g_sector_stride, cudaStream_t stream);
 
 // G: block-layout G of n_slots measurements, sector (slot, spin) at g_sector_stride * (2 slot + spin).
+// Returns the number of kernels launched.
 template <typename GT>
-void launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream);
+int launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream);
 
 }  // namespace dcaacc

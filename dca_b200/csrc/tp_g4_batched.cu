@@ -232,6 +232,147 @@ updateG4SinglebandBatched(const TpDims dims, const float2* __restrict__ G, long 
   }
 }
 
+// Direct term only: sum_m sum_s -s_m/2 G_s(k1 w1; k2 w2) G_s(k2+q w2+x; k1+q w1+x), which is the same
+// for PH-magnetic and PH-charge with one band.  The disconnected terms come from the tensor-core
+// GEMM (tp_g4_disc.cu) in `disc`: per problem (iwq, iq, channel) an M x M matrix (M = Nc Nw) with
+// m = k1 + Nc w1 fastest.  Only the A and B blocks are staged.  The flush goes through shared
+// memory so that consecutive lanes touch consecutive k1 of G4 and of `disc`.
+template <int NC>
+__global__ void __launch_bounds__(256, 2)
+updateG4SinglebandDirect(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
+                         const int* __restrict__ signs, int n_slots, const int* __restrict__ k_add,
+                         const int* __restrict__ q_list, const int* __restrict__ wex_list,
+                         const float2* __restrict__ disc, double2* const* __restrict__ G4, bool atomic,
+                         int q_chunk, int* __restrict__ err) {
+  constexpr int R = NC;
+  constexpr int BLK = R * R;
+  const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq;
+  const int tiles = nw * nw;
+  const int n_qchunks = (nq + q_chunk - 1) / q_chunk;
+  int w1, w2;
+  tileOfIndex(blockIdx.x % tiles, nw, w1, w2);
+  const int rest = blockIdx.x / tiles;
+  const int iwq = rest / n_qchunks, q0 = (rest % n_qchunks) * q_chunk;
+  const int wex = wex_list[iwq];
+  const int ext = dims.ext;
+  const int t = threadIdx.x;
+  const int qp = q_chunk + 1;  // padded row of the flush table
+  const int ql = t % q_chunk, k1 = t / q_chunk;
+  const int iq = q0 + ql;
+  const bool active = iq < nq && k1 < NC;
+  const int q = active ? q_list[iq] : 0;
+
+  const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
+  const long b_A = (static_cast<long>(w1e) * nw_ext + w2e) * BLK;
+  const long b_B = (static_cast<long>(w2x) * nw_ext + w1x) * BLK;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);     // [2]
+  float2* stage = reinterpret_cast<float2*>(smem_raw + 16);  // [2][A0 B0 A1 B1][BLK]
+
+  int b_off[NC];
+  const int k1q = k_add[k1 % NC + NC * q];
+#pragma unroll
+  for (int j = 0; j < NC; ++j)
+    b_off[j] = k_add[j + NC * q] * R + k1q;
+  const int a_off = (k1 % NC) * R;
+
+  constexpr uint32_t blk_bytes = BLK * sizeof(float2);
+  auto issue = [&](int slot, int st) {
+    float2* dst = stage + st * 4 * BLK;
+    mbarArriveExpectTx(&bar[st], 4 * blk_bytes);
+    const float2* src0 = G + g_sector_stride * (2 * slot);
+    const float2* src1 = src0 + g_sector_stride;
+    bulkCopyG2S(dst + 0 * BLK, src0 + b_A, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 1 * BLK, src0 + b_B, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 2 * BLK, src1 + b_A, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 3 * BLK, src1 + b_B, blk_bytes, &bar[st]);
+  };
+  if (t == 0) {
+    mbarInit(&bar[0], 1);
+    mbarInit(&bar[1], 1);
+    fenceBarrierInit();
+  }
+  __syncthreads();
+  if (t == 0) {
+    issue(0, 0);
+    if (n_slots > 1)
+      issue(1, 1);
+  }
+
+  float2 acc[NC];
+#pragma unroll
+  for (int j = 0; j < NC; ++j)
+    acc[j] = make_float2(0.f, 0.f);
+
+  for (int m = 0; m < n_slots; ++m) {
+    const int st = m & 1;
+    const bool ok = mbarWait(&bar[st], (m >> 1) & 1, err);
+    if (!__syncthreads_and(ok))
+      return;  // uniform bail-out; the host reports the error word
+    float2* S = stage + st * 4 * BLK;
+    const float nhs = -0.5f * static_cast<float>(signs[m]);
+    for (int e = t; e < BLK; e += blockDim.x) {  // A_0, A_1 *= -s/2
+      float2 a = S[e];
+      S[e] = make_float2(nhs * a.x, nhs * a.y);
+      a = S[2 * BLK + e];
+      S[2 * BLK + e] = make_float2(nhs * a.x, nhs * a.y);
+    }
+    __syncthreads();
+    if (active) {
+      const float2* A0 = S + a_off;
+      const float2* B0 = S + 1 * BLK;
+      const float2* A1 = S + 2 * BLK + a_off;
+      const float2* B1 = S + 3 * BLK;
+#pragma unroll
+      for (int j = 0; j < NC; ++j) {
+        cfma(acc[j], A0[j], B0[b_off[j]]);
+        cfma(acc[j], A1[j], B1[b_off[j]]);
+      }
+    }
+    fenceProxyAsync();  // this thread's generic writes to the stage precede the next bulk copy
+    __syncthreads();    // stage st is free again
+    if (t == 0 && m + 2 < n_slots)
+      issue(m + 2, st);
+  }
+
+  // Flush: table T[j][k1][ql] (rows padded to qp), then lanes take consecutive k1.
+  float2* T = stage;
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < NC; ++j)
+      T[(j * NC + k1) * qp + ql] = acc[j];
+  }
+  __syncthreads();
+  const long M = static_cast<long>(NC) * nw;
+  const long s_w1 = NC, s_k2 = s_w1 * nw, s_w2 = s_k2 * NC, s_q = s_w2 * nw, s_wq = s_q * nq;
+  const int n_ch = dims.n_channels;
+  for (int idx = t; idx < NC * NC * q_chunk; idx += blockDim.x) {
+    const int fk1 = idx % NC, j = (idx / NC) % NC, fql = idx / (NC * NC);
+    const int fiq = q0 + fql;
+    if (fiq >= nq)
+      continue;
+    const float2 v = T[(j * NC + fk1) * qp + fql];
+    const long g4i = fk1 + w1 * s_w1 + j * s_k2 + w2 * s_w2 + fiq * s_q + iwq * s_wq;
+    const long di = (j + static_cast<long>(NC) * w2) * M + fk1 + static_cast<long>(NC) * w1;
+    for (int c = 0; c < n_ch; ++c) {
+      const float2 dv = disc[(static_cast<long>(iwq * nq + fiq) * n_ch + c) * M * M + di];
+      double2* p = G4[c] + g4i;
+      const double re = static_cast<double>(v.x + dv.x), im = static_cast<double>(v.y + dv.y);
+      if (atomic) {
+        atomicAdd(&p->x, re);
+        atomicAdd(&p->y, im);
+      }
+      else {
+        double2 o = *p;
+        o.x += re;
+        o.y += im;
+        *p = o;
+      }
+    }
+  }
+}
+
 template <int NC, bool MAG, bool CHARGE>
 void launchBatched(const G4Args& a, const float2* G, long stride, cudaStream_t stream) {
   const TpDims& d = a.dims;
@@ -250,42 +391,64 @@ void launchBatched(const G4Args& a, const float2* G, long stride, cudaStream_t s
 }
 
 template <int NC>
-bool launchForNc(const G4Args& a, const float2* G, long stride, bool mag, bool charge, cudaStream_t s) {
+void launchDirect(const G4Args& a, const float2* G, long stride, const float2* disc, cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  const int q_chunk = std::max(1, std::min(d.nq, 256 / NC));
+  const int threads = NC * q_chunk;
+  const int qp = q_chunk + 1;
+  const size_t smem = 16 + sizeof(float2) * std::max<size_t>(2 * 4 * NC * NC, size_t(NC) * NC * qp);
+  auto k = updateG4SinglebandDirect<NC>;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int n_qchunks = (d.nq + q_chunk - 1) / q_chunk;
+  const long blocks = long(d.nw) * d.nw * d.nwq * n_qchunks;
+  k<<<static_cast<unsigned>(blocks), threads, smem, stream>>>(d, G, stride, a.signs, a.n_slots, a.k_add,
+                                                              a.q_list, a.wex_list, disc, a.G4, a.atomic,
+                                                              q_chunk, a.err);
+  DCAACC_LAUNCH_CHECK();
+}
+
+template <int NC>
+int launchForNc(const G4Args& a, const float2* G, long stride, bool mag, bool charge, cudaStream_t s) {
+  if (const float2* disc = launchDiscGemm(a, G, stride, s)) {
+    launchDirect<NC>(a, G, stride, disc, s);
+    return 3;
+  }
   if (mag && charge)
     launchBatched<NC, true, true>(a, G, stride, s);
   else if (mag)
     launchBatched<NC, true, false>(a, G, stride, s);
   else
     launchBatched<NC, false, true>(a, G, stride, s);
-  return true;
+  return 1;
 }
 
 }  // namespace
 
-bool launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
-                                     cudaStream_t stream) {
+int launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
+                                    cudaStream_t stream) {
   const TpDims& d = a.dims;
-  if (d.nb != 1)
-    return false;
+  if (!singlebandBatchedApplies(d))
+    return 0;
   bool mag = false, charge = false;
-  for (int c = 0; c < d.n_channels; ++c) {
-    if (d.channels[c] == 2)
-      mag = true;
-    else if (d.channels[c] == 3)
-      charge = true;
-    else
-      return false;
-  }
+  for (int c = 0; c < d.n_channels; ++c)
+    (d.channels[c] == 2 ? mag : charge) = true;
   switch (d.nc) {
     case 4:
       return launchForNc<4>(a, G, g_sector_stride, mag, charge, stream);
     case 8:
       return launchForNc<8>(a, G, g_sector_stride, mag, charge, stream);
-    case 16:
-      return launchForNc<16>(a, G, g_sector_stride, mag, charge, stream);
     default:
-      return false;
+      return launchForNc<16>(a, G, g_sector_stride, mag, charge, stream);
   }
+}
+
+bool singlebandBatchedApplies(const TpDims& d) {
+  if (d.nb != 1 || (d.nc != 4 && d.nc != 8 && d.nc != 16))
+    return false;
+  for (int c = 0; c < d.n_channels; ++c)
+    if (d.channels[c] != 2 && d.channels[c] != 3)
+      return false;
+  return d.n_channels > 0;
 }
 
 }  // namespace dcaacc

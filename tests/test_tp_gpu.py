@@ -87,6 +87,38 @@ def test_mixed_equals_fp64_gpu_at_full_batch():
     assert max(errs) <= MIXED_TOL
 
 
+def _run_timed(case, simt_only, monkeypatch, **kw):
+    """Mixed run with stage timing on; DCAACC_TP_SIMT_ONLY selects the update path at creation."""
+    from dca_b200.accumulators import TpAccumulator
+    monkeypatch.setenv("DCAACC_TP_SIMT_ONLY", "1" if simt_only else "0")
+    acc = TpAccumulator(case.G0, case.tp_params(precision=1, **kw))
+    acc.enable_timing(True)
+    acc.resetAccumulation(0)
+    for m in case.measurements:
+        acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    acc.finalize()
+    return acc
+
+
+@pytest.mark.parametrize("wname,n_meas,max_batch", [("c1", 6, 4), ("c3", 9, 4), ("c3", 70, 72)])
+def test_tensor_core_disconnected_terms_match_oracle(oracle_lib, monkeypatch, wname, n_meas, max_batch):
+    """The one-band PH update with its disconnected terms on tcgen05 (split BF16, FP32 accumulate)
+    against the all-SIMT update and an FP64 reference: the oracle for c1, the FP64 GPU path (pinned
+    to the oracle above) for c3.  (c3, 70, 72) takes two K chunks in the GEMM (batch padded to
+    128); c1 (M = 64) pads the rows to one 128-row tile."""
+    case = case_from_workload(W.WORKLOADS[wname], n_meas)
+    tc = _run_timed(case, False, monkeypatch, max_batch=max_batch)
+    simt = _run_timed(case, True, monkeypatch, max_batch=max_batch)
+    batches = -(-n_meas // max_batch)
+    assert tc.stage_times()["update_g4"][1] == 3 * batches      # planes + GEMM + direct term
+    assert simt.stage_times()["update_g4"][1] == batches
+    exact = run_oracle(oracle_lib, case) if wname == "c1" else run_gpu(case, precision=0, max_batch=1)
+    for got, ref, want in zip(tc.get_G4(), simt.get_G4(), exact.get_G4()):
+        print(wname, n_meas, "tensor-core / SIMT relative errors:", rel_err(got, want), rel_err(ref, want))
+        assert rel_err(got, want) <= MIXED_TOL
+        assert rel_err(ref, want) <= MIXED_TOL
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_sum_to_equals_single_accumulator(precision):
     case, _ = golden("sq2_all")
