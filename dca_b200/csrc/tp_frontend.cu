@@ -91,15 +91,17 @@ rowTransformKernel(const TpDims dims, const SectorDesc* __restrict__ sectors,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int MS = IB + 1;               // padded row of Ms (no bank conflicts across jc)
   C* Xs = reinterpret_cast<C*>(smem_raw);   // [n_orb][JC][WC]
-  C* Fs = Xs + JC * WC * n_orb;             // [nb][nc][nc]
+  C* Fs = Xs + JC * WC * n_orb;             // [nb][r][k]: lanes that differ in k read distinct banks
   C* Ts = Fs + nb * nc * nc;                // [IB][WC]
   Real* Ms = reinterpret_cast<Real*>(Ts + IB * WC);  // [JC][MS]
   int* rs = reinterpret_cast<int*>(Ms + JC * MS);    // [n_orb + 1]
 
   const int* pr = perm_r + sd.vtx_off;
   const int* pc = perm_c + sd.vtx_off;
-  for (int idx = t; idx < nb * nc * nc; idx += blockDim.x)
-    Fs[idx] = loadC<Real>(Fb + idx);
+  for (int idx = t; idx < nb * nc * nc; idx += blockDim.x) {  // Fb is (b, k, r); Fs is (b, r, k)
+    const int b = idx / (nc * nc), k = (idx / nc) % nc, r = idx % nc;
+    Fs[(b * nc + r) * nc + k] = loadC<Real>(Fb + idx);
+  }
   for (int idx = t; idx <= n_orb; idx += blockDim.x)
     rs[idx] = row_start[sd.orb_off + idx];
   const int jc_count = min(JC, n - jj0);
@@ -156,10 +158,10 @@ rowTransformKernel(const TpDims dims, const SectorDesc* __restrict__ sectors,
       continue;
     const int b1 = row % nb, k1 = row / nb;
     const C* x = Xs + b1 * JC * WC + c * WC + ww;
-    const C* f = Fs + (b1 * nc + k1) * nc;
+    const C* f = Fs + b1 * nc * nc + k1;
     C a = mk(Real(0), Real(0));
     for (int r1 = 0; r1 < nc; ++r1)
-      cfma(a, f[r1], x[nb * r1 * JC * WC]);
+      cfma(a, f[r1 * nc], x[nb * r1 * JC * WC]);
     Xp[sd.x_off + (static_cast<long>(we) * n + jj0 + c) * R + row] = a;
   }
 }

@@ -77,13 +77,23 @@ DiscShape discShape(const TpDims& d, int batch) {
   return s;
 }
 
-// One thread per (slot, row) of one problem (blockIdx.y = iwq * nq + iq, blockIdx.z = channel).
-// A planes: [prob][plane][P rows][kp], B planes: [prob][plane][2P rows][kp].
-__global__ void discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
-                                 const int* __restrict__ signs, int n_slots, int Bp, int P,
-                                 const int* __restrict__ k_add, const int* __restrict__ q_list,
-                                 const int* __restrict__ wex_list, __nv_bfloat16* __restrict__ Ap,
-                                 __nv_bfloat16* __restrict__ Bpl) {
+// Eight BF16 values packed for one 16-byte store.
+struct Pack8 {
+  __nv_bfloat16 v[8];
+};
+__device__ inline void store8(__nv_bfloat16* dst, const Pack8& p) {
+  *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(&p);
+}
+
+// One thread per (row, group of 8 measurements) of one problem (blockIdx.y = iwq * nq + iq,
+// blockIdx.z = channel); the 8 groups of a row are adjacent threads, so each plane row is written
+// with contiguous 16-byte stores.  A planes: [prob][plane][P rows][kp], B planes:
+// [prob][plane][2P rows][kp], kp = 2 Bp.
+__global__ void __launch_bounds__(256)
+discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
+                 const int* __restrict__ signs, int n_slots, int Bp, int P, const int* __restrict__ k_add,
+                 const int* __restrict__ q_list, const int* __restrict__ wex_list,
+                 __nv_bfloat16* __restrict__ Ap, __nv_bfloat16* __restrict__ Bpl) {
   const int nc = dims.nc, nw_ext = dims.nw_ext, ext = dims.ext, R = dims.R;
   const int M = nc * dims.nw;
   const int p = blockIdx.y;
@@ -97,39 +107,57 @@ __global__ void discPlanesKernel(const TpDims dims, const float2* __restrict__ G
   const long prob = static_cast<long>(p) * gridDim.z + ch;
   __nv_bfloat16* A = Ap + prob * kPlanes * plane_a;
   __nv_bfloat16* Bm = Bpl + prob * kPlanes * plane_b;
-  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(Bp) * P;
+  const int groups = Bp / 8;
+  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * P;
        idx += long(gridDim.x) * blockDim.x) {
-    const int row = static_cast<int>(idx % P);
-    const int slot = static_cast<int>(idx / P);
-    float2 u = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
-    if (slot < n_slots && row < M) {
+    const int grp = static_cast<int>(idx % groups);
+    const int row = static_cast<int>(idx / groups);
+    const int slot0 = grp * 8;
+    long bc = 0, be = 0;
+    const bool in_row = row < M;
+    if (in_row) {
       const int k = row % nc, w = row / nc;
-      const float hs = 0.5f * static_cast<float>(signs[slot]);
-      const float2* G0s = G + g_sector_stride * (2 * slot);
-      const float2* G1s = G0s + g_sector_stride;
       const int kq = k_add[k + nc * q];
       const int we = w + ext, wx = we + wex;
-      const long bc = (static_cast<long>(we) * nw_ext + wx) * R * R + static_cast<long>(k) * R + kq;
-      const long be = (static_cast<long>(wx) * nw_ext + we) * R * R + static_cast<long>(kq) * R + k;
-      const float2 c0 = G0s[bc], c1 = G1s[bc], e0 = G0s[be], e1 = G1s[be];
-      u = make_float2(hs * (c0.x + sg * c1.x), hs * (c0.y + sg * c1.y));
-      v = make_float2(e0.x + sg * e1.x, e0.y + sg * e1.y);
+      bc = (static_cast<long>(we) * nw_ext + wx) * R * R + static_cast<long>(k) * R + kq;
+      be = (static_cast<long>(wx) * nw_ext + we) * R * R + static_cast<long>(kq) * R + k;
+    }
+    Pack8 ur[kPlanes], ui[kPlanes], vr[kPlanes], vi[kPlanes], mvi[kPlanes];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int slot = slot0 + e;
+      float2 u = make_float2(0.f, 0.f), v = make_float2(0.f, 0.f);
+      if (in_row && slot < n_slots) {
+        const float hs = 0.5f * static_cast<float>(signs[slot]);
+        const float2* G0s = G + g_sector_stride * (2 * slot);
+        const float2* G1s = G0s + g_sector_stride;
+        const float2 c0 = G0s[bc], c1 = G1s[bc], e0 = G0s[be], e1 = G1s[be];
+        u = make_float2(hs * (c0.x + sg * c1.x), hs * (c0.y + sg * c1.y));
+        v = make_float2(e0.x + sg * e1.x, e0.y + sg * e1.y);
+      }
+      const Split3 a = split3(u.x), b = split3(u.y), c = split3(v.x), d = split3(v.y), f = split3(-v.y);
+      ur[0].v[e] = a.h, ur[1].v[e] = a.m, ur[2].v[e] = a.l;
+      ui[0].v[e] = b.h, ui[1].v[e] = b.m, ui[2].v[e] = b.l;
+      vr[0].v[e] = c.h, vr[1].v[e] = c.m, vr[2].v[e] = c.l;
+      vi[0].v[e] = d.h, vi[1].v[e] = d.m, vi[2].v[e] = d.l;
+      mvi[0].v[e] = f.h, mvi[1].v[e] = f.m, mvi[2].v[e] = f.l;
     }
     // A: row m = k + nc w, columns slot (real) and Bp + slot (imaginary).
-    const Split3 ur = split3(u.x), ui = split3(u.y);
-    const long a0 = static_cast<long>(row) * kp + slot, a1 = a0 + Bp;
-    A[a0] = ur.h, A[plane_a + a0] = ur.m, A[2 * plane_a + a0] = ur.l;
-    A[a1] = ui.h, A[plane_a + a1] = ui.m, A[2 * plane_a + a1] = ui.l;
     // B: complex column n = row in block cb = n / 64; real-part row cb*128 + c holds
     // [Vr | -Vi], imaginary-part row cb*128 + 64 + c holds [Vi | Vr].
     const int cb = row / kTileNc, cc = row % kTileNc;
     const long rre = static_cast<long>(cb) * 2 * kTileNc + cc, rim = rre + kTileNc;
-    const Split3 vr = split3(v.x), vi = split3(v.y), mvi = split3(-v.y);
-    const long bre0 = rre * kp + slot, bre1 = bre0 + Bp, bim0 = rim * kp + slot, bim1 = bim0 + Bp;
-    Bm[bre0] = vr.h, Bm[plane_b + bre0] = vr.m, Bm[2 * plane_b + bre0] = vr.l;
-    Bm[bre1] = mvi.h, Bm[plane_b + bre1] = mvi.m, Bm[2 * plane_b + bre1] = mvi.l;
-    Bm[bim0] = vi.h, Bm[plane_b + bim0] = vi.m, Bm[2 * plane_b + bim0] = vi.l;
-    Bm[bim1] = vr.h, Bm[plane_b + bim1] = vr.m, Bm[2 * plane_b + bim1] = vr.l;
+    const long a0 = static_cast<long>(row) * kp + slot0, a1 = a0 + Bp;
+    const long bre0 = rre * kp + slot0, bre1 = bre0 + Bp, bim0 = rim * kp + slot0, bim1 = bim0 + Bp;
+#pragma unroll
+    for (int pl = 0; pl < kPlanes; ++pl) {
+      store8(A + pl * plane_a + a0, ur[pl]);
+      store8(A + pl * plane_a + a1, ui[pl]);
+      store8(Bm + pl * plane_b + bre0, vr[pl]);
+      store8(Bm + pl * plane_b + bre1, mvi[pl]);
+      store8(Bm + pl * plane_b + bim0, vi[pl]);
+      store8(Bm + pl * plane_b + bim1, vr[pl]);
+    }
   }
 }
 
@@ -274,7 +302,7 @@ const float2* launchDiscGemm(const G4Args& a, const float2* G, long g_sector_str
   __nv_bfloat16* Bpl = Ap + size_t(s.probs) * kPlanes * s.plane_a;
   float2* out = reinterpret_cast<float2*>(Bpl + size_t(s.probs) * kPlanes * s.plane_b);
   {
-    const long work = long(s.Bp) * s.P;
+    const long work = long(s.Bp / 8) * s.P;
     const dim3 grid(static_cast<unsigned>(std::max(1L, std::min(1024L, (work + 255) / 256))), d.nq * d.nwq,
                     d.n_channels);
     discPlanesKernel<<<grid, 256, 0, stream>>>(d, G, g_sector_stride, a.signs, a.n_slots, s.Bp, s.P, a.k_add,
