@@ -50,6 +50,10 @@ __device__ inline void bulkCopyG2S(void* dst, const void* src, uint32_t bytes, u
       : "memory");
 }
 
+__device__ inline void mbarArrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+
 __device__ inline bool mbarTryWait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(

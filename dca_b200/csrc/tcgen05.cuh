@@ -101,6 +101,22 @@ __device__ inline void ld32x32bx16(uint32_t taddr, float (&v)[16]) {
     v[i] = __uint_as_float(r[i]);
 }
 
+// As ld32x32bx16, 32 consecutive columns.
+__device__ inline void ld32x32bx32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 32; ++i)
+    v[i] = __uint_as_float(r[i]);
+}
+
 __device__ inline void waitLd() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -112,6 +128,21 @@ __device__ inline void cpAsync16(void* smem_dst, const void* gmem_src) {
 
 __device__ inline void cpAsyncWaitAll() {
   asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// ---- Tensor memory access (TMA) ----
+// 3-D tiled load (box from the tensor map) into shared memory, completing `bytes` of the
+// mbarrier's transaction count.  Plain (non-multicast) form only.  The innermost coordinate x
+// must be a multiple of 16 bytes' worth of elements.
+__device__ inline void tmaLoad3d(void* smem_dst, const void* tmap, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smemAddr(smem_dst)), "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smemAddr(bar))
+      : "memory");
+}
+
+__device__ inline void prefetchTensorMap(const void* tmap) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
 }
 
 }  // namespace tc

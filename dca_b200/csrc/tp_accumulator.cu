@@ -162,13 +162,26 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   const size_t x_elems = n_sec * size_t(R) * max_order_ * nw_ext;
   const size_t g_elems = n_sec * size_t(g_sector_stride_);
   if (mixed_) {
-    X32_.alloc(x_elems);
+    // The mixed path runs its front-end and the disconnected terms of the one-band PH channels on
+    // the tensor cores, unless DCAACC_TP_SIMT_ONLY=1 selects the all-SIMT kernels (kept to compare
+    // both paths).
+    const char* simt_env = std::getenv("DCAACC_TP_SIMT_ONLY");
+    const bool simt_only = simt_env && std::strcmp(simt_env, "1") == 0;
     G32_.alloc(g_elems);
-    // The disconnected terms of the one-band PH channels run on the tensor cores unless
-    // DCAACC_TP_SIMT_ONLY=1 (kept to compare both paths).
-    const char* simt_only = std::getenv("DCAACC_TP_SIMT_ONLY");
-    if (singlebandBatchedApplies(dims_) && !(simt_only && std::strcmp(simt_only, "1") == 0))
-      disc_.alloc(discScratchBytes(dims_, max_batch_));
+    if (simt_only) {
+      X32_.alloc(x_elems);
+    }
+    else {
+      tc_front_ = true;
+      const FrontTcShape fs = frontTcShape(dims_, int(n_sec), max_order_);
+      ftc_mem_.alloc(frontTcBytes(fs));
+      DCAACC_CUDA_CHECK(cudaMemset(ftc_mem_.get(), 0, ftc_mem_.bytes()));  // padding rows stay zero
+      frontTcInit(ftc_, fs, ftc_mem_.get());
+      orb_r_d_.alloc(n_vtx);
+      orb_c_d_.alloc(n_vtx);
+      if (singlebandBatchedApplies(dims_))
+        disc_.alloc(discScratchBytes(dims_, max_batch_));
+    }
   }
   else {
     X64_.alloc(x_elems);
@@ -181,9 +194,11 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   rstart_h_.alloc(n_sec * n_orb1);
   cstart_h_.alloc(n_sec * n_orb1);
   signs_h_.alloc(max_batch_);
+  orb_r_h_.alloc(n_vtx);
+  orb_c_h_.alloc(n_vtx);
   DCAACC_CUDA_CHECK(cudaEventRecord(upload_done_, stream_));
 
-  if (frontendSmemRequirement(dims_, max_order_, !mixed_) > 227 * 1024)
+  if (!tc_front_ && frontendSmemRequirement(dims_, max_order_, !mixed_) > 227 * 1024)
     invalid("max_order too large for the front-end's shared-memory tiles");
   G4_host_.assign(c.n_channels, {});
 }
@@ -295,6 +310,13 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
       std::copy_n(perm_r_h_.get() + vtx_off, n, perm_c_h_.get() + vtx_off);
       std::copy_n(rstart_h_.get() + orb_off, n_orb + 1, cstart_h_.get() + orb_off);
     }
+    // Orbital of each sorted position (the tensor-core front-end's per-vertex phases).
+    for (int o = 0; o < n_orb; ++o) {
+      const int* rs = rstart_h_.get() + orb_off;
+      const int* cs = cstart_h_.get() + orb_off;
+      std::fill(orb_r_h_.get() + vtx_off + rs[o], orb_r_h_.get() + vtx_off + rs[o + 1], o);
+      std::fill(orb_c_h_.get() + vtx_off + cs[o], orb_c_h_.get() + vtx_off + cs[o + 1], o);
+    }
     std::copy_n(x.tau, n, tau_h_.get() + vtx_off);
 
     const double* Mptr = x.M;
@@ -340,6 +362,10 @@ void TpAccumulator::process() {
   h2d(rstart_d_.get(), rstart_h_.get(), sizeof(int) * n_sec * n_orb1);
   h2d(cstart_d_.get(), cstart_h_.get(), sizeof(int) * n_sec * n_orb1);
   h2d(signs_d_.get(), signs_h_.get(), sizeof(int) * slots_);
+  if (tc_front_) {
+    h2d(orb_r_d_.get(), orb_r_h_.get(), sizeof(int) * vtx_used_);
+    h2d(orb_c_d_.get(), (non_density_ ? orb_c_h_ : orb_r_h_).get(), sizeof(int) * vtx_used_);
+  }
   DCAACC_CUDA_CHECK(cudaEventRecord(upload_done_, stream_));
 
   FrontendArgs fa{};
@@ -359,9 +385,16 @@ void TpAccumulator::process() {
   if (n_max_batch_ > 0) {
     cudaEvent_t b = nullptr;
     timeBegin(DCAACC_STAGE_TWIDDLE, &b);
-    launchTwiddles(fa, stream_);
-    launches_ += non_density_ ? 2 : 1;
-    timeEnd(DCAACC_STAGE_TWIDDLE, b, non_density_ ? 2 : 1);
+    int n_prep;
+    if (tc_front_) {
+      n_prep = launchFrontendTcPrep(fa, ftc_, orb_r_d_.get(), orb_c_d_.get(), stream_);
+    }
+    else {
+      launchTwiddles(fa, stream_);
+      n_prep = non_density_ ? 2 : 1;
+    }
+    launches_ += n_prep;
+    timeEnd(DCAACC_STAGE_TWIDDLE, b, n_prep);
   }
   G4Args ga{};
   ga.dims = dims_;
@@ -378,13 +411,17 @@ void TpAccumulator::process() {
   ga.disc_scratch_bytes = disc_.bytes();
   cudaEvent_t b = nullptr;
   timeBegin(DCAACC_STAGE_ROW, &b);
-  if (mixed_)
+  if (tc_front_)
+    launchFrontendTcRow(fa, ftc_, err_d_.get(), stream_);
+  else if (mixed_)
     launchRowTransform<float>(fa, X32_.get(), stream_);
   else
     launchRowTransform<double>(fa, X64_.get(), stream_);
   timeEnd(DCAACC_STAGE_ROW, b, 1);
   timeBegin(DCAACC_STAGE_COL, &b);
-  if (mixed_)
+  if (tc_front_)
+    launchFrontendTcCol(fa, ftc_, G32_.get(), g_sector_stride_, err_d_.get(), stream_);
+  else if (mixed_)
     launchColTransform<float>(fa, X32_.get(), G32_.get(), g_sector_stride_, stream_);
   else
     launchColTransform<double>(fa, X64_.get(), G64_.get(), g_sector_stride_, stream_);

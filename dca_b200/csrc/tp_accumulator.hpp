@@ -16,6 +16,7 @@
 
 #include "../../include/dcaacc.h"
 #include "common.cuh"
+#include "tp_frontend.hpp"
 #include "tp_layout.hpp"
 
 namespace dcaacc {
@@ -151,10 +152,16 @@ private:
   DevBuf<double2> X64_, G64_;  // FP64 mode
   DevBuf<float2> X32_, G32_;   // mixed mode
   DevBuf<unsigned char> disc_;  // mixed mode, one band: tensor-core disconnected-term workspace
+  // Mixed mode: tensor-core front-end (operand planes + TMA descriptors) and the orbital of each
+  // vertex in row / column order.
+  bool tc_front_ = false;
+  DevBuf<unsigned char> ftc_mem_;
+  FrontTcWorkspace ftc_{};
+  DevBuf<int> orb_r_d_, orb_c_d_;
   // Pinned staging of the batch being assembled.
   PinBuf<SectorDesc> sectors_h_;
   PinBuf<double> tau_h_;
-  PinBuf<int> perm_r_h_, perm_c_h_, rstart_h_, cstart_h_, signs_h_;
+  PinBuf<int> perm_r_h_, perm_c_h_, rstart_h_, cstart_h_, signs_h_, orb_r_h_, orb_c_h_;
 
   // Batch bookkeeping.
   int slots_ = 0;         // measurements staged

@@ -1,6 +1,7 @@
 // Launch interface of the two-particle front-end kernels (tp_frontend.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -37,5 +38,37 @@ void launchColTransform(const FrontendArgs& a, const cplx_t<Real>* Xp, cplx_t<Re
                         long g_sector_stride, cudaStream_t stream);
 
 size_t frontendSmemRequirement(const TpDims& d, int n_max, bool fp64);
+
+// ---- Tensor-core front-end of the mixed path (tp_frontend_tc.cu) ----
+// Workspace: split-BF16 operand planes for a batch of n_sectors sectors of order <= max_order.
+struct FrontTcShape {
+  int D;    // R * NwExt, rows and columns of G
+  int Dp;   // D rounded up to 128 (GEMM row tiles)
+  int Dq;   // D rounded up to 64 (complex column tiles)
+  int Kr;   // max_order rounded up to 64 (vertex extent of every plane row)
+  int n_sectors;
+  size_t pr_elems, mb_elems, ac_elems, bq_elems;  // BF16 elements of P, M, X' and Q planes
+};
+struct FrontTcWorkspace {
+  FrontTcShape shape;
+  void* pr = nullptr;
+  void* mb = nullptr;
+  void* ac = nullptr;
+  void* bq = nullptr;
+  CUtensorMap tm_pr, tm_mb, tm_ac, tm_bq;  // TMA descriptors of the four plane arrays
+};
+FrontTcShape frontTcShape(const TpDims& d, int n_sectors, int max_order);
+size_t frontTcBytes(const FrontTcShape& s);
+// Carves `mem` (frontTcBytes, zero-filled by the caller) and encodes the tensor maps.
+void frontTcInit(FrontTcWorkspace& w, const FrontTcShape& s, void* mem);
+// Twiddles in (w, vertex) order into a.Tr / a.Tc and the P, M and Q planes; returns the number of
+// kernels launched.  orb_r / orb_c: orbital (band + nb site) of each vertex in row / column order.
+int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const int* orb_r, const int* orb_c,
+                         cudaStream_t stream);
+// X' = P M (one launch).
+void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* err, cudaStream_t stream);
+// G = X' Q^H + beta G0 delta into the block-layout G (one launch).
+void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
+                         int* err, cudaStream_t stream);
 
 }  // namespace dcaacc
