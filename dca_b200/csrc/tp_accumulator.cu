@@ -407,6 +407,13 @@ void TpAccumulator::process() {
   ga.G4 = G4_ptrs_.get();
   ga.atomic = atomic_;
   ga.err = err_d_.get();
+  {
+    std::vector<int> seen(dims_.nc, 0);
+    int distinct = 0;
+    for (int q : q_list_)
+      distinct += seen[q]++ == 0;
+    ga.q_all = distinct == dims_.nc && int(q_list_.size()) == dims_.nc;
+  }
   ga.disc_scratch = disc_.get();
   ga.disc_scratch_bytes = disc_.bytes();
   cudaEvent_t b = nullptr;

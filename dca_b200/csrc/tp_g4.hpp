@@ -21,6 +21,7 @@ struct G4Args {
   double2* const* G4;   // [n_channels] device pointers to each channel's running sum (device array)
   bool atomic;          // several accumulators share G4
   int* err;             // device error word (async_copy.cuh kErr* bits)
+  bool q_all = false;             // q_list is a permutation of all Nc cluster momenta
   void* disc_scratch = nullptr;   // workspace of the tensor-core disconnected-term GEMM (or null)
   size_t disc_scratch_bytes = 0;
 };

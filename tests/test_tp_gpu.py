@@ -100,19 +100,32 @@ def _run_timed(case, simt_only, monkeypatch, **kw):
     return acc
 
 
-@pytest.mark.parametrize("wname,n_meas,max_batch", [("c1", 6, 4), ("c3", 9, 4), ("c3", 70, 72)])
+def _small_all_transfers(cluster_kind, freq_transfer):
+    """c1-like single-band workloads with every momentum transfer and both PH channels: they take
+    the outer-product direct-term kernel at Nc = 4 and 8."""
+    import dataclasses
+    return dataclasses.replace(W.WORKLOADS["c1"], name=f"all-q {cluster_kind[0]}", cluster_kind=cluster_kind,
+                               all_transfers=True, freq_transfer=freq_transfer, channels=(2, 3))
+
+
+EXTRA_WORKLOADS = {"sq2_allq": _small_all_transfers(("square", 2), 1),
+                   "betts8_allq": _small_all_transfers(("betts8",), 0)}
+
+
+@pytest.mark.parametrize("wname,n_meas,max_batch", [("c1", 6, 4), ("sq2_allq", 5, 4), ("betts8_allq", 5, 4),
+                                                     ("c3", 9, 4), ("c3", 70, 72)])
 def test_tensor_core_disconnected_terms_match_oracle(oracle_lib, monkeypatch, wname, n_meas, max_batch):
     """The one-band PH update with its disconnected terms on tcgen05 (split BF16, FP32 accumulate)
     against the all-SIMT update and an FP64 reference: the oracle for c1, the FP64 GPU path (pinned
     to the oracle above) for c3.  (c3, 70, 72) takes two K chunks in the GEMM (batch padded to
     128); c1 (M = 64) pads the rows to one 128-row tile."""
-    case = case_from_workload(W.WORKLOADS[wname], n_meas)
+    case = case_from_workload(EXTRA_WORKLOADS.get(wname) or W.WORKLOADS[wname], n_meas)
     tc = _run_timed(case, False, monkeypatch, max_batch=max_batch)
     simt = _run_timed(case, True, monkeypatch, max_batch=max_batch)
     batches = -(-n_meas // max_batch)
     assert tc.stage_times()["update_g4"][1] == 3 * batches      # planes + GEMM + direct term
     assert simt.stage_times()["update_g4"][1] == batches
-    exact = run_oracle(oracle_lib, case) if wname == "c1" else run_gpu(case, precision=0, max_batch=1)
+    exact = run_oracle(oracle_lib, case) if wname != "c3" else run_gpu(case, precision=0, max_batch=1)
     for got, ref, want in zip(tc.get_G4(), simt.get_G4(), exact.get_G4()):
         print(wname, n_meas, "tensor-core / SIMT relative errors:", rel_err(got, want), rel_err(ref, want))
         assert rel_err(got, want) <= MIXED_TOL
