@@ -331,26 +331,27 @@ def run_ours(args, world, rank, local):
                 "traffic": None, "peak_source": peak_src}
     elif dom in ("col_transform", "row_transform") and os.environ.get("DCAACC_TP_SIMT_ONLY") != "1":
         # Tensor-core front-end.  Algorithmic flops: the complex contractions themselves,
-        # G = X' Q^H (8 D^2 n per sector) or X' = P M (4 D n^2, M real).  Split BF16 issues six
-        # BF16 products per such flop, so the roofline is the measured dense BF16 peak / 6; the
-        # issued MMA rate (padded K, six products) is reported beside it against the plain peak.
+        # G = X' Q^H (8 D^2 n per sector) or X' = P M (4 D n^2, M real).  The split-FP16 products
+        # cost three FP16 MMAs per such flop (two planes, three plane products), so the roofline
+        # is the measured dense BF16/FP16 peak / 3; the issued MMA rate (tiles of 128 x 128,
+        # K padded to 32) is reported beside it against the plain peak.
         ns = np.array([s.n for m in pool for s in m.sectors], dtype=np.float64)  # both halves
-        npad64 = np.ceil(ns / 64) * 64
-        npad128 = np.ceil(ns / 128) * 128
-        Dp, Dq = -(-D // 128) * 128, -(-D // 64) * 64
+        chunks = np.ceil(ns / 32)
+        Dp = -(-D // 128) * 128
         per_step = B / len(pool)  # pool holds two batches' measurements
+        mma_flop = 2.0 * 128 * 128 * 16
         if dom == "col_transform":
             alg = per_step * float(np.sum(8.0 * D * D * ns))
-            mma = per_step * float(np.sum(6 * 2.0 * Dp * (2 * Dq) * (2 * npad64)))
+            mma = per_step * float(np.sum((Dp // 128) ** 2 * chunks * 24 * mma_flop))
             kern = "frontGemmKernel<1> (column step, G = X' Q^H + beta G0 delta)"
         else:
             alg = per_step * float(np.sum(4.0 * D * ns * ns))
-            mma = per_step * float(np.sum(6 * 2.0 * (2 * Dp) * npad128 * npad64))
+            mma = per_step * float(np.sum((Dp // 128) * np.ceil(ns / 128) * chunks * 12 * mma_flop))
             kern = "frontGemmKernel<0> (row step, X' = P M)"
         sec = per_launch_ms / 1e3
-        roof = {"kernel": kern, "bound": "tensor", "achieved": alg / sec / 1e12, "peak": bf16_tf / 6,
+        roof = {"kernel": kern, "bound": "tensor", "achieved": alg / sec / 1e12, "peak": bf16_tf / 3,
                 "unit": "TFLOP/s", "traffic": None, "peak_source": peak_src,
-                "peak_note": "measured dense BF16 TFLOP/s / 6 (six BF16 products per split-BF16 flop)",
+                "peak_note": "measured dense BF16 TFLOP/s / 3 (three FP16 MMAs per split-FP16 flop)",
                 "mma_issued_tflops": mma / sec / 1e12, "mma_frac_of_bf16_peak": mma / sec / 1e12 / bf16_tf}
     else:
         # Front-end stages are dominated by their global traffic (M / X' / G, FP32 complex).

@@ -33,10 +33,25 @@ __device__ inline uint64_t smemDescSw128(const void* tile_base) {
   return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
+// K-major operand tile with 64-byte swizzle: rows of 32 FP16 / BF16 (64 bytes), 8-row atoms of 512 B
+// (the layout a TMA load with CU_TENSOR_MAP_SWIZZLE_64B writes).  Base 1024-byte aligned.
+__device__ inline uint64_t smemDescSw64(const void* tile_base) {
+  const uint64_t addr = smemAddr(tile_base);
+  return ((addr >> 4) & 0x3FFFull) | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
+}
+
+// Instruction descriptor bit that negates A (D += -A B^T).
+constexpr uint32_t kNegateA = 1u << 13;
+
 // Advance a descriptor's start address by `bytes` (a K step of 16 BF16 inside a swizzle atom is
 // 32 bytes; the swizzle is applied on absolute address bits, so this is exact for 1 KB-aligned atoms).
 __device__ inline uint64_t descAdvance(uint64_t desc, uint32_t bytes) {
   return desc + static_cast<uint64_t>(bytes >> 4);
+}
+
+// FP16 x FP16 -> FP32 (A and B formats 0).
+__host__ __device__ constexpr uint32_t instrDescF16F32(int M, int N) {
+  return (1u << 4) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
 }
 
 __host__ __device__ constexpr uint32_t instrDescBf16F32(int M, int N) {
@@ -69,7 +84,8 @@ __device__ inline void fenceAfterThreadSync() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// D[tmem] (+)= A[smem] * B[smem]^T, one thread issues.  accumulate = 0 overwrites D.
+// D[tmem] (+)= A[smem] * B[smem]^T, one thread issues (kind::f16: BF16 or FP16 operands, both
+// the same type, as the instruction descriptor says).  accumulate = 0 overwrites D.
 __device__ inline void mmaBf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
                                uint32_t accumulate) {
   asm volatile(

@@ -175,8 +175,9 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
       tc_front_ = true;
       const FrontTcShape fs = frontTcShape(dims_, int(n_sec), max_order_);
       ftc_mem_.alloc(frontTcBytes(fs));
-      DCAACC_CUDA_CHECK(cudaMemset(ftc_mem_.get(), 0, ftc_mem_.bytes()));  // padding rows stay zero
-      frontTcInit(ftc_, fs, ftc_mem_.get());
+      // Padding rows stay zero; ordered before the scale kernel frontTcInit launches on stream_.
+      DCAACC_CUDA_CHECK(cudaMemsetAsync(ftc_mem_.get(), 0, ftc_mem_.bytes(), stream_));
+      frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
       orb_r_d_.alloc(n_vtx);
       orb_c_d_.alloc(n_vtx);
       if (singlebandBatchedApplies(dims_))

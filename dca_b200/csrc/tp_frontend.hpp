@@ -44,10 +44,10 @@ size_t frontendSmemRequirement(const TpDims& d, int n_max, bool fp64);
 struct FrontTcShape {
   int D;    // R * NwExt, rows and columns of G
   int Dp;   // D rounded up to 128 (GEMM row tiles)
-  int Dq;   // D rounded up to 64 (complex column tiles)
-  int Kr;   // max_order rounded up to 64 (vertex extent of every plane row)
+  int Dq;   // D rounded up to 128 (GEMM complex column tiles)
+  int Kr;   // max_order rounded up to 64 (vertex extent of each real / imaginary half of a plane row)
   int n_sectors;
-  size_t pr_elems, mb_elems, ac_elems, bq_elems;  // BF16 elements of P, M, X' and Q planes
+  size_t pr_elems, mb_elems, ac_elems, bq_elems;  // FP16 elements of P, M, X' and Q planes
 };
 struct FrontTcWorkspace {
   FrontTcShape shape;
@@ -55,12 +55,19 @@ struct FrontTcWorkspace {
   void* mb = nullptr;
   void* ac = nullptr;
   void* bq = nullptr;
+  int* eP = nullptr;       // [spin][Dp] power-of-two exponents of P's rows
+  int* eQ = nullptr;       // [spin][Dp] ... of Q's rows
+  float* mInv = nullptr;   // [sector][Kr] inverse scales of M's rows j
+  float* xInv = nullptr;   // [sector][Dp][Kr / 32] inverse scales of X' row chunks
+  int n_sm = 0;            // SMs of the device (persistent GEMM grids)
   CUtensorMap tm_pr, tm_mb, tm_ac, tm_bq;  // TMA descriptors of the four plane arrays
 };
 FrontTcShape frontTcShape(const TpDims& d, int n_sectors, int max_order);
 size_t frontTcBytes(const FrontTcShape& s);
-// Carves `mem` (frontTcBytes, zero-filled by the caller) and encodes the tensor maps.
-void frontTcInit(FrontTcWorkspace& w, const FrontTcShape& s, void* mem);
+// Carves `mem` (frontTcBytes, zero-filled by the caller), encodes the tensor maps and computes the
+// P / Q row scales from the device G0 slice (one launch on `stream`).
+void frontTcInit(FrontTcWorkspace& w, const FrontTcShape& s, void* mem, const TpDims& d, const double2* G0,
+                 cudaStream_t stream);
 // Twiddles in (w, vertex) order into a.Tr / a.Tc and the P, M and Q planes; returns the number of
 // kernels launched.  orb_r / orb_c: orbital (band + nb site) of each vertex in row / column order.
 int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const int* orb_r, const int* orb_c,

@@ -9,30 +9,49 @@
 // vertices i in row-sorted order and the column vertices j in column-sorted order:
 //   P(rho1, i) = G0_s(b1, b_i; k1, w1) e^{i k1 (x_i + a_{b_i})} e^{i w1 tau_i}
 //   Q(rho2, j) = -(1/Nc) e^{i k2 (x_j + a_{b_j})} e^{i w2 tau_j} conj(G0_s(b_j, b2; k2, w2))
-//   X' = P M          (row step,    real GEMM [Pr; Pi] x M)
-//   G  = X' Q^H + beta G0_s(b1, b2; k1, w1) delta_{k1 k2} delta_{w1 w2}
-//                     (column step, real GEMM [X'r | X'i] x rows [Qr | Qi] and [-Qi | Qr])
+//   X' = P M          (row step)
+//   G  = X' Q^H + beta G0_s(b1, b2; k1, w1) delta_{k1 k2} delta_{w1 w2}     (column step)
 // where x_i, b_i are vertex i's site and band.  This is the reference's G exactly (the band sums
 // of -G0 G~ G0 become the G0 factors inside P and Q).
 //
-// Precision: every operand is split into three BF16 planes (x = hi + mid + lo to 2^-24), and the
-// six plane products above 2^-24 (lh, mm, hl, mh, hm, hh, smallest first) are accumulated in FP32
-// tensor memory.  The tensor core's accumulation does not round to nearest and its error grows with
-// the number of MMAs that feed one accumulator, and the diagonal blocks of G are coherent sums over
-// the vertices; so each 64-wide K chunk goes to a fresh pair of accumulators, which the epilogue
-// warps read and add into FP32 registers in round-to-nearest while the next chunk runs
-// (double-buffered tensor memory: 2 chunks x 2 accumulators x 128 columns = all 512 columns).
+// Precision.  Every operand is split into two FP16 planes, x ~ hi + lo (22 significant bits), and
+// the three plane products lo*hi, hi*lo, hi*hi are accumulated in FP32 tensor memory (the dropped
+// lo*lo is below 2^-22).  FP16's exponent range is handled with exact power-of-two scales chosen so
+// that the largest magnitude of each scaled row (or row chunk) lies in [2^13, 2^15): then nothing
+// overflows, and every entry down to 2^-17 of that maximum keeps a normal lo part.  P and Q rows
+// are scaled by a bound from |G0| (which fixes the magnitude of every entry); M columns by their
+// maximum; X' per (row, 32-wide K chunk, real and imaginary parts together) by the maximum the row
+// step's epilogue sees, and the column step undoes that scale chunk by chunk.  Against the FP64 G,
+// the split's own error is about 3e-8 relative (Frobenius) on the 4x4-cluster workload, the same
+// order as rounding G to FP32; the FP32 accumulation that follows dominates.  The tensor core's
+// FP32 accumulation does not round to nearest and its error grows with the number of MMAs that
+// feed one accumulator, and the diagonal blocks of G are coherent sums over the vertices; so every
+// 32-wide K chunk goes to a fresh accumulator pair (small products first), which the epilogue
+// warps read and add into FP32 registers in round-to-nearest while the next chunk runs.
 //
-// GEMM kernel: CTA = 128 rows x 128 real columns, 320 threads, one CTA per SM (shared memory).
-//   warp 0      TMA producer: per K chunk, 3 A planes + 3 B planes (64 x 128 boxes, 128-byte
-//               swizzle) into one of two shared-memory stages;
-//   warp 1      allocates tensor memory; one thread issues the 24 MMAs of a chunk and commits
-//               them to the stage's "empty" barrier and the accumulator pair's "full" barrier;
-//   warps 2-9   promote each finished accumulator pair into registers, then run the epilogue
-//               (row step: split X' into the column step's planes; column step: store G).
+// Both steps are complex-pair GEMMs.  A stage holds one 32-wide K chunk of the real and the
+// imaginary part of A (and of B in the column step), 2 FP16 planes each, as 64-byte-swizzled
+// 128-row tiles; per 16-wide K step and plane product the MMAs are
+//   row step:    Re += Ar Mt,   Im += Ai Mt                         (M real)
+//   column step: Re += Ar Br^T + Ai Bi^T,  Im += Ai Br^T - Ar Bi^T  (negate-A for the last)
+// into 128 x 128 FP32 accumulators Re and Im (columns 0-127 and 128-255 of a 256-column buffer;
+// two buffers, chunk parity, = all 512 tensor-memory columns).  So the column step's B operand is
+// Q itself, not the doubled real form [Qr | Qi; -Qi | Qr], and each staged byte feeds twice the
+// MMAs of a real-form 128 x 64-complex tile.
+//
+// GEMM kernel: persistent, one CTA per SM (shared memory), 576 threads (18 warps: five share one
+// SM sub-partition's 16K registers, so at most 96 registers per thread), tiles of 128 rows x 128
+// (complex) columns taken round-robin over (sector, row tile, column tile).
+//   warp 0      TMA producer: 3-stage ring over the chunks of all of the CTA's tiles;
+//   warp 1      allocates tensor memory; one thread issues a chunk's MMAs and commits them to the
+//               stage's "empty" barrier and the accumulator buffer's "full" barrier;
+//   warps 2-17  promote each finished accumulator buffer into registers (warp w: lanes
+//               32 (w % 4) .. + 31, complex columns 32 ((w - 2) / 4) .. + 31), then run the tile's
+//               epilogue while the next tile's chunks load and multiply (row step: rescale and
+//               split X' into the column step's planes; column step: unscale and store G).
 // Every wait is bounded (kWaitLimit polls, then the error word is set and the roles stop).
 #include <cuda.h>
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,15 +67,22 @@ namespace dcaacc {
 
 namespace {
 
-constexpr int kPl = 3;                                  // BF16 planes per operand
-constexpr int kBM = 128;                                // rows per CTA
-constexpr int kBN = 128;                                // real accumulator columns per CTA
-constexpr int kBK = 64;                                 // K per stage: one 128-byte swizzle atom
-constexpr uint32_t kTileBytes = kBM * kBK * 2;          // one plane of A or B: 16 KB
-constexpr uint32_t kStageBytes = 2 * kPl * kTileBytes;  // 96 KB
-constexpr int kStages = 2;
-constexpr size_t kGemmSmem = 1024 + kStages * kStageBytes + 128;
-constexpr int kGemmThreads = 320;
+constexpr int kPl = 2;                            // FP16 planes per operand
+constexpr int kBM = 128;                          // rows per tile
+constexpr int kBN = 128;                          // (complex) columns per tile
+constexpr int kBK = 32;                           // K per chunk: one 64-byte swizzle row
+constexpr uint32_t kBox = kBM * kBK * 2;          // one 128 x 32 FP16 box: 8 KB
+constexpr uint32_t kStageStride = 4 * kPl * kBox; // A re, A im, B re, B im (x planes): 64 KB
+constexpr int kStages = 3;
+constexpr size_t kGemmSmem = 1024 + kStages * kStageStride + 256;
+constexpr int kEpiWarps = 16;
+constexpr int kGemmThreads = 32 * (2 + kEpiWarps);  // 576
+constexpr int kScaleTop = 14;  // scaled maxima land in [2^14, 2^15) (one binade lower for bounds)
+
+// Offsets inside a stage.
+__host__ __device__ constexpr uint32_t boxOff(int part, int plane) {
+  return static_cast<uint32_t>(part * kPl + plane) * kBox;  // part: 0 A re, 1 A im, 2 B re, 3 B im
+}
 
 // Matsubara frequency of extended index w (vertex_frequency_domain.hpp, EXTENDED).
 __device__ inline double extFreq(int w, int nw_ext, double beta) {
@@ -66,34 +92,62 @@ __device__ inline double extFreq(int w, int nw_ext, double beta) {
   return -M_PI / beta * (1 + 2 * (half - 1 - w));
 }
 
-struct Split3d {
-  __nv_bfloat16 h, m, l;
-};
-// x = h + m + l to about 2^-24 |x|, each part rounded to nearest from the exact remainder.
-__device__ inline Split3d split3d(double x) {
-  const __nv_bfloat16 h = __double2bfloat16(x);
-  const double r1 = x - static_cast<double>(__bfloat162float(h));
-  const __nv_bfloat16 m = __double2bfloat16(r1);
-  const double r2 = r1 - static_cast<double>(__bfloat162float(m));
-  return {h, m, __double2bfloat16(r2)};
+// Exponent e with mx * 2^e in [2^14, 2^15) (0 for mx = 0).
+__device__ inline int scaleExp(double mx) {
+  return mx > 0 ? kScaleTop - ilogb(mx) : 0;
 }
-__device__ inline Split3d split3f(float x) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(x);
-  const float r1 = x - __bfloat162float(h);
-  const __nv_bfloat16 m = __float2bfloat16_rn(r1);
-  const float r2 = r1 - __bfloat162float(m);
-  return {h, m, __float2bfloat16_rn(r2)};
+
+struct Split2 {
+  __half h, l;
+};
+// x * 2^e = h + l with |x 2^e - h - l| <= 2^-22 |x 2^e| (both parts rounded to nearest).
+__device__ inline Split2 split2d(double x, int e) {
+  const double y = ldexp(x, e);
+  const __half h = __double2half(y);
+  return {h, __double2half(y - static_cast<double>(__half2float(h)))};
+}
+__device__ inline Split2 split2f(float x, int e) {
+  const float y = ldexpf(x, e);
+  const __half h = __float2half_rn(y);
+  return {h, __float2half_rn(y - __half2float(h))};
 }
 
 struct Pack8 {
-  __nv_bfloat16 v[8];
+  __half v[8];
 };
-__device__ inline void store8(__nv_bfloat16* dst, const Pack8& p) {
+__device__ inline void store8(__half* dst, const Pack8& p) {
   *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(&p);
 }
 
 __device__ inline double2 zmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Row scales of P and Q per (spin, rho) from |G0|: P row rho1 holds G0_s(b1, b; k1, w1) times unit
+// phases, Q row rho2 holds G0_s(b, b2; k2, w2) / Nc.  Stored as exponents; rows >= D get 0.
+__global__ void operandScalesKernel(const TpDims dims, const double2* __restrict__ G0, int D, int Dp,
+                                    int* __restrict__ eP, int* __restrict__ eQ) {
+  const int nb = dims.nb, nc = dims.nc, R = dims.R, nw_ext = dims.nw_ext;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < 2 * Dp; idx += gridDim.x * blockDim.x) {
+    const int s = idx / Dp, rho = idx % Dp;
+    int ep = 0, eq = 0;
+    if (rho < D) {
+      const int r = rho % R, w = rho / R, b = r % nb, k = r / nb;
+      const double2* g0s = G0 + static_cast<long>(s) * nw_ext * nc * nb * nb;
+      double mp = 0, mq = 0;
+      for (int c = 0; c < nb; ++c) {
+        const double2 gp = g0s[b + nb * (c + nb * (k + nc * w))];
+        const double2 gq = g0s[c + nb * (b + nb * (k + nc * w))];
+        mp = fmax(mp, hypot(gp.x, gp.y));
+        mq = fmax(mq, hypot(gq.x, gq.y));
+      }
+      // hypot and the phase products round; one binade of margin keeps the maxima below 2^15.
+      ep = scaleExp(mp) - 1;
+      eq = scaleExp(mq / nc) - 1;
+    }
+    eP[idx] = ep;
+    eQ[idx] = eq;
+  }
 }
 
 // T(w, i) = e^{i w tau_{perm[i]}}, per sector in (w, i) order: T[vtx_off * NwExt + w * n + i].
@@ -113,166 +167,158 @@ __global__ void twiddleWiKernel(const SectorDesc* __restrict__ sectors, const do
   }
 }
 
-// Row operand P, planes [sector][plane][2 Dp rows][Kr]: rows 0..Dp-1 real part, Dp..2Dp-1
-// imaginary part; columns i < roundup(n, 64) (zero for i >= n).  One thread per (rho, 8 columns).
+// Phase operand (P for the rows, Q for the columns), planes [sector][plane][rows][2 Kr]: real part
+// at column v, imaginary part at column Kr + v, for vertices v < roundup(n, 32) (zero for v >= n);
+// rows rho < D.  One thread per (rho, 8 vertices).
+//   ROW = true:  P(rho, i) 2^eP  = G0_s(b1, b_i; k1, w) Fb(b_i, k1, x_i) T(w, i) 2^eP
+//   ROW = false: Q(rho, j) 2^eQ  = -(1/Nc) Fb(b_j, k2, x_j) T(w, j) conj(G0_s(b_j, b2; k2, w)) 2^eQ
+template <bool ROW>
 __global__ void __launch_bounds__(256)
-buildRowOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, const double2* __restrict__ T,
-                      const int* __restrict__ orb, const double2* __restrict__ Fb, const double2* __restrict__ G0,
-                      int D, int Dp, int Kr, __nv_bfloat16* __restrict__ out) {
-  const SectorDesc sd = sectors[blockIdx.y];
-  const int n = sd.n;
-  const int groups = (n + kBK - 1) / kBK * (kBK / 8);
-  const int nb = dims.nb, nc = dims.nc, R = dims.R, nw_ext = dims.nw_ext;
-  const long plane = 2L * Dp * Kr;
-  __nv_bfloat16* o = out + static_cast<long>(blockIdx.y) * kPl * plane;
-  const double2* g0s = G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
-  const double2* Ts = T + static_cast<long>(sd.vtx_off) * nw_ext;
-  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * D;
-       idx += long(gridDim.x) * blockDim.x) {
-    const int grp = static_cast<int>(idx % groups);
-    const int rho = static_cast<int>(idx / groups);
-    const int r = rho % R, w = rho / R, b1 = r % nb, k1 = r / nb;
-    Pack8 re[kPl], im[kPl];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int i = grp * 8 + e;
-      double2 v = make_double2(0., 0.);
-      if (i < n) {
-        const int oi = orb[sd.vtx_off + i];
-        const int bi = oi % nb, xi = oi / nb;
-        v = zmul(zmul(g0s[b1 + nb * (bi + nb * (k1 + nc * w))], Fb[(bi * nc + k1) * nc + xi]),
-                 Ts[static_cast<long>(w) * n + i]);
-      }
-      const Split3d a = split3d(v.x), b = split3d(v.y);
-      re[0].v[e] = a.h, re[1].v[e] = a.m, re[2].v[e] = a.l;
-      im[0].v[e] = b.h, im[1].v[e] = b.m, im[2].v[e] = b.l;
-    }
-#pragma unroll
-    for (int pl = 0; pl < kPl; ++pl) {
-      store8(o + pl * plane + static_cast<long>(rho) * Kr + grp * 8, re[pl]);
-      store8(o + pl * plane + static_cast<long>(Dp + rho) * Kr + grp * 8, im[pl]);
-    }
-  }
-}
-
-// M operand, planes [sector][plane][Kr rows j][Kr columns i]: M(perm_r[i], perm_c[j]) for
-// i, j < n, zero up to i < roundup(n, 64) and j < min(roundup(n, 128), Kr).
-__global__ void __launch_bounds__(256)
-buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restrict__ perm_r,
-                    const int* __restrict__ perm_c, int Kr, __nv_bfloat16* __restrict__ out) {
-  const SectorDesc sd = sectors[blockIdx.y];
-  const int n = sd.n;
-  const int groups = (n + kBK - 1) / kBK * (kBK / 8);
-  const int rows = min((n + kBN - 1) / kBN * kBN, Kr);
-  const long plane = static_cast<long>(Kr) * Kr;
-  __nv_bfloat16* o = out + static_cast<long>(blockIdx.y) * kPl * plane;
-  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * rows;
-       idx += long(gridDim.x) * blockDim.x) {
-    const int grp = static_cast<int>(idx % groups);
-    const int j = static_cast<int>(idx / groups);
-    const double* col = j < n ? sd.M + static_cast<long>(sd.ldm) * perm_c[sd.vtx_off + j] : nullptr;
-    Pack8 v[kPl];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int i = grp * 8 + e;
-      const double m = (col && i < n) ? col[perm_r[sd.vtx_off + i]] : 0.;
-      const Split3d s = split3d(m);
-      v[0].v[e] = s.h, v[1].v[e] = s.m, v[2].v[e] = s.l;
-    }
-#pragma unroll
-    for (int pl = 0; pl < kPl; ++pl)
-      store8(o + pl * plane + static_cast<long>(j) * Kr + grp * 8, v[pl]);
-  }
-}
-
-// Column operand Q, planes [sector][plane][2 Dq rows][2 Kr]: for rho2 = 64 cb + c, row 128 cb + c
-// holds [Qr | Qi] and row 128 cb + 64 + c holds [-Qi | Qr] (imaginary parts at column Kr + j).
-__global__ void __launch_bounds__(256)
-buildColOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, const double2* __restrict__ T,
-                      const int* __restrict__ orb, const double2* __restrict__ Fb, const double2* __restrict__ G0,
-                      int D, int Dq, int Kr, __nv_bfloat16* __restrict__ out) {
+buildPhaseOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, const double2* __restrict__ T,
+                        const int* __restrict__ orb, const double2* __restrict__ Fb, const double2* __restrict__ G0,
+                        const int* __restrict__ eRow, int D, int Dp, int rows, int Kr, __half* __restrict__ out) {
   const SectorDesc sd = sectors[blockIdx.y];
   const int n = sd.n;
   const int groups = (n + kBK - 1) / kBK * (kBK / 8);
   const int nb = dims.nb, nc = dims.nc, R = dims.R, nw_ext = dims.nw_ext;
   const long kp = 2L * Kr;
-  const long plane = 2L * Dq * kp;
-  __nv_bfloat16* o = out + static_cast<long>(blockIdx.y) * kPl * plane;
+  const long plane = static_cast<long>(rows) * kp;
+  __half* o = out + static_cast<long>(blockIdx.y) * kPl * plane;
   const double2* g0s = G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
   const double2* Ts = T + static_cast<long>(sd.vtx_off) * nw_ext;
-  const double scale = -1.0 / nc;
+  const double qscale = -1.0 / nc;
   for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * D;
        idx += long(gridDim.x) * blockDim.x) {
     const int grp = static_cast<int>(idx % groups);
     const int rho = static_cast<int>(idx / groups);
-    const int r = rho % R, w = rho / R, b2 = r % nb, k2 = r / nb;
-    Pack8 qr[kPl], qi[kPl], mqi[kPl];
+    const int r = rho % R, w = rho / R, b = r % nb, k = r / nb;
+    const int e = eRow[sd.spin * Dp + rho];
+    Pack8 re[kPl], im[kPl];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int j = grp * 8 + e;
-      double2 v = make_double2(0., 0.);
-      if (j < n) {
-        const int oj = orb[sd.vtx_off + j];
-        const int bj = oj % nb, xj = oj / nb;
-        const double2 g = g0s[bj + nb * (b2 + nb * (k2 + nc * w))];
-        v = zmul(zmul(Fb[(bj * nc + k2) * nc + xj], Ts[static_cast<long>(w) * n + j]), make_double2(g.x, -g.y));
-        v.x *= scale;
-        v.y *= scale;
+    for (int x = 0; x < 8; ++x) {
+      const int v = grp * 8 + x;
+      double2 z = make_double2(0., 0.);
+      if (v < n) {
+        const int ov = orb[sd.vtx_off + v];
+        const int bv = ov % nb, xv = ov / nb;
+        const double2 ph = zmul(Fb[(bv * nc + k) * nc + xv], Ts[static_cast<long>(w) * n + v]);
+        if (ROW) {
+          z = zmul(g0s[b + nb * (bv + nb * (k + nc * w))], ph);
+        }
+        else {
+          const double2 g = g0s[bv + nb * (b + nb * (k + nc * w))];
+          z = zmul(ph, make_double2(g.x, -g.y));
+          z.x *= qscale;
+          z.y *= qscale;
+        }
       }
-      const Split3d a = split3d(v.x), b = split3d(v.y), c = split3d(-v.y);
-      qr[0].v[e] = a.h, qr[1].v[e] = a.m, qr[2].v[e] = a.l;
-      qi[0].v[e] = b.h, qi[1].v[e] = b.m, qi[2].v[e] = b.l;
-      mqi[0].v[e] = c.h, mqi[1].v[e] = c.m, mqi[2].v[e] = c.l;
+      const Split2 a = split2d(z.x, e), c = split2d(z.y, e);
+      re[0].v[x] = a.h, re[1].v[x] = a.l;
+      im[0].v[x] = c.h, im[1].v[x] = c.l;
     }
-    const long rre = static_cast<long>(rho / 64) * 128 + rho % 64, rim = rre + 64;
 #pragma unroll
     for (int pl = 0; pl < kPl; ++pl) {
-      __nv_bfloat16* op = o + pl * plane;
-      store8(op + rre * kp + grp * 8, qr[pl]);
-      store8(op + rre * kp + Kr + grp * 8, qi[pl]);
-      store8(op + rim * kp + grp * 8, mqi[pl]);
-      store8(op + rim * kp + Kr + grp * 8, qr[pl]);
+      __half* op = o + pl * plane + static_cast<long>(rho) * kp + grp * 8;
+      store8(op, re[pl]);
+      store8(op + Kr, im[pl]);
     }
+  }
+}
+
+// M operand, planes [sector][plane][Kr rows j][Kr columns i]: M(perm_r[i], perm_c[j]) * 2^{e_j}
+// for i, j < n, zero up to i < roundup(n, 32) and j < min(roundup(n, 128), Kr).  One warp per
+// row j: the first pass finds the row's maximum, the second writes the scaled planes; 2^{-e_j}
+// goes to mInv[sector][j].
+__global__ void __launch_bounds__(256)
+buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restrict__ perm_r,
+                    const int* __restrict__ perm_c, int Kr, __half* __restrict__ out, float* __restrict__ mInv) {
+  const SectorDesc sd = sectors[blockIdx.y];
+  const int n = sd.n;
+  const int groups = (n + kBK - 1) / kBK * (kBK / 8);
+  const int rows = min((n + kBN - 1) / kBN * kBN, Kr);
+  const long plane = static_cast<long>(Kr) * Kr;
+  __half* o = out + static_cast<long>(blockIdx.y) * kPl * plane;
+  const int lane = threadIdx.x % 32;
+  const int warps = gridDim.x * (blockDim.x / 32);
+  for (int j = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; j < rows; j += warps) {
+    const double* col = j < n ? sd.M + static_cast<long>(sd.ldm) * perm_c[sd.vtx_off + j] : nullptr;
+    double mx = 0;
+    if (col)
+      for (int i = lane; i < n; i += 32)
+        mx = fmax(mx, fabs(col[perm_r[sd.vtx_off + i]]));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    const int e = scaleExp(mx);
+    for (int grp = lane; grp < groups; grp += 32) {
+      Pack8 v[kPl];
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        const int i = grp * 8 + x;
+        const double m = (col && i < n) ? col[perm_r[sd.vtx_off + i]] : 0.;
+        const Split2 s = split2d(m, e);
+        v[0].v[x] = s.h, v[1].v[x] = s.l;
+      }
+#pragma unroll
+      for (int pl = 0; pl < kPl; ++pl)
+        store8(o + pl * plane + static_cast<long>(j) * Kr + grp * 8, v[pl]);
+    }
+    if (lane == 0)
+      mInv[static_cast<long>(blockIdx.y) * Kr + j] = ldexpf(1.f, -e);
   }
 }
 
 struct GemmParams {
   TpDims dims;
   const SectorDesc* sectors;
+  int n_sectors;
   int D, Dp, Kr;
-  __nv_bfloat16* ac;  // row step: X' planes out
-  float2* G;          // column step: G out
+  int mt, nt;           // row and column tiles per sector
+  const int* eP;        // [spin][Dp] row exponents of P
+  const int* eQ;        // [spin][Dp] row exponents of Q
+  const float* mInv;    // [sector][Kr] 2^-e of M's rows j (row step's output columns)
+  float* xInv;          // [sector][Dp][Kr / 32] 2^-e of each X' row chunk (real and imaginary)
+  __half* ac;           // row step: X' planes out
+  float2* G;            // column step: G out
   long g_sector_stride;
   const double2* G0;
   int* err;
 };
 
-// MODE 0: row step, A = P planes (2 Dp rows), B = M planes (rows j), output X' planes.
-// MODE 1: column step, A = X' planes (Dp rows), B = Q planes (interleaved rows), output G.
-// grid (A rows / 128, column tiles, n_sectors).
+// Tile t of the persistent schedule -> (sector, row tile, column tile, K chunks); chunks < 0 when
+// the tile has no work (row step: columns j beyond the sector's order).
+template <int MODE>
+__device__ inline void tileOf(const GemmParams& p, int t, int& sec, int& mt, int& nt, int& chunks) {
+  const int per = p.mt * p.nt;
+  sec = t / per;
+  const int rem = t % per;
+  mt = rem / p.nt;
+  nt = rem % p.nt;
+  const int n = p.sectors[sec].n;
+  chunks = (n + kBK - 1) / kBK;
+  if (MODE == 0 && nt * kBN >= n)
+    chunks = -1;
+}
+
+// MODE 0: row step, A = P planes, B = M planes (rows j), output X' planes and their chunk scales.
+// MODE 1: column step, A = X' planes, B = Q planes, output G.
 template <int MODE>
 __global__ void __launch_bounds__(kGemmThreads, 1)
 frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const GemmParams p) {
-  const int sec = blockIdx.z;
-  const SectorDesc sd = p.sectors[sec];
-  const int n = sd.n;
-  const int m0 = blockIdx.x * kBM;
-  const int nt = blockIdx.y;
-  const int nc1 = (n + kBK - 1) / kBK;  // K chunks over the vertices
-  if (MODE == 0 && nt * kBN >= n)
-    return;  // whole CTA: no columns j of this sector in this tile
-  const int n_chunks = MODE == 0 ? nc1 : 2 * nc1;
+  constexpr uint32_t stage_bytes = (MODE == 0 ? 3 : 4) * kPl * kBox;
+  const int n_tiles = p.n_sectors * p.mt * p.nt;
+  const int kxc = p.Kr / kBK;  // X' row chunks (scale table stride)
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * kStageBytes);
-  uint64_t* full = bars;          // [kStages] TMA -> MMA
-  uint64_t* empty = bars + 2;     // [kStages] MMA -> TMA
-  uint64_t* acc_full = bars + 4;  // [2] MMA -> epilogue
-  uint64_t* acc_empty = bars + 6; // [2] epilogue -> MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * kStageStride);
+  uint64_t* full = bars;                     // [kStages] TMA -> MMA
+  uint64_t* empty = bars + kStages;          // [kStages] MMA -> TMA
+  uint64_t* acc_full = bars + 2 * kStages;   // [2] MMA -> epilogue
+  uint64_t* acc_empty = acc_full + 2;        // [2] epilogue -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
 
   const int t = threadIdx.x, warp = t / 32, lane = t % 32;
   int* err = p.err;
@@ -287,7 +333,7 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     }
     for (int b = 0; b < 2; ++b) {
       mbarInit(&acc_full[b], 1);
-      mbarInit(&acc_empty[b], 8);  // one arrival per epilogue warp
+      mbarInit(&acc_empty[b], kEpiWarps);  // one arrival per epilogue warp
     }
     fenceBarrierInit();
     tc::prefetchTensorMap(&tmA);
@@ -300,144 +346,198 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
   if (warp == 0) {
     if (lane == 0) {
-      int issued = 0;
-      for (int c = 0; c < n_chunks; ++c) {
-        const int s = c & 1;
-        if (c >= 2 && !mbarWait(&empty[s], ((c >> 1) - 1) & 1, err))
-          break;
-        const int kx = (MODE == 0 || c < nc1) ? c * kBK : p.Kr + (c - nc1) * kBK;
-        unsigned char* st = base + s * kStageBytes;
-        mbarArriveExpectTx(&full[s], kStageBytes);
+      int g = 0;  // chunks issued (global over the CTA's tiles)
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        int sec, mt, nt, chunks;
+        tileOf<MODE>(p, tile, sec, mt, nt, chunks);
+        for (int c = 0; c < chunks; ++c, ++g) {
+          const int s = g % kStages, use = g / kStages;
+          if (use > 0 && !mbarWait(&empty[s], (use - 1) & 1, err)) {
+            ok = false;
+            break;
+          }
+          unsigned char* st = base + s * kStageStride;
+          mbarArriveExpectTx(&full[s], stage_bytes);
+          const int xr = c * kBK, xi = p.Kr + c * kBK;
 #pragma unroll
-        for (int pl = 0; pl < kPl; ++pl)
-          tc::tmaLoad3d(st + pl * kTileBytes, &tmA, kx, m0, sec * kPl + pl, &full[s]);
-#pragma unroll
-        for (int pl = 0; pl < kPl; ++pl)
-          tc::tmaLoad3d(st + (kPl + pl) * kTileBytes, &tmB, kx, nt * kBN, sec * kPl + pl, &full[s]);
-        ++issued;
+          for (int pl = 0; pl < kPl; ++pl) {
+            const int z = sec * kPl + pl;
+            tc::tmaLoad3d(st + boxOff(0, pl), &tmA, xr, mt * kBM, z, &full[s]);
+            tc::tmaLoad3d(st + boxOff(1, pl), &tmA, xi, mt * kBM, z, &full[s]);
+            tc::tmaLoad3d(st + boxOff(2, pl), &tmB, xr, nt * kBN, z, &full[s]);
+            if (MODE == 1)
+              tc::tmaLoad3d(st + boxOff(3, pl), &tmB, xi, nt * kBN, z, &full[s]);
+          }
+        }
       }
       // Loads still in flight are waited for (bounded) before the CTA can exit; on the normal
       // path every issued stage has been consumed already.
-      for (int c = max(0, issued - 2); c < issued; ++c)
-        mbarWait(&full[c & 1], (c >> 1) & 1, err);
+      for (int c = max(0, g - kStages); c < g; ++c)
+        mbarWait(&full[c % kStages], (c / kStages) & 1, err);
     }
   }
   else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = tc::instrDescBf16F32(kBM, kBN);
-      // (A plane, B plane) pairs kept by the three-way split, smallest first.
-      const int pa[6] = {2, 1, 0, 1, 0, 0};
-      const int pb[6] = {0, 1, 2, 0, 1, 0};
-      for (int c = 0; c < n_chunks; ++c) {
-        const int s = c & 1, pb2 = c & 1;
-        if (!mbarWait(&full[s], (c >> 1) & 1, err))
-          break;
-        if (c >= 2 && !mbarWait(&acc_empty[pb2], ((c >> 1) - 1) & 1, err))
-          break;
-        tc::fenceAfterThreadSync();
-        unsigned char* st = base + s * kStageBytes;
-#pragma unroll
-        for (int pp = 0; pp < 6; ++pp) {
-          const uint64_t da = tc::smemDescSw128(st + pa[pp] * kTileBytes);
-          const uint64_t db = tc::smemDescSw128(st + (kPl + pb[pp]) * kTileBytes);
-#pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {
-            const uint32_t col = static_cast<uint32_t>(2 * pb2 + (kk >> 1)) * 128;
-            tc::mmaBf16(tmem + col, tc::descAdvance(da, kk * 32), tc::descAdvance(db, kk * 32), idesc,
-                        (pp | (kk & 1)) != 0);
+      constexpr uint32_t idesc = tc::instrDescF16F32(kBM, kBN);
+      // (A plane, B plane) products kept by the two-way split, smallest first: lo*hi, hi*lo, hi*hi.
+      const int pa[3] = {1, 0, 0};
+      const int pb[3] = {0, 1, 0};
+      int g = 0;
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        int sec, mt, nt, chunks;
+        tileOf<MODE>(p, tile, sec, mt, nt, chunks);
+        for (int c = 0; c < chunks; ++c, ++g) {
+          const int s = g % kStages, buf = g & 1;
+          if (!mbarWait(&full[s], (g / kStages) & 1, err) ||
+              (g >= 2 && !mbarWait(&acc_empty[buf], ((g >> 1) - 1) & 1, err))) {
+            ok = false;
+            break;
           }
+          tc::fenceAfterThreadSync();
+          unsigned char* st = base + s * kStageStride;
+          const uint32_t re = tmem + buf * 256, im = re + 128;
+#pragma unroll
+          for (int pp = 0; pp < 3; ++pp) {
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {  // 2 x K16 per 32-wide chunk: 32 bytes each
+              const uint32_t first = (pp | kk) != 0;
+              const uint64_t ar = tc::descAdvance(tc::smemDescSw64(st + boxOff(0, pa[pp])), kk * 32);
+              const uint64_t ai = tc::descAdvance(tc::smemDescSw64(st + boxOff(1, pa[pp])), kk * 32);
+              const uint64_t br = tc::descAdvance(tc::smemDescSw64(st + boxOff(2, pb[pp])), kk * 32);
+              if (MODE == 0) {
+                tc::mmaBf16(re, ar, br, idesc, first);
+                tc::mmaBf16(im, ai, br, idesc, first);
+              }
+              else {
+                const uint64_t bi = tc::descAdvance(tc::smemDescSw64(st + boxOff(3, pb[pp])), kk * 32);
+                tc::mmaBf16(re, ar, br, idesc, first);
+                tc::mmaBf16(re, ai, bi, idesc, 1);
+                tc::mmaBf16(im, ai, br, idesc, first);
+                tc::mmaBf16(im, ar, bi, idesc | tc::kNegateA, 1);
+              }
+            }
+          }
+          tc::commitTo(&empty[s]);
+          tc::commitTo(&acc_full[buf]);
         }
-        tc::commitTo(&empty[s]);
-        tc::commitTo(&acc_full[pb2]);
       }
     }
   }
   else {
-    // Epilogue warps 2..9: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (rows of the tile);
-    // warps 2-5 take the first half of this thread's columns, warps 6-9 the second half.
+    // Epilogue warps 2..17: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (rows of the tile)
+    // and complex columns 32 cg .. + 31, cg = (w - 2) / 4.
     const int quarter = warp & 3;
-    const int half = (warp - 2) >> 2;
+    const int cg = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = static_cast<uint32_t>(quarter * 32) << 16;
-    // MODE 0: acc[i] = column h*64 + i.  MODE 1: acc[i] = Re, acc[32 + i] = Im of complex
-    // column h*32 + i (tensor-memory columns h*32 + i and 64 + h*32 + i).
-    float acc[64];
-#pragma unroll
-    for (int i = 0; i < 64; ++i)
-      acc[i] = 0.f;
+    int g = 0;
     bool ok = true;
-    for (int c = 0; c < n_chunks; ++c) {
-      const int pb2 = c & 1;
-      ok = __all_sync(0xffffffffu, mbarWait(&acc_full[pb2], (c >> 1) & 1, err));
+    for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+      int sec, mt, nt, chunks;
+      tileOf<MODE>(p, tile, sec, mt, nt, chunks);
+      if (chunks < 0)
+        continue;
+      const SectorDesc sd = p.sectors[sec];
+      float ar[32], ai[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        ar[i] = ai[i] = 0.f;
+      const int rho = mt * kBM + row;
+      const float* xinv = p.xInv + (static_cast<long>(sec) * p.Dp + rho) * kxc;
+      for (int c = 0; c < chunks; ++c, ++g) {
+        const int buf = g & 1;
+        // Column step: the A rows of chunk c carry the scale 2^e of that X' row chunk; undo it.
+        const float f = MODE == 1 ? xinv[c] : 1.f;
+        ok = __all_sync(0xffffffffu, mbarWait(&acc_full[buf], (g >> 1) & 1, err));
+        if (!ok)
+          break;
+        tc::fenceAfterThreadSync();
+        const uint32_t col = tmem + lane_addr + buf * 256 + cg * 32;
+#pragma unroll
+        for (int piece = 0; piece < 2; ++piece) {
+          float v[16];
+          tc::ld32x32bx16(col + piece * 16, v);
+          tc::waitLd();
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            ar[piece * 16 + i] = fmaf(v[i], f, ar[piece * 16 + i]);
+          tc::ld32x32bx16(col + 128 + piece * 16, v);
+          tc::waitLd();
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            ai[piece * 16 + i] = fmaf(v[i], f, ai[piece * 16 + i]);
+        }
+        tc::fenceBeforeThreadSync();
+        __syncwarp();
+        if (lane == 0)
+          mbarArrive(&acc_empty[buf]);
+      }
       if (!ok)
         break;
-      tc::fenceAfterThreadSync();
-#pragma unroll
-      for (int part = 0; part < 2; ++part) {
-        const uint32_t col = MODE == 0 ? half * 64 + part * 32 : part * 64 + half * 32;
-        float v0[32], v1[32];
-        tc::ld32x32bx32(tmem + lane_addr + (2 * pb2) * 128 + col, v0);
-        tc::ld32x32bx32(tmem + lane_addr + (2 * pb2 + 1) * 128 + col, v1);
-        tc::waitLd();
-#pragma unroll
-        for (int i = 0; i < 32; ++i)
-          acc[part * 32 + i] += v0[i] + v1[i];
-      }
-      tc::fenceBeforeThreadSync();
-      __syncwarp();
-      if (lane == 0)
-        mbarArrive(&acc_empty[pb2]);
-    }
-    if (ok) {
       if (MODE == 0) {
-        // X'(rho', j) -> column-step planes: rho' < Dp real part at column j, else imaginary part
-        // of row rho' - Dp at column Kr + j; only j < roundup(n, 64) (the range the column step
-        // reads).
-        const int rho = m0 + row;
-        const int dst = rho < p.Dp ? rho : rho - p.Dp;
-        const int koff = rho < p.Dp ? 0 : p.Kr;
-        const int n_pad = nc1 * kBK;
-        const long kp = 2L * p.Kr;
-        const long plane = static_cast<long>(p.Dp) * kp;
-        __nv_bfloat16* o = p.ac + static_cast<long>(sec) * kPl * plane + static_cast<long>(dst) * kp + koff;
-#pragma unroll
-        for (int g = 0; g < 8; ++g) {
-          const int j0 = nt * kBN + half * 64 + g * 8;
-          if (j0 < n_pad) {
-            Pack8 hi, mid, lo;
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              const Split3d s = split3f(acc[g * 8 + e]);
-              hi.v[e] = s.h, mid.v[e] = s.m, lo.v[e] = s.l;
-            }
-            store8(o + j0, hi);
-            store8(o + plane + j0, mid);
-            store8(o + 2 * plane + j0, lo);
-          }
-        }
-      }
-      else {
-        const TpDims& d = p.dims;
-        const int rho1 = m0 + row;
-        if (rho1 < p.D) {
-          const int R = d.R, nb = d.nb, nc = d.nc, nw_ext = d.nw_ext;
-          const int r1 = rho1 % R, w1 = rho1 / R, b1 = r1 % nb, k1 = r1 / nb;
-          float2* gout = p.G + p.g_sector_stride * (2 * sd.slot + sd.spin);
-          const double2* g0s = p.G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
-          const float beta = static_cast<float>(d.beta);
+        // X'(rho, j) = acc 2^{-eP(rho)} 2^{-e_j}, j = 128 nt + 32 cg + i: one 32-wide K chunk of the
+        // column step (written only if that step reads it, j0 < roundup(n, 32)), stored scaled by
+        // 2^s from the chunk's maximum over real and imaginary parts.
+        const int j0 = nt * kBN + cg * 32;
+        if (j0 < chunks * kBK) {
+          const float pinv = ldexpf(1.f, -p.eP[sd.spin * p.Dp + rho]);
+          const float* minv = p.mInv + static_cast<long>(sec) * p.Kr + j0;
+          float mx = 0.f;
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
-            const int rho2 = nt * 64 + half * 32 + i;
-            if (rho2 < p.D) {
-              const int r2 = rho2 % R, w2 = rho2 / R;
-              float2 v = make_float2(acc[i], acc[32 + i]);
-              if (w2 == w1 && r2 / nb == k1) {
-                const double2 g = g0s[b1 + nb * (r2 % nb + nb * (k1 + nc * w1))];
-                v.x += beta * static_cast<float>(g.x);
-                v.y += beta * static_cast<float>(g.y);
-              }
-              gout[(static_cast<long>(w1) * nw_ext + w2) * R * R + static_cast<long>(r1) * R + r2] = v;
+            const float sc = pinv * minv[i];
+            ar[i] *= sc;
+            ai[i] *= sc;
+            mx = fmaxf(mx, fmaxf(fabsf(ar[i]), fabsf(ai[i])));
+          }
+          const int e = mx > 0.f ? kScaleTop - ilogbf(mx) : 0;
+          const long kp = 2L * p.Kr;
+          const long plane = static_cast<long>(p.Dp) * kp;
+          __half* o = p.ac + static_cast<long>(sec) * kPl * plane + static_cast<long>(rho) * kp + j0;
+#pragma unroll
+          for (int g8 = 0; g8 < 4; ++g8) {
+            Pack8 hr, lr, hi, li;
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+              const Split2 a = split2f(ar[g8 * 8 + x], e), b = split2f(ai[g8 * 8 + x], e);
+              hr.v[x] = a.h, lr.v[x] = a.l, hi.v[x] = b.h, li.v[x] = b.l;
             }
+            store8(o + g8 * 8, hr);
+            store8(o + plane + g8 * 8, lr);
+            store8(o + p.Kr + g8 * 8, hi);
+            store8(o + plane + p.Kr + g8 * 8, li);
+          }
+          p.xInv[(static_cast<long>(sec) * p.Dp + rho) * kxc + j0 / kBK] = ldexpf(1.f, -e);
+        }
+      }
+      else if (rho < p.D) {
+        const TpDims& d = p.dims;
+        const int R = d.R, nb = d.nb, nc = d.nc, nw_ext = d.nw_ext;
+        const int r1 = rho % R, w1 = rho / R, b1 = r1 % nb, k1 = r1 / nb;
+        float2* gout = p.G + p.g_sector_stride * (2 * sd.slot + sd.spin) + (static_cast<long>(w1) * nw_ext) * R * R +
+                       static_cast<long>(r1) * R;
+        const double2* g0s = p.G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
+        const int* eq = p.eQ + sd.spin * p.Dp;
+        const float beta = static_cast<float>(d.beta);
+        const int rho0 = nt * kBN + cg * 32;
+        int r2 = rho0 % R, w2 = rho0 / R;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          if (rho0 + i < p.D) {
+            const float qinv = ldexpf(1.f, -eq[rho0 + i]);
+            float2 v = make_float2(ar[i] * qinv, ai[i] * qinv);
+            if (w2 == w1 && r2 / nb == k1) {
+              const double2 g0 = g0s[b1 + nb * (r2 % nb + nb * (k1 + nc * w1))];
+              v.x += beta * static_cast<float>(g0.x);
+              v.y += beta * static_cast<float>(g0.y);
+            }
+            gout[static_cast<long>(w2) * R * R + r2] = v;
+          }
+          if (++r2 == R) {
+            r2 = 0;
+            ++w2;
           }
         }
       }
@@ -469,15 +569,15 @@ EncodeTiledFn encodeTiledFn() {
   return fn;
 }
 
-// BF16 planes [depth][rows][cols] (cols fastest), 64 x 128 x 1 boxes, 128-byte swizzle; rows or
+// FP16 planes [depth][rows][cols] (cols fastest), 32 x 128 x 1 boxes, 64-byte swizzle; rows or
 // columns beyond the extents read as zero.
 void makePlaneMap(CUtensorMap* map, void* base, long cols, long rows, long depth) {
   const cuuint64_t dims[3] = {cuuint64_t(cols), cuuint64_t(rows), cuuint64_t(depth)};
   const cuuint64_t strides[2] = {cuuint64_t(cols) * 2, cuuint64_t(cols) * rows * 2};
   const cuuint32_t box[3] = {kBK, kBM, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = encodeTiledFn()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
-                                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+  const CUresult r = encodeTiledFn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, base, dims, strides, box, estr,
+                                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
     throw Error(DCAACC_CUDA_ERR, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
@@ -487,38 +587,88 @@ unsigned gridX(long work) {
   return static_cast<unsigned>(std::max(1L, std::min(4096L, (work + 255) / 256)));
 }
 
+size_t align256(size_t b) {
+  return (b + 255) / 256 * 256;
+}
+
+GemmParams gemmParams(const FrontendArgs& a, const FrontTcWorkspace& w, int* err) {
+  const FrontTcShape& s = w.shape;
+  GemmParams p{};
+  p.dims = a.dims;
+  p.sectors = a.sectors;
+  p.n_sectors = a.n_sectors;
+  p.D = s.D;
+  p.Dp = s.Dp;
+  p.Kr = s.Kr;
+  p.eP = w.eP;
+  p.eQ = w.eQ;
+  p.mInv = w.mInv;
+  p.xInv = w.xInv;
+  p.ac = static_cast<__half*>(w.ac);
+  p.G0 = a.G0;
+  p.err = err;
+  return p;
+}
+
+template <int MODE>
+void launchGemm(const GemmParams& p, const CUtensorMap& ta, const CUtensorMap& tb, int n_sm, cudaStream_t stream) {
+  auto k = frontGemmKernel<MODE>;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGemmSmem)));
+  const long tiles = long(p.n_sectors) * p.mt * p.nt;
+  const unsigned grid = static_cast<unsigned>(std::max(1L, std::min<long>(tiles, n_sm)));
+  k<<<grid, kGemmThreads, kGemmSmem, stream>>>(ta, tb, p);
+  DCAACC_LAUNCH_CHECK();
+}
+
 }  // namespace
 
 FrontTcShape frontTcShape(const TpDims& d, int n_sectors, int max_order) {
   FrontTcShape s;
   s.D = d.R * d.nw_ext;
   s.Dp = (s.D + kBM - 1) / kBM * kBM;
-  s.Dq = (s.D + 63) / 64 * 64;
-  s.Kr = (std::max(max_order, 1) + kBK - 1) / kBK * kBK;
+  s.Dq = (s.D + kBN - 1) / kBN * kBN;
+  s.Kr = (std::max(max_order, 1) + 63) / 64 * 64;
   s.n_sectors = n_sectors;
-  s.pr_elems = size_t(n_sectors) * kPl * 2 * s.Dp * s.Kr;
+  s.pr_elems = size_t(n_sectors) * kPl * s.Dp * 2 * s.Kr;
   s.mb_elems = size_t(n_sectors) * kPl * s.Kr * s.Kr;
   s.ac_elems = size_t(n_sectors) * kPl * s.Dp * 2 * s.Kr;
-  s.bq_elems = size_t(n_sectors) * kPl * 2 * s.Dq * 2 * s.Kr;
+  s.bq_elems = size_t(n_sectors) * kPl * s.Dq * 2 * s.Kr;
   return s;
 }
 
 size_t frontTcBytes(const FrontTcShape& s) {
-  return (s.pr_elems + s.mb_elems + s.ac_elems + s.bq_elems) * sizeof(__nv_bfloat16);
+  const size_t planes = align256((s.pr_elems + s.mb_elems + s.ac_elems + s.bq_elems) * sizeof(__half));
+  const size_t scales = align256(2 * sizeof(int) * 2 * s.Dp) + align256(sizeof(float) * s.n_sectors * s.Kr) +
+                        align256(sizeof(float) * s.n_sectors * size_t(s.Dp) * (s.Kr / kBK));
+  return planes + scales;
 }
 
-void frontTcInit(FrontTcWorkspace& w, const FrontTcShape& s, void* mem) {
+void frontTcInit(FrontTcWorkspace& w, const FrontTcShape& s, void* mem, const TpDims& d, const double2* G0,
+                 cudaStream_t stream) {
   w.shape = s;
-  __nv_bfloat16* b = static_cast<__nv_bfloat16*>(mem);
-  w.pr = b;
-  w.mb = b + s.pr_elems;
-  w.ac = b + s.pr_elems + s.mb_elems;
-  w.bq = b + s.pr_elems + s.mb_elems + s.ac_elems;
+  unsigned char* b = static_cast<unsigned char*>(mem);
+  __half* h = reinterpret_cast<__half*>(b);
+  w.pr = h;
+  w.mb = h + s.pr_elems;
+  w.ac = h + s.pr_elems + s.mb_elems;
+  w.bq = h + s.pr_elems + s.mb_elems + s.ac_elems;
+  size_t off = align256((s.pr_elems + s.mb_elems + s.ac_elems + s.bq_elems) * sizeof(__half));
+  w.eP = reinterpret_cast<int*>(b + off);
+  w.eQ = w.eP + 2 * s.Dp;
+  off += align256(2 * sizeof(int) * 2 * s.Dp);
+  w.mInv = reinterpret_cast<float*>(b + off);
+  off += align256(sizeof(float) * s.n_sectors * s.Kr);
+  w.xInv = reinterpret_cast<float*>(b + off);
   const long depth = long(s.n_sectors) * kPl;
-  makePlaneMap(&w.tm_pr, w.pr, s.Kr, 2L * s.Dp, depth);
+  makePlaneMap(&w.tm_pr, w.pr, 2L * s.Kr, s.Dp, depth);
   makePlaneMap(&w.tm_mb, w.mb, s.Kr, s.Kr, depth);
   makePlaneMap(&w.tm_ac, w.ac, 2L * s.Kr, s.Dp, depth);
-  makePlaneMap(&w.tm_bq, w.bq, 2L * s.Kr, 2L * s.Dq, depth);
+  makePlaneMap(&w.tm_bq, w.bq, 2L * s.Kr, s.Dq, depth);
+  int dev = 0;
+  DCAACC_CUDA_CHECK(cudaGetDevice(&dev));
+  DCAACC_CUDA_CHECK(cudaDeviceGetAttribute(&w.n_sm, cudaDevAttrMultiProcessorCount, dev));
+  operandScalesKernel<<<gridX(2L * s.Dp), 256, 0, stream>>>(d, G0, s.D, s.Dp, w.eP, w.eQ);
+  DCAACC_LAUNCH_CHECK();
 }
 
 int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const int* orb_r, const int* orb_c,
@@ -539,15 +689,15 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
     ++launches;
   }
   const long groups = (a.n_max + kBK - 1) / kBK * (kBK / 8);
-  buildRowOperandKernel<<<dim3(gridX(groups * s.D), a.n_sectors), 256, 0, stream>>>(
-      d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, s.D, s.Dp, s.Kr, static_cast<__nv_bfloat16*>(w.pr));
+  buildPhaseOperandKernel<true><<<dim3(gridX(groups * s.D), a.n_sectors), 256, 0, stream>>>(
+      d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, s.D, s.Dp, s.Dp, s.Kr, static_cast<__half*>(w.pr));
   DCAACC_LAUNCH_CHECK();
   const long mrows = std::min<long>((a.n_max + kBN - 1) / kBN * kBN, s.Kr);
-  buildMOperandKernel<<<dim3(gridX(groups * mrows), a.n_sectors), 256, 0, stream>>>(a.sectors, a.perm_r,
-                                                                                    a.perm_c, s.Kr, static_cast<__nv_bfloat16*>(w.mb));
+  buildMOperandKernel<<<dim3(static_cast<unsigned>((mrows + 7) / 8), a.n_sectors), 256, 0, stream>>>(
+      a.sectors, a.perm_r, a.perm_c, s.Kr, static_cast<__half*>(w.mb), w.mInv);
   DCAACC_LAUNCH_CHECK();
-  buildColOperandKernel<<<dim3(gridX(groups * s.D), a.n_sectors), 256, 0, stream>>>(
-      d, a.sectors, a.Tc, orb_c, a.Fb, a.G0, s.D, s.Dq, s.Kr, static_cast<__nv_bfloat16*>(w.bq));
+  buildPhaseOperandKernel<false><<<dim3(gridX(groups * s.D), a.n_sectors), 256, 0, stream>>>(
+      d, a.sectors, a.Tc, orb_c, a.Fb, a.G0, w.eQ, s.D, s.Dp, s.Dq, s.Kr, static_cast<__half*>(w.bq));
   DCAACC_LAUNCH_CHECK();
   return launches + 3;
 }
@@ -556,40 +706,21 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
   const FrontTcShape& s = w.shape;
   if (a.n_max == 0)
     return;
-  GemmParams p{};
-  p.dims = a.dims;
-  p.sectors = a.sectors;
-  p.D = s.D;
-  p.Dp = s.Dp;
-  p.Kr = s.Kr;
-  p.ac = static_cast<__nv_bfloat16*>(w.ac);
-  p.G0 = a.G0;
-  p.err = err;
-  auto k = frontGemmKernel<0>;
-  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGemmSmem)));
-  const dim3 grid(2 * s.Dp / kBM, (a.n_max + kBN - 1) / kBN, a.n_sectors);
-  k<<<grid, kGemmThreads, kGemmSmem, stream>>>(w.tm_pr, w.tm_mb, p);
-  DCAACC_LAUNCH_CHECK();
+  GemmParams p = gemmParams(a, w, err);
+  p.mt = s.Dp / kBM;
+  p.nt = (a.n_max + kBN - 1) / kBN;
+  launchGemm<0>(p, w.tm_pr, w.tm_mb, w.n_sm, stream);
 }
 
 void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
                          int* err, cudaStream_t stream) {
   const FrontTcShape& s = w.shape;
-  GemmParams p{};
-  p.dims = a.dims;
-  p.sectors = a.sectors;
-  p.D = s.D;
-  p.Dp = s.Dp;
-  p.Kr = s.Kr;
+  GemmParams p = gemmParams(a, w, err);
   p.G = G;
   p.g_sector_stride = g_sector_stride;
-  p.G0 = a.G0;
-  p.err = err;
-  auto k = frontGemmKernel<1>;
-  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGemmSmem)));
-  const dim3 grid(s.Dp / kBM, s.Dq / 64, a.n_sectors);
-  k<<<grid, kGemmThreads, kGemmSmem, stream>>>(w.tm_ac, w.tm_bq, p);
-  DCAACC_LAUNCH_CHECK();
+  p.mt = s.Dp / kBM;
+  p.nt = s.Dq / kBN;
+  launchGemm<1>(p, w.tm_ac, w.tm_bq, w.n_sm, stream);
 }
 
 }  // namespace dcaacc
