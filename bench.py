@@ -240,8 +240,7 @@ def run_ours(args, world, rank, local):
 
     def step(i, M_src):
         base = (i % 2) * B
-        for j in range(base, base + B):
-            acc.accumulate(M_src[j], configs[j], signs[j])
+        acc.accumulate_batch(M_src[base:base + B], configs[base:base + B], signs[base:base + B])
         acc.flush()
 
     for i in range(args.warmup):

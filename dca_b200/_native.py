@@ -67,13 +67,15 @@ class SpConfig(ctypes.Structure):
 
 
 class Sector(ctypes.Structure):
+    """dcaacc_sector; the pointer fields are declared void* (same ABI) so that addresses can be
+    assigned as integers without building ctypes pointer objects per call."""
     _fields_ = [
         ("n", c_int32),
-        ("tau", POINTER(c_double)),
-        ("left_band", POINTER(c_int32)),
-        ("right_band", POINTER(c_int32)),
-        ("left_site", POINTER(c_int32)),
-        ("right_site", POINTER(c_int32)),
+        ("tau", c_void_p),          # const double*
+        ("left_band", c_void_p),    # const int32_t*
+        ("right_band", c_void_p),
+        ("left_site", c_void_p),
+        ("right_site", c_void_p),
         ("M", c_void_p),
         ("ldm", c_int32),
         ("m_on_device", c_int32),

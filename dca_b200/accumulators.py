@@ -100,37 +100,44 @@ class TpParameters:
         return (nb, nb, nb, nb, nc, nw, nc, nw, len(self.k_ex), len(self.w_ex))
 
 
-def _make_sectors(M_pair, configs, keep: list):
-    secs = (N.Sector * 2)()
-    for s in range(2):
-        c = configs[s]
-        n = int(np.asarray(c.tau).shape[0])
-        arrs = [np.ascontiguousarray(c.tau, np.float64)]
-        for name in ("left_band", "right_band", "left_site", "right_site"):
-            arrs.append(np.ascontiguousarray(getattr(c, name), np.int32))
-        keep.extend(arrs)
-        M = M_pair[s]
-        sec = secs[s]
-        sec.n = n
-        sec.tau = _dptr(arrs[0])
-        sec.left_band, sec.right_band, sec.left_site, sec.right_site = (_iptr(a) for a in arrs[1:])
-        if hasattr(M, "is_cuda") and M.is_cuda:
-            import torch
+def _addr(a: np.ndarray) -> int:
+    return a.__array_interface__["data"][0]
 
-            if M.dtype != torch.float64:
-                raise LogicError("device M must be float64")
-            if n and not (M.stride(0) == 1 and M.stride(1) >= max(n, 1)):
-                M = M.t().contiguous().t()  # column major
-            keep.append(M)
-            sec.M = ctypes.c_void_p(M.data_ptr())
-            sec.ldm = max(M.stride(1), 1) if n else 1
-            sec.m_on_device = 1
-        else:
-            Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
-            keep.append(Mh)
-            sec.M = ctypes.c_void_p(Mh.ctypes.data)
-            sec.ldm = max(n, 1)
-            sec.m_on_device = 0
+
+def _fill_sector(sec, M, c, keep: list):
+    tau = np.ascontiguousarray(c.tau, np.float64)
+    n = int(tau.shape[0])
+    bands_sites = [np.ascontiguousarray(getattr(c, name), np.int32)
+                   for name in ("left_band", "right_band", "left_site", "right_site")]
+    keep.append(tau)
+    keep.extend(bands_sites)
+    sec.n = n
+    sec.tau = _addr(tau)
+    sec.left_band, sec.right_band, sec.left_site, sec.right_site = (_addr(a) for a in bands_sites)
+    if hasattr(M, "is_cuda") and M.is_cuda:
+        import torch
+
+        if M.dtype != torch.float64:
+            raise LogicError("device M must be float64")
+        if n and not (M.stride(0) == 1 and M.stride(1) >= max(n, 1)):
+            M = M.t().contiguous().t()  # column major
+        keep.append(M)
+        sec.M = M.data_ptr()
+        sec.ldm = max(M.stride(1), 1) if n else 1
+        sec.m_on_device = 1
+    else:
+        Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
+        keep.append(Mh)
+        sec.M = _addr(Mh)
+        sec.ldm = max(n, 1)
+        sec.m_on_device = 0
+
+
+def _make_sectors(M_pair, configs, keep: list, count: int = 1):
+    """Sector descriptors for `count` measurements: M_pair / configs hold 2 * count entries."""
+    secs = (N.Sector * (2 * count))()
+    for s in range(2 * count):
+        _fill_sector(secs[s], M_pair[s], configs[s], keep)
     return secs
 
 
@@ -181,6 +188,20 @@ class TpAccumulator:
         flops = ctypes.c_double(0)
         _check(N.lib.dcaacc_tp_accumulate(self._h, secs, int(sign), ctypes.byref(flops)))
         self._last_inputs = keep  # device M must outlive the queued work
+        return flops.value
+
+    def accumulate_batch(self, Ms, configs, signs) -> float:
+        """Several measurements in one call (dcaacc_tp_accumulate_batch): Ms[m] and configs[m] are
+        measurement m's pairs, signs[m] its sign.  Same result as calling accumulate per
+        measurement."""
+        count = len(signs)
+        keep: list = []
+        secs = _make_sectors([M for pair in Ms for M in pair], [c for pair in configs for c in pair], keep,
+                             count)
+        sg = np.ascontiguousarray(signs, np.int32)
+        flops = ctypes.c_double(0)
+        _check(N.lib.dcaacc_tp_accumulate_batch(self._h, count, secs, _iptr(sg), ctypes.byref(flops)))
+        self._last_inputs = keep
         return flops.value
 
     def flush(self):

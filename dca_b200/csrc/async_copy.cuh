@@ -1,9 +1,12 @@
 // Bulk asynchronous global -> shared copies (the TMA unit's 1D "cp.async.bulk" path) completed
 // through shared-memory mbarriers, for sm_100a.  No cluster multicast is used anywhere.
 //
-// Every wait is bounded: after kWaitLimit polls the waiting thread records a timeout in the
-// kernel's error word and the kernel skips the rest of its work, so a wrong transaction count
-// can never hang the GPU; the host turns the error word into DCAACC_DEVICE_INDEX_ERR.
+// Every wait is bounded: after kWaitLimit polls (each may suspend the thread for up to
+// kWaitHintNs while the phase is incomplete) the waiting thread records a timeout in the kernel's
+// error word and the kernel skips the rest of its work, so a wrong transaction count can never
+// hang the GPU (worst case about kWaitLimit * kWaitHintNs = 2 s); the host turns the error word
+// into DCAACC_DEVICE_INDEX_ERR.  The suspend hint keeps waiting warps from spending issue slots on
+// polling.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -12,7 +15,8 @@
 
 namespace dcaacc {
 
-constexpr uint32_t kWaitLimit = 1u << 26;  // ~seconds of polling; reached only on a bug
+constexpr uint32_t kWaitLimit = 1u << 20;  // reached only on a bug
+constexpr uint32_t kWaitHintNs = 2000;     // suspend-time hint of one poll
 
 // Error word bits written by kernels (read back by the host after the launch).
 constexpr int kErrBarrierTimeout = 1;
@@ -58,10 +62,10 @@ __device__ inline bool mbarTryWait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smemAddr(bar)), "r"(parity)
+      : "r"(smemAddr(bar)), "r"(parity), "r"(kWaitHintNs)
       : "memory");
   return ok != 0;
 }

@@ -84,7 +84,8 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   DCAACC_CUDA_CHECK(cudaGetDevice(&device_));
   DCAACC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   own_stream_ = true;
-  DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&upload_done_, cudaEventDisableTiming));
+  for (auto& h : hstage_)
+    DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&h.uploaded, cudaEventDisableTiming));
 
   // ---- G0 slice over the extended mesh (tp_accumulator_base.hpp:210-221) ----
   {
@@ -188,16 +189,18 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
     X64_.alloc(x_elems);
     G64_.alloc(g_elems);
   }
-  sectors_h_.alloc(n_sec);
-  tau_h_.alloc(n_vtx);
-  perm_r_h_.alloc(n_vtx);
-  perm_c_h_.alloc(n_vtx);
-  rstart_h_.alloc(n_sec * n_orb1);
-  cstart_h_.alloc(n_sec * n_orb1);
-  signs_h_.alloc(max_batch_);
-  orb_r_h_.alloc(n_vtx);
-  orb_c_h_.alloc(n_vtx);
-  DCAACC_CUDA_CHECK(cudaEventRecord(upload_done_, stream_));
+  for (auto& h : hstage_) {
+    h.sectors.alloc(n_sec);
+    h.tau.alloc(n_vtx);
+    h.perm_r.alloc(n_vtx);
+    h.perm_c.alloc(n_vtx);
+    h.rstart.alloc(n_sec * n_orb1);
+    h.cstart.alloc(n_sec * n_orb1);
+    h.signs.alloc(max_batch_);
+    h.orb_r.alloc(n_vtx);
+    h.orb_c.alloc(n_vtx);
+    DCAACC_CUDA_CHECK(cudaEventRecord(h.uploaded, stream_));
+  }
 
   if (!tc_front_ && frontendSmemRequirement(dims_, max_order_, !mixed_) > 227 * 1024)
     invalid("max_order too large for the front-end's shared-memory tiles");
@@ -211,15 +214,17 @@ TpAccumulator::~TpAccumulator() {
     cudaEventDestroy(t.begin);
     cudaEventDestroy(t.end);
   }
-  if (upload_done_)
-    cudaEventDestroy(upload_done_);
+  for (auto& h : hstage_)
+    if (h.uploaded)
+      cudaEventDestroy(h.uploaded);
   if (own_stream_ && stream_)
     cudaStreamDestroy(stream_);
 }
 
 void TpAccumulator::reset() {
   // resetAccumulation: zero G4 and arm accumulate (tp_accumulator_gpu.hpp:285-296).
-  DCAACC_CUDA_CHECK(cudaEventSynchronize(upload_done_));
+  for (auto& h : hstage_)
+    DCAACC_CUDA_CHECK(cudaEventSynchronize(h.uploaded));
   slots_ = 0;
   vtx_used_ = 0;
   x_used_ = 0;
@@ -275,7 +280,7 @@ double TpAccumulator::flopEstimate(const dcaacc_sector* sec) const {
 
 void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
   if (slots_ == 0)
-    DCAACC_CUDA_CHECK(cudaEventSynchronize(upload_done_));  // staging buffers free again
+    DCAACC_CUDA_CHECK(cudaEventSynchronize(hs().uploaded));  // this staging set is free again
   const int slot = slots_;
   const int n_orb = dims_.n_orb;
   for (int s = 0; s < 2; ++s) {
@@ -304,21 +309,21 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
         perm[fill[o]++] = v;
       }
     };
-    sort_side(false, perm_r_h_.get() + vtx_off, rstart_h_.get() + orb_off);
+    sort_side(false, hs().perm_r.get() + vtx_off, hs().rstart.get() + orb_off);
     if (non_density_)
-      sort_side(true, perm_c_h_.get() + vtx_off, cstart_h_.get() + orb_off);
+      sort_side(true, hs().perm_c.get() + vtx_off, hs().cstart.get() + orb_off);
     else {
-      std::copy_n(perm_r_h_.get() + vtx_off, n, perm_c_h_.get() + vtx_off);
-      std::copy_n(rstart_h_.get() + orb_off, n_orb + 1, cstart_h_.get() + orb_off);
+      std::copy_n(hs().perm_r.get() + vtx_off, n, hs().perm_c.get() + vtx_off);
+      std::copy_n(hs().rstart.get() + orb_off, n_orb + 1, hs().cstart.get() + orb_off);
     }
     // Orbital of each sorted position (the tensor-core front-end's per-vertex phases).
     for (int o = 0; o < n_orb; ++o) {
-      const int* rs = rstart_h_.get() + orb_off;
-      const int* cs = cstart_h_.get() + orb_off;
-      std::fill(orb_r_h_.get() + vtx_off + rs[o], orb_r_h_.get() + vtx_off + rs[o + 1], o);
-      std::fill(orb_c_h_.get() + vtx_off + cs[o], orb_c_h_.get() + vtx_off + cs[o + 1], o);
+      const int* rs = hs().rstart.get() + orb_off;
+      const int* cs = hs().cstart.get() + orb_off;
+      std::fill(hs().orb_r.get() + vtx_off + rs[o], hs().orb_r.get() + vtx_off + rs[o + 1], o);
+      std::fill(hs().orb_c.get() + vtx_off + cs[o], hs().orb_c.get() + vtx_off + cs[o + 1], o);
     }
-    std::copy_n(x.tau, n, tau_h_.get() + vtx_off);
+    std::copy_n(x.tau, n, hs().tau.get() + vtx_off);
 
     const double* Mptr = x.M;
     int ldm = std::max(x.ldm, 1);
@@ -338,12 +343,12 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
     d.spin = s;
     d.slot = slot;
     d.x_off = x_used_;
-    sectors_h_[sidx] = d;
+    hs().sectors[sidx] = d;
     x_used_ += long(dims_.R) * n * dims_.nw_ext;
     vtx_used_ += n;
     n_max_batch_ = std::max(n_max_batch_, n);
   }
-  signs_h_[slot] = sign;
+  hs().signs[slot] = sign;
   ++slots_;
 }
 
@@ -356,18 +361,19 @@ void TpAccumulator::process() {
     if (bytes)
       DCAACC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
   };
-  h2d(sectors_d_.get(), sectors_h_.get(), sizeof(SectorDesc) * n_sec);
-  h2d(tau_d_.get(), tau_h_.get(), sizeof(double) * vtx_used_);
-  h2d(perm_r_d_.get(), perm_r_h_.get(), sizeof(int) * vtx_used_);
-  h2d(perm_c_d_.get(), perm_c_h_.get(), sizeof(int) * vtx_used_);
-  h2d(rstart_d_.get(), rstart_h_.get(), sizeof(int) * n_sec * n_orb1);
-  h2d(cstart_d_.get(), cstart_h_.get(), sizeof(int) * n_sec * n_orb1);
-  h2d(signs_d_.get(), signs_h_.get(), sizeof(int) * slots_);
+  h2d(sectors_d_.get(), hs().sectors.get(), sizeof(SectorDesc) * n_sec);
+  h2d(tau_d_.get(), hs().tau.get(), sizeof(double) * vtx_used_);
+  h2d(perm_r_d_.get(), hs().perm_r.get(), sizeof(int) * vtx_used_);
+  h2d(perm_c_d_.get(), hs().perm_c.get(), sizeof(int) * vtx_used_);
+  h2d(rstart_d_.get(), hs().rstart.get(), sizeof(int) * n_sec * n_orb1);
+  h2d(cstart_d_.get(), hs().cstart.get(), sizeof(int) * n_sec * n_orb1);
+  h2d(signs_d_.get(), hs().signs.get(), sizeof(int) * slots_);
   if (tc_front_) {
-    h2d(orb_r_d_.get(), orb_r_h_.get(), sizeof(int) * vtx_used_);
-    h2d(orb_c_d_.get(), (non_density_ ? orb_c_h_ : orb_r_h_).get(), sizeof(int) * vtx_used_);
+    h2d(orb_r_d_.get(), hs().orb_r.get(), sizeof(int) * vtx_used_);
+    h2d(orb_c_d_.get(), (non_density_ ? hs().orb_c : hs().orb_r).get(), sizeof(int) * vtx_used_);
   }
-  DCAACC_CUDA_CHECK(cudaEventRecord(upload_done_, stream_));
+  DCAACC_CUDA_CHECK(cudaEventRecord(hs().uploaded, stream_));
+  hset_ ^= 1;
 
   FrontendArgs fa{};
   fa.dims = dims_;

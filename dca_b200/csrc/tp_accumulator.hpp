@@ -138,7 +138,6 @@ private:
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
   bool own_stream_ = false;
-  cudaEvent_t upload_done_ = nullptr;
   DevBuf<double2> G0_, Fb_;
   DevBuf<int> k_add_d_, k_sub_d_, q_d_, wex_d_;
   std::vector<DevBuf<double2>> G4_;
@@ -158,10 +157,19 @@ private:
   DevBuf<unsigned char> ftc_mem_;
   FrontTcWorkspace ftc_{};
   DevBuf<int> orb_r_d_, orb_c_d_;
-  // Pinned staging of the batch being assembled.
-  PinBuf<SectorDesc> sectors_h_;
-  PinBuf<double> tau_h_;
-  PinBuf<int> perm_r_h_, perm_c_h_, rstart_h_, cstart_h_, signs_h_, orb_r_h_, orb_c_h_;
+  // Pinned staging of the batch being assembled, double-buffered: the host fills one set while the
+  // uploads from the other (queued behind the previous batch's kernels) are still pending.
+  struct HostStage {
+    PinBuf<SectorDesc> sectors;
+    PinBuf<double> tau;
+    PinBuf<int> perm_r, perm_c, rstart, cstart, signs, orb_r, orb_c;
+    cudaEvent_t uploaded = nullptr;  // the uploads from this set have completed
+  };
+  HostStage hstage_[2];
+  int hset_ = 0;  // set being filled
+  HostStage& hs() {
+    return hstage_[hset_];
+  }
 
   // Batch bookkeeping.
   int slots_ = 0;         // measurements staged

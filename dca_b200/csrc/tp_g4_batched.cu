@@ -378,23 +378,23 @@ updateG4SinglebandDirect(const TpDims dims, const float2* __restrict__ G, long g
 //   D(k1, k2 = k1 - d, q = l1 - k1) = sum_m sum_s alpha_sd(k1) beta_sd(l1),
 //   alpha_sd(k1) = -s_m/2 G_s(k1 w1; k1-d w2),   beta_sd(l1) = G_s(l1-d w2+x; l1 w1+x),
 // (the cluster momenta form a group, so k2 + q = l1 - d).  Thread (d, k1 block, l1 block) keeps a
-// (Nc/4) x (Nc/4) tile of complex sums in registers and, per measurement and spin, reads Nc/4
-// alphas and Nc/4 betas for (Nc/4)^2 complex FMAs (the other direct-term kernels read two values
-// per FMA).  Per measurement the staged G blocks are re-laid out into alpha / beta rows, d-major
-// with rows padded to Nc + 2 (16-byte aligned, few bank conflicts), with -s/2 folded into alpha.
-// The flush goes through a shared table so that lanes touch consecutive k1 of G4 and of `disc`.
-template <int NC>
-__global__ void __launch_bounds__(NC * 16)
+// TA x TB tile of complex sums in registers and, per measurement and spin, gathers its TA alphas
+// and TB betas straight from the staged G blocks (fixed shared-memory offsets, computed once) for
+// TA TB complex FMAs.  Measurements are staged eight deep (bulk copies); per-stage "empty"
+// barriers let the warps drift apart instead of meeting at a block barrier per measurement.  The flush goes through a shared table so that lanes touch consecutive k1
+// of G4 and of `disc`.
+template <int NC, int TA, int TB>
+__global__ void __launch_bounds__(NC * (NC / TA) * (NC / TB))
 updateG4SinglebandOuter(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
                         const int* __restrict__ signs, int n_slots, const int* __restrict__ k_sub,
                         const int* __restrict__ q_list, const int* __restrict__ wex_list,
                         const float2* __restrict__ disc, double2* const* __restrict__ G4, bool atomic,
                         int* __restrict__ err) {
   constexpr int BLK = NC * NC;
-  constexpr int TL = NC / 4;      // tile edge per thread
-  constexpr int NT = NC * 16;     // threads
-  constexpr int AR = NC + 2;      // padded alpha / beta row
-  constexpr int QP = NC + 1;      // padded row of the flush table
+  constexpr int NKB = NC / TA, NLB = NC / TB;
+  constexpr int NT = NC * NKB * NLB;  // threads
+  constexpr int QP = NC + 1;          // padded row of the flush table
+  constexpr int DEPTH = 8;            // staged measurements
   const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq;
   int w1, w2;
   tileOfIndex(blockIdx.x % (nw * nw), nw, w1, w2);
@@ -402,19 +402,22 @@ updateG4SinglebandOuter(const TpDims dims, const float2* __restrict__ G, long g_
   const int wex = wex_list[iwq];
   const int ext = dims.ext;
   const int t = threadIdx.x;
-  const int d = t / 16, k1_0 = ((t % 16) / 4) * TL, l1_0 = (t % 4) * TL;
+  const int d = t / (NKB * NLB), sub = t % (NKB * NLB);
+  const int k1_0 = (sub / NLB) * TA, l1_0 = (sub % NLB) * TB;
 
   const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
   const long b_A = (static_cast<long>(w1e) * nw_ext + w2e) * BLK;
   const long b_B = (static_cast<long>(w2x) * nw_ext + w1x) * BLK;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);       // [2]
-  int* ksub = reinterpret_cast<int*>(smem_raw + 16);           // [NC * NC]
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);      // [DEPTH] copies landed
+  uint64_t* empty = full + DEPTH;                               // [DEPTH] all warps done reading
+  int* ksub = reinterpret_cast<int*>(smem_raw + 16 * DEPTH);   // [NC * NC]
   int* qinv = ksub + BLK;                                      // [NC]
-  float2* region = reinterpret_cast<float2*>(smem_raw + 16 + 4 * (BLK + NC + 4));
-  float2* stage = region;                                      // [2][A0 B0 A1 B1][BLK]
-  float2* ab = stage + 2 * 4 * BLK;                            // [spin][alpha, beta][d][AR]
+  float2* region = reinterpret_cast<float2*>(smem_raw + 16 * DEPTH + 4 * (BLK + NC + 4));
+  static_assert((16 * DEPTH + 4 * (BLK + NC + 4)) % 16 == 0, "bulk-copy destinations need 16-byte alignment");
+  const int lane = t % 32;
+  float2* stage = region;                                      // [DEPTH][A0 B0 A1 B1][BLK]
   float2* T = region;                                          // flush table, after the batch loop
 
   for (int e = t; e < BLK; e += NT)
@@ -423,146 +426,201 @@ updateG4SinglebandOuter(const TpDims dims, const float2* __restrict__ G, long g_
     qinv[q_list[e]] = e;
 
   constexpr uint32_t blk_bytes = BLK * sizeof(float2);
-  auto issue = [&](int slot, int st) {
+  auto issue = [&](int slot) {
+    const int st = slot % DEPTH;
     float2* dst = stage + st * 4 * BLK;
-    mbarArriveExpectTx(&bar[st], 4 * blk_bytes);
+    mbarArriveExpectTx(&full[st], 4 * blk_bytes);
     const float2* src0 = G + g_sector_stride * (2 * slot);
     const float2* src1 = src0 + g_sector_stride;
-    bulkCopyG2S(dst + 0 * BLK, src0 + b_A, blk_bytes, &bar[st]);
-    bulkCopyG2S(dst + 1 * BLK, src0 + b_B, blk_bytes, &bar[st]);
-    bulkCopyG2S(dst + 2 * BLK, src1 + b_A, blk_bytes, &bar[st]);
-    bulkCopyG2S(dst + 3 * BLK, src1 + b_B, blk_bytes, &bar[st]);
+    bulkCopyG2S(dst + 0 * BLK, src0 + b_A, blk_bytes, &full[st]);
+    bulkCopyG2S(dst + 1 * BLK, src0 + b_B, blk_bytes, &full[st]);
+    bulkCopyG2S(dst + 2 * BLK, src1 + b_A, blk_bytes, &full[st]);
+    bulkCopyG2S(dst + 3 * BLK, src1 + b_B, blk_bytes, &full[st]);
   };
   if (t == 0) {
-    mbarInit(&bar[0], 1);
-    mbarInit(&bar[1], 1);
+    for (int s2 = 0; s2 < DEPTH; ++s2) {
+      mbarInit(&full[s2], 1);
+      mbarInit(&empty[s2], NT / 32);
+    }
     fenceBarrierInit();
   }
   __syncthreads();
-  if (t == 0) {
-    issue(0, 0);
-    if (n_slots > 1)
-      issue(1, 1);
-  }
+  if (t == 0)
+    for (int m = 0; m < DEPTH && m < n_slots; ++m)
+      issue(m);
 
-  float2 acc[TL][TL];
+  // Fixed gather offsets inside a staged block: alpha from A (row k1, column k1 - d), beta from B
+  // (row l1 - d, column l1).
+  int oa[TA], ob[TB];
 #pragma unroll
-  for (int a = 0; a < TL; ++a)
+  for (int a = 0; a < TA; ++a)
+    oa[a] = (k1_0 + a) * NC + ksub[d + NC * (k1_0 + a)];
 #pragma unroll
-    for (int b = 0; b < TL; ++b)
+  for (int b = 0; b < TB; ++b)
+    ob[b] = ksub[d + NC * (l1_0 + b)] * NC + l1_0 + b;
+
+  // Sums of -s_m alpha beta (the factor 1/2 is applied at the flush); the sign selects the loop
+  // body (uniform across the CTA), so no multiply is spent on it.
+  float2 acc[TA][TB];
+#pragma unroll
+  for (int a = 0; a < TA; ++a)
+#pragma unroll
+    for (int b = 0; b < TB; ++b)
       acc[a][b] = make_float2(0.f, 0.f);
 
+  // Each warp arrives on empty[stage] when it is done with a measurement; thread 0 waits for all
+  // warps there before re-filling the stage, so the other warps can run up to DEPTH - 1
+  // measurements ahead of the slowest one instead of meeting at a block barrier.
+  bool ok = true;
+  int sg = n_slots > 0 ? signs[0] : 1;
   for (int m = 0; m < n_slots; ++m) {
-    const int st = m & 1;
-    const bool ok = mbarWait(&bar[st], (m >> 1) & 1, err);
-    if (!__syncthreads_and(ok))
-      return;  // uniform bail-out; the host reports the error word
+    const int st = m % DEPTH;
+    const int sg_next = m + 1 < n_slots ? signs[m + 1] : 1;
+    ok = __all_sync(0xffffffffu, mbarWait(&full[st], (m / DEPTH) & 1, err));
+    if (!ok)
+      break;
     const float2* S = stage + st * 4 * BLK;
-    const float nhs = -0.5f * static_cast<float>(signs[m]);
-    // Re-layout: part p = (spin, alpha|beta); x (k1 or l1) fastest, so the gathers from the
-    // row-major blocks fall in distinct banks.
-#pragma unroll
-    for (int r = 0; r < 4 * BLK / NT; ++r) {
-      const int e = t + r * NT;
-      const int part = e / BLK, rem = e % BLK, dd = rem / NC, x = rem % NC;
-      const int spin = part >> 1;
-      const int km = ksub[dd + NC * x];  // x - d
-      float2 v;
-      if (part & 1) {
-        v = S[(2 * spin + 1) * BLK + km * NC + x];
-      }
-      else {
-        v = S[(2 * spin) * BLK + x * NC + km];
-        v = make_float2(nhs * v.x, nhs * v.y);
-      }
-      ab[(part * NC + dd) * AR + x] = v;
-    }
-    fenceProxyAsync();  // this thread's accesses to the stage precede the next bulk copy into it
-    __syncthreads();    // alpha / beta ready; stage st free
-    if (t == 0 && m + 2 < n_slots)
-      issue(m + 2, st);
+    const bool add = sg < 0;
 #pragma unroll
     for (int spin = 0; spin < 2; ++spin) {
-      const float2* al = ab + ((2 * spin) * NC + d) * AR + k1_0;
-      const float2* be = ab + ((2 * spin + 1) * NC + d) * AR + l1_0;
-      float2 av[TL], bv[TL];
+      const float2* A = S + (2 * spin) * BLK;
+      const float2* B = S + (2 * spin + 1) * BLK;
+      float2 av[TA], bv[TB];
 #pragma unroll
-      for (int a = 0; a < TL; a += 2) {
-        if constexpr (TL >= 2) {
-          const float4 x = *reinterpret_cast<const float4*>(al + a);
-          av[a] = make_float2(x.x, x.y);
-          av[a + 1] = make_float2(x.z, x.w);
-          const float4 y = *reinterpret_cast<const float4*>(be + a);
-          bv[a] = make_float2(y.x, y.y);
-          bv[a + 1] = make_float2(y.z, y.w);
-        }
+      for (int a = 0; a < TA; ++a)
+        av[a] = A[oa[a]];
+#pragma unroll
+      for (int b = 0; b < TB; ++b)
+        bv[b] = B[ob[b]];
+      if (add) {
+#pragma unroll
+        for (int a = 0; a < TA; ++a)
+#pragma unroll
+          for (int b = 0; b < TB; ++b)
+            cfma(acc[a][b], av[a], bv[b]);
       }
-      if constexpr (TL == 1) {
-        av[0] = al[0];
-        bv[0] = be[0];
+      else {
+#pragma unroll
+        for (int a = 0; a < TA; ++a)
+#pragma unroll
+          for (int b = 0; b < TB; ++b) {
+            float2& c = acc[a][b];
+            c.x = fmaf(-av[a].x, bv[b].x, c.x);
+            c.x = fmaf(av[a].y, bv[b].y, c.x);
+            c.y = fmaf(-av[a].x, bv[b].y, c.y);
+            c.y = fmaf(-av[a].y, bv[b].x, c.y);
+          }
       }
-#pragma unroll
-      for (int a = 0; a < TL; ++a)
-#pragma unroll
-        for (int b = 0; b < TL; ++b)
-          cfma(acc[a][b], av[a], bv[b]);
     }
-    __syncthreads();  // alpha / beta free for the next measurement
+    sg = sg_next;
+    __syncwarp();
+    if (lane == 0)
+      mbarArrive(&empty[st]);  // release: this warp's reads of the stage are done
+    if (t == 0 && m + DEPTH < n_slots) {
+      if (!mbarWait(&empty[st], (m / DEPTH) & 1, err)) {
+        ok = false;  // the other warps see the missing copy as a timeout of their own
+        break;
+      }
+      issue(m + DEPTH);
+    }
   }
+  if (__syncthreads_or(!ok))
+    return;  // uniform bail-out; the host reports the error word
 
   // Flush table T[k2][k1][qi] (rows padded to QP), then lanes take consecutive k1.
 #pragma unroll
-  for (int a = 0; a < TL; ++a)
+  for (int a = 0; a < TA; ++a)
 #pragma unroll
-    for (int b = 0; b < TL; ++b) {
+    for (int b = 0; b < TB; ++b) {
       const int k1 = k1_0 + a, l1 = l1_0 + b;
       const int k2 = ksub[d + NC * k1];
       const int qi = qinv[ksub[k1 + NC * l1]];
-      T[(k2 * NC + k1) * QP + qi] = acc[a][b];
+      T[(k2 * NC + k1) * QP + qi] = make_float2(0.5f * acc[a][b].x, 0.5f * acc[a][b].y);
     }
   __syncthreads();
   const long M = static_cast<long>(NC) * nw;
   const long s_w1 = NC, s_k2 = s_w1 * nw, s_w2 = s_k2 * NC, s_q = s_w2 * nw, s_wq = s_q * nq;
   const int n_ch = dims.n_channels;
-  for (int idx = t; idx < NC * NC * nq; idx += NT) {
-    const int fk1 = idx % NC, j = (idx / NC) % NC, fqi = idx / (NC * NC);
-    const float2 v = T[(j * NC + fk1) * QP + fqi];
-    const long g4i = fk1 + w1 * s_w1 + j * s_k2 + w2 * s_w2 + fqi * s_q + iwq * s_wq;
-    const long di = (j + static_cast<long>(NC) * w2) * M + fk1 + static_cast<long>(NC) * w1;
+  // Four entries per thread and pass, all their loads issued before any add, so the DRAM round
+  // trips of the flush overlap instead of running one entry at a time.
+  constexpr int U = 4;
+  const int total = NC * NC * nq;
+  for (int base = t; base < total; base += U * NT) {
+    float2 v[U];
+    long g4i[U], di[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = min(base + u * NT, total - 1);
+      const int fk1 = idx % NC, j = (idx / NC) % NC, fqi = idx / (NC * NC);
+      v[u] = T[(j * NC + fk1) * QP + fqi];
+      g4i[u] = fk1 + w1 * s_w1 + j * s_k2 + w2 * s_w2 + fqi * s_q + iwq * s_wq;
+      di[u] = (static_cast<long>(iwq * nq + fqi) * n_ch * M + j + static_cast<long>(NC) * w2) * M + fk1 +
+              static_cast<long>(NC) * w1;
+    }
     for (int c = 0; c < n_ch; ++c) {
-      const float2 dv = disc[(static_cast<long>(iwq * nq + fqi) * n_ch + c) * M * M + di];
-      double2* p = G4[c] + g4i;
-      const double re = static_cast<double>(v.x + dv.x), im = static_cast<double>(v.y + dv.y);
-      if (atomic) {
-        atomicAdd(&p->x, re);
-        atomicAdd(&p->y, im);
+      float2 dv[U];
+      double2 o[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        dv[u] = __ldg(disc + di[u] + static_cast<long>(c) * M * M);
+        o[u] = atomic ? make_double2(0., 0.) : G4[c][g4i[u]];
       }
-      else {
-        double2 o = *p;
-        o.x += re;
-        o.y += im;
-        *p = o;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (base + u * NT >= total)
+          continue;
+        double2* p = G4[c] + g4i[u];
+        const double re = static_cast<double>(v[u].x + dv[u].x), im = static_cast<double>(v[u].y + dv[u].y);
+        if (atomic) {
+          atomicAdd(&p->x, re);
+          atomicAdd(&p->y, im);
+        }
+        else {
+          o[u].x += re;
+          o[u].y += im;
+          *p = o[u];
+        }
       }
     }
   }
 }
 
 template <int NC>
+struct OuterTile;  // per-thread tile (k1 x l1) of the outer-product kernel
+// A beta gather B[l1 - d][l1] falls in the bank of column l1, so the threads of a warp that read
+// betas at once should span few d values: with 4 x 4 tiles a warp holds two d values (2-way at
+// most), and the alphas A[k1][k1 - d] spread over distinct banks.
+template <>
+struct OuterTile<16> {
+  static constexpr int TA = 4, TB = 4;
+};
+template <>
+struct OuterTile<8> {
+  static constexpr int TA = 2, TB = 2;
+};
+template <>
+struct OuterTile<4> {
+  static constexpr int TA = 1, TB = 1;
+};
+
+template <int NC>
 size_t outerSmem() {
   constexpr int BLK = NC * NC;
-  const size_t loop = sizeof(float2) * (2 * 4 * BLK + 4 * NC * (NC + 2));
+  const size_t loop = sizeof(float2) * 8 * 4 * BLK;
   const size_t table = sizeof(float2) * size_t(NC) * NC * (NC + 1);
-  return 16 + 4 * (BLK + NC + 4) + std::max(loop, table);
+  return 16 * 8 + 4 * (BLK + NC + 4) + std::max(loop, table);
 }
 
 template <int NC>
 void launchOuter(const G4Args& a, const float2* G, long stride, const float2* disc, cudaStream_t stream) {
   const TpDims& d = a.dims;
+  constexpr int TA = OuterTile<NC>::TA, TB = OuterTile<NC>::TB;
   const size_t smem = outerSmem<NC>();
-  auto k = updateG4SinglebandOuter<NC>;
+  auto k = updateG4SinglebandOuter<NC, TA, TB>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long blocks = long(d.nw) * d.nw * d.nwq;
-  k<<<static_cast<unsigned>(blocks), NC * 16, smem, stream>>>(d, G, stride, a.signs, a.n_slots, a.k_sub, a.q_list,
+  constexpr int threads = NC * (NC / TA) * (NC / TB);
+  k<<<static_cast<unsigned>(blocks), threads, smem, stream>>>(d, G, stride, a.signs, a.n_slots, a.k_sub, a.q_list,
                                                               a.wex_list, disc, a.G4, a.atomic, a.err);
   DCAACC_LAUNCH_CHECK();
 }

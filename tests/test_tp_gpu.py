@@ -156,6 +156,22 @@ def test_sum_to_equals_single_accumulator(precision):
         assert np.all(zero == 0)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_accumulate_batch_equals_single_calls(precision):
+    """dcaacc_tp_accumulate_batch stages the same measurements in the same order: identical G4."""
+    from dca_b200.accumulators import TpAccumulator
+    case = case_from_workload(W.WORKLOADS["c1"], 7)
+    single = run_gpu(case, precision=precision, max_batch=3)
+    acc = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=3))
+    acc.resetAccumulation(0)
+    ms = case.measurements
+    acc.accumulate_batch([[s.M for s in m.sectors] for m in ms], [list(m.sectors) for m in ms],
+                         [m.sign for m in ms])
+    acc.finalize()
+    for a, b in zip(acc.get_G4(), single.get_G4()):
+        assert np.array_equal(a, b)
+
+
 def test_device_resident_m_matches_host_m():
     import torch
     case, _ = golden("mb3_all")
