@@ -277,7 +277,7 @@ struct GemmParams {
   const int* eP;        // [spin][Dp] row exponents of P
   const int* eQ;        // [spin][Dp] row exponents of Q
   const float* mInv;    // [sector][Kr] 2^-e of M's rows j (row step's output columns)
-  float* xInv;          // [sector][Dp][Kr / 32] 2^-e of each X' row chunk (real and imaginary)
+  float* xInv;          // [sector][Dp / 128][Kr / 32] 2^-e of X' per (128-row tile, 32-wide chunk)
   __half* ac;           // row step: X' planes out
   float2* G;            // column step: G out
   long g_sector_stride;
@@ -301,14 +301,17 @@ __device__ inline void tileOf(const GemmParams& p, int t, int& sec, int& mt, int
 }
 
 // MODE 0: row step, A = P planes, B = M planes (rows j), output X' planes and their chunk scales.
-// MODE 1: column step, A = X' planes, B = Q planes, output G.
+// MODE 1: column step on the transpose, A = Q planes (rows rho2), B = X' planes (rows rho1):
+//   tensor-memory lane = rho2, so consecutive lanes store consecutive columns of a G block row
+//   (two full 128-byte lines per store instruction); output G.
 template <int MODE>
 __global__ void __launch_bounds__(kGemmThreads, 1)
 frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 const GemmParams p) {
   constexpr uint32_t stage_bytes = (MODE == 0 ? 3 : 4) * kPl * kBox;
   const int n_tiles = p.n_sectors * p.mt * p.nt;
-  const int kxc = p.Kr / kBK;  // X' row chunks (scale table stride)
+  const int kxc = p.Kr / kBK;  // X' chunks per row (scale table stride)
+  const int xtiles = p.Dp / kBM;
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base =
@@ -319,6 +322,8 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
   uint64_t* acc_full = bars + 2 * kStages;   // [2] MMA -> epilogue
   uint64_t* acc_empty = acc_full + 2;        // [2] epilogue -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+  uint64_t* red_bar = bars + 12;                     // epilogue warps exchanged their chunk maxima
+  float* red = reinterpret_cast<float*>(bars + 16);  // [2][4 quarters][4 column groups] chunk maxima
 
   const int t = threadIdx.x, warp = t / 32, lane = t % 32;
   int* err = p.err;
@@ -335,6 +340,7 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
       mbarInit(&acc_full[b], 1);
       mbarInit(&acc_empty[b], kEpiWarps);  // one arrival per epilogue warp
     }
+    mbarInit(red_bar, kEpiWarps);
     fenceBarrierInit();
     tc::prefetchTensorMap(&tmA);
     tc::prefetchTensorMap(&tmB);
@@ -412,10 +418,11 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
               }
               else {
                 const uint64_t bi = tc::descAdvance(tc::smemDescSw64(st + boxOff(3, pb[pp])), kk * 32);
+                // G^T: Re = Qr Xr^T + Qi Xi^T, Im = Qr Xi^T - Qi Xr^T.
                 tc::mmaBf16(re, ar, br, idesc, first);
                 tc::mmaBf16(re, ai, bi, idesc, 1);
-                tc::mmaBf16(im, ai, br, idesc, first);
-                tc::mmaBf16(im, ar, bi, idesc | tc::kNegateA, 1);
+                tc::mmaBf16(im, ar, bi, idesc, first);
+                tc::mmaBf16(im, ai, br, idesc | tc::kNegateA, 1);
               }
             }
           }
@@ -432,20 +439,21 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const int cg = (warp - 2) >> 2;
     const int row = quarter * 32 + lane;
     const uint32_t lane_addr = static_cast<uint32_t>(quarter * 32) << 16;
-    int g = 0;
+    int g = 0, tiles_done = 0;
     bool ok = true;
     for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
       int sec, mt, nt, chunks;
       tileOf<MODE>(p, tile, sec, mt, nt, chunks);
       if (chunks < 0)
         continue;
+      ++tiles_done;
       const SectorDesc sd = p.sectors[sec];
       float ar[32], ai[32];
 #pragma unroll
       for (int i = 0; i < 32; ++i)
         ar[i] = ai[i] = 0.f;
       const int rho = mt * kBM + row;
-      const float* xinv = p.xInv + (static_cast<long>(sec) * p.Dp + rho) * kxc;
+      const float* xinv = p.xInv + (static_cast<long>(sec) * xtiles + nt) * kxc;
       for (int c = 0; c < chunks; ++c, ++g) {
         const int buf = g & 1;
         // Column step: the A rows of chunk c carry the scale 2^e of that X' row chunk; undo it.
@@ -478,13 +486,16 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         break;
       if (MODE == 0) {
         // X'(rho, j) = acc 2^{-eP(rho)} 2^{-e_j}, j = 128 nt + 32 cg + i: one 32-wide K chunk of the
-        // column step (written only if that step reads it, j0 < roundup(n, 32)), stored scaled by
-        // 2^s from the chunk's maximum over real and imaginary parts.
+        // column step, whose B tile (128 rows rho of this tile) needs one scale for the whole
+        // chunk: the maximum over the four warps with this column group, exchanged through `red`
+        // (double-buffered by tile parity) at a barrier of the 16 epilogue warps.  The chunk is
+        // written only if the column step reads it (j0 < roundup(n, 32)).
         const int j0 = nt * kBN + cg * 32;
-        if (j0 < chunks * kBK) {
+        const bool live = j0 < chunks * kBK;
+        float mx = 0.f;
+        if (live) {
           const float pinv = ldexpf(1.f, -p.eP[sd.spin * p.Dp + rho]);
           const float* minv = p.mInv + static_cast<long>(sec) * p.Kr + j0;
-          float mx = 0.f;
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
             const float sc = pinv * minv[i];
@@ -492,6 +503,21 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             ai[i] *= sc;
             mx = fmaxf(mx, fmaxf(fabsf(ar[i]), fabsf(ai[i])));
           }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+          mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        float* rb = red + (tiles_done & 1) * 16;
+        __syncwarp();
+        if (lane == 0) {
+          rb[quarter * 4 + cg] = mx;
+          mbarArrive(red_bar);  // release: this warp's maximum is visible to the waiters
+        }
+        ok = __all_sync(0xffffffffu, mbarWait(red_bar, (tiles_done - 1) & 1, err));
+        if (!ok)
+          break;
+        mx = fmaxf(fmaxf(rb[cg], rb[4 + cg]), fmaxf(rb[8 + cg], rb[12 + cg]));
+        if (live) {
           const int e = mx > 0.f ? kScaleTop - ilogbf(mx) : 0;
           const long kp = 2L * p.Kr;
           const long plane = static_cast<long>(p.Dp) * kp;
@@ -509,35 +535,36 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             store8(o + p.Kr + g8 * 8, hi);
             store8(o + plane + p.Kr + g8 * 8, li);
           }
-          p.xInv[(static_cast<long>(sec) * p.Dp + rho) * kxc + j0 / kBK] = ldexpf(1.f, -e);
+          if (quarter == 0 && lane == 0)
+            p.xInv[(static_cast<long>(sec) * xtiles + mt) * kxc + j0 / kBK] = ldexpf(1.f, -e);
         }
       }
       else if (rho < p.D) {
+        // Lane row rho = rho2 (a column of G), columns i -> rho1 = 128 nt + 32 cg + i (rows of G):
+        // G(rho1, rho2) = acc 2^{-eQ(rho2)} + beta G0 delta.
         const TpDims& d = p.dims;
         const int R = d.R, nb = d.nb, nc = d.nc, nw_ext = d.nw_ext;
-        const int r1 = rho % R, w1 = rho / R, b1 = r1 % nb, k1 = r1 / nb;
-        float2* gout = p.G + p.g_sector_stride * (2 * sd.slot + sd.spin) + (static_cast<long>(w1) * nw_ext) * R * R +
-                       static_cast<long>(r1) * R;
+        const int r2 = rho % R, w2 = rho / R, b2 = r2 % nb, k2 = r2 / nb;
+        float2* gout = p.G + p.g_sector_stride * (2 * sd.slot + sd.spin) + static_cast<long>(w2) * R * R + r2;
         const double2* g0s = p.G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
-        const int* eq = p.eQ + sd.spin * p.Dp;
+        const float qinv = ldexpf(1.f, -p.eQ[sd.spin * p.Dp + rho]);
         const float beta = static_cast<float>(d.beta);
         const int rho0 = nt * kBN + cg * 32;
-        int r2 = rho0 % R, w2 = rho0 / R;
+        int r1 = rho0 % R, w1 = rho0 / R;
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
           if (rho0 + i < p.D) {
-            const float qinv = ldexpf(1.f, -eq[rho0 + i]);
             float2 v = make_float2(ar[i] * qinv, ai[i] * qinv);
-            if (w2 == w1 && r2 / nb == k1) {
-              const double2 g0 = g0s[b1 + nb * (r2 % nb + nb * (k1 + nc * w1))];
+            if (w1 == w2 && r1 / nb == k2) {
+              const double2 g0 = g0s[r1 % nb + nb * (b2 + nb * (k2 + nc * w2))];
               v.x += beta * static_cast<float>(g0.x);
               v.y += beta * static_cast<float>(g0.y);
             }
-            gout[static_cast<long>(w2) * R * R + r2] = v;
+            gout[static_cast<long>(w1) * nw_ext * R * R + static_cast<long>(r1) * R] = v;
           }
-          if (++r2 == R) {
-            r2 = 0;
-            ++w2;
+          if (++r1 == R) {
+            r1 = 0;
+            ++w1;
           }
         }
       }
@@ -639,7 +666,7 @@ FrontTcShape frontTcShape(const TpDims& d, int n_sectors, int max_order) {
 size_t frontTcBytes(const FrontTcShape& s) {
   const size_t planes = align256((s.pr_elems + s.mb_elems + s.ac_elems + s.bq_elems) * sizeof(__half));
   const size_t scales = align256(2 * sizeof(int) * 2 * s.Dp) + align256(sizeof(float) * s.n_sectors * s.Kr) +
-                        align256(sizeof(float) * s.n_sectors * size_t(s.Dp) * (s.Kr / kBK));
+                        align256(sizeof(float) * s.n_sectors * size_t(s.Dp / kBM) * (s.Kr / kBK));
   return planes + scales;
 }
 
@@ -718,9 +745,9 @@ void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float
   GemmParams p = gemmParams(a, w, err);
   p.G = G;
   p.g_sector_stride = g_sector_stride;
-  p.mt = s.Dp / kBM;
-  p.nt = s.Dq / kBN;
-  launchGemm<1>(p, w.tm_ac, w.tm_bq, w.n_sm, stream);
+  p.mt = s.Dq / kBM;  // rows of G^T: rho2
+  p.nt = s.Dp / kBN;  // columns of G^T: rho1
+  launchGemm<1>(p, w.tm_bq, w.tm_ac, w.n_sm, stream);
 }
 
 }  // namespace dcaacc
