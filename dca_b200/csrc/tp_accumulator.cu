@@ -181,8 +181,11 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
       orb_r_d_.alloc(n_vtx);
       orb_c_d_.alloc(n_vtx);
-      if (singlebandBatchedApplies(dims_))
+      if (discGemmApplies(dims_, max_batch_)) {
         disc_.alloc(discScratchBytes(dims_, max_batch_));
+        discInit(disc_ws_, dims_, max_batch_, disc_.get(), disc_.bytes());
+        have_disc_ = true;
+      }
     }
   }
   else {
@@ -421,8 +424,7 @@ void TpAccumulator::process() {
       distinct += seen[q]++ == 0;
     ga.q_all = distinct == dims_.nc && int(q_list_.size()) == dims_.nc;
   }
-  ga.disc_scratch = disc_.get();
-  ga.disc_scratch_bytes = disc_.bytes();
+  ga.disc = have_disc_ ? &disc_ws_ : nullptr;
   cudaEvent_t b = nullptr;
   timeBegin(DCAACC_STAGE_ROW, &b);
   if (tc_front_)

@@ -17,6 +17,7 @@
 #include "../../include/dcaacc.h"
 #include "common.cuh"
 #include "tp_frontend.hpp"
+#include "tp_g4.hpp"
 #include "tp_layout.hpp"
 
 namespace dcaacc {
@@ -151,6 +152,8 @@ private:
   DevBuf<double2> X64_, G64_;  // FP64 mode
   DevBuf<float2> X32_, G32_;   // mixed mode
   DevBuf<unsigned char> disc_;  // mixed mode, one band: tensor-core disconnected-term workspace
+  DiscWorkspace disc_ws_{};
+  bool have_disc_ = false;
   // Mixed mode: tensor-core front-end (operand planes + TMA descriptors) and the orbital of each
   // vertex in row / column order.
   bool tc_front_ = false;

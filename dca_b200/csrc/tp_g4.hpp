@@ -1,6 +1,7 @@
 // Launch interface of the G4 update kernel (tp_g4.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -22,8 +23,20 @@ struct G4Args {
   bool atomic;          // several accumulators share G4
   int* err;             // device error word (async_copy.cuh kErr* bits)
   bool q_all = false;             // q_list is a permutation of all Nc cluster momenta
-  void* disc_scratch = nullptr;   // workspace of the tensor-core disconnected-term GEMM (or null)
-  size_t disc_scratch_bytes = 0;
+  const struct DiscWorkspace* disc = nullptr;  // tensor-core disconnected-term workspace (or null)
+};
+
+// Workspace of the tensor-core disconnected-term GEMM (tp_g4_disc.cu): U / V operand planes, their
+// row scales, the FP32 result and the TMA descriptors, for batches of up to max_batch measurements.
+struct DiscWorkspace {
+  void* U = nullptr;
+  void* V = nullptr;
+  int* eU = nullptr;
+  int* eV = nullptr;
+  float2* out = nullptr;
+  int max_batch = 0;
+  int n_sm = 0;
+  CUtensorMap tm_u, tm_v;
 };
 
 // dst += src; src = 0 (sumTo of two accumulators on the same device).
@@ -38,10 +51,12 @@ bool singlebandBatchedApplies(const TpDims& d);
 int launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
                                     cudaStream_t stream);
 
-// Tensor-core disconnected terms (tp_g4_disc.cu).  Workspace for batches of up to max_batch
-// measurements; launchDiscGemm returns the device result (per problem an M x M FP32 matrix), or
-// null when a.disc_scratch is missing or too small.
+// Tensor-core disconnected terms (tp_g4_disc.cu): one band, PH channels, batches of at most 256.
+// discInit carves `mem` (discScratchBytes) and builds the descriptors; launchDiscGemm returns the
+// device result (per problem an M x M FP32 matrix), or null without a workspace.
+bool discGemmApplies(const TpDims& d, int max_batch);
 size_t discScratchBytes(const TpDims& d, int max_batch);
+void discInit(DiscWorkspace& w, const TpDims& d, int max_batch, void* mem, size_t bytes);
 const float2* launchDiscGemm(const G4Args& a, const float2* G, long g_sector_stride, cudaStream_t stream);
 
 // G: block-layout G of n_slots measurements, sector (slot, spin) at g_sector_stride * (2 slot + spin).
