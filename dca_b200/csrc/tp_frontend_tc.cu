@@ -124,7 +124,9 @@ __global__ void twiddleWiKernel(const SectorDesc* __restrict__ sectors, const do
 
 // Phase operand (P for the rows, Q for the columns), planes [sector][plane][rows][2 Kr]: real part
 // at column v, imaginary part at column Kr + v, for vertices v < roundup(n, 32) (zero for v >= n);
-// rows rho < D.  One thread per (rho, 8 vertices).
+// rows rho = r + R w < D.  One thread per (w, 8 vertices): it loads the 8 twiddles and orbitals once
+// and walks the R rows of frequency w, writing 16 bytes per plane and part per row (consecutive
+// threads: consecutive vertex groups of one row).
 //   ROW = true:  P(rho, i) 2^eP  = G0_s(b1, b_i; k1, w) Fb(b_i, k1, x_i) T(w, i) 2^eP
 //   ROW = false: Q(rho, j) 2^eQ  = -(1/Nc) Fb(b_j, k2, x_j) T(w, j) conj(G0_s(b_j, b2; k2, w)) 2^eQ
 template <bool ROW>
@@ -141,41 +143,49 @@ buildPhaseOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sector
   __half* o = out + static_cast<long>(blockIdx.y) * kPl * plane;
   const double2* g0s = G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
   const double2* Ts = T + static_cast<long>(sd.vtx_off) * nw_ext;
+  const int* es = eRow + sd.spin * Dp;
   const double qscale = -1.0 / nc;
-  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * D;
+  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * nw_ext;
        idx += long(gridDim.x) * blockDim.x) {
     const int grp = static_cast<int>(idx % groups);
-    const int rho = static_cast<int>(idx / groups);
-    const int r = rho % R, w = rho / R, b = r % nb, k = r / nb;
-    const double e = pow2d(eRow[sd.spin * Dp + rho]);
-    Pack8 re[kPl], im[kPl];
+    const int w = static_cast<int>(idx / groups);
+    double2 tv[8];
+    int bv[8], xv[8];
 #pragma unroll
     for (int x = 0; x < 8; ++x) {
       const int v = grp * 8 + x;
-      double2 z = make_double2(0., 0.);
-      if (v < n) {
-        const int ov = orb[sd.vtx_off + v];
-        const int bv = ov % nb, xv = ov / nb;
-        const double2 ph = zmul(Fb[(bv * nc + k) * nc + xv], Ts[static_cast<long>(w) * n + v]);
+      const bool in = v < n;
+      tv[x] = in ? Ts[static_cast<long>(w) * n + v] : make_double2(0., 0.);
+      const int ov = in ? orb[sd.vtx_off + v] : 0;
+      bv[x] = ov % nb;
+      xv[x] = ov / nb;
+    }
+    for (int r = 0; r < R; ++r) {
+      const int b = r % nb, k = r / nb;
+      const int rho = r + R * w;
+      const double sc = pow2d(es[rho]);
+      Pack8 re[kPl], im[kPl];
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        const double2 ph = zmul(Fb[(bv[x] * nc + k) * nc + xv[x]], tv[x]);
+        double2 z;
         if (ROW) {
-          z = zmul(g0s[b + nb * (bv + nb * (k + nc * w))], ph);
+          z = zmul(g0s[b + nb * (bv[x] + nb * (k + nc * w))], ph);
         }
         else {
-          const double2 g = g0s[bv + nb * (b + nb * (k + nc * w))];
-          z = zmul(ph, make_double2(g.x, -g.y));
-          z.x *= qscale;
-          z.y *= qscale;
+          const double2 g = g0s[bv[x] + nb * (b + nb * (k + nc * w))];
+          z = zmul(ph, make_double2(g.x * qscale, -g.y * qscale));
         }
+        const Split2 a = split2d(z.x, sc), c = split2d(z.y, sc);
+        re[0].v[x] = a.h, re[1].v[x] = a.l;
+        im[0].v[x] = c.h, im[1].v[x] = c.l;
       }
-      const Split2 a = split2d(z.x, e), c = split2d(z.y, e);
-      re[0].v[x] = a.h, re[1].v[x] = a.l;
-      im[0].v[x] = c.h, im[1].v[x] = c.l;
-    }
 #pragma unroll
-    for (int pl = 0; pl < kPl; ++pl) {
-      __half* op = o + pl * plane + static_cast<long>(rho) * kp + grp * 8;
-      store8(op, re[pl]);
-      store8(op + Kr, im[pl]);
+      for (int pl = 0; pl < kPl; ++pl) {
+        __half* op = o + pl * plane + static_cast<long>(rho) * kp + grp * 8;
+        store8(op, re[pl]);
+        store8(op + Kr, im[pl]);
+      }
     }
   }
 }
@@ -320,14 +330,14 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
     ++launches;
   }
   const long groups = (a.n_max + kBK - 1) / kBK * (kBK / 8);
-  buildPhaseOperandKernel<true><<<dim3(gridX(groups * s.D), a.n_sectors), 256, 0, stream>>>(
+  buildPhaseOperandKernel<true><<<dim3(gridX(groups * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
       d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, s.D, s.Dp, s.Dp, s.Kr, static_cast<__half*>(w.pr));
   DCAACC_LAUNCH_CHECK();
   const long mrows = std::min<long>((a.n_max + kBN - 1) / kBN * kBN, s.Kr);
   buildMOperandKernel<<<dim3(static_cast<unsigned>((mrows + 7) / 8), a.n_sectors), 256, 0, stream>>>(
       a.sectors, a.perm_r, a.perm_c, s.Kr, static_cast<__half*>(w.mb), w.mInv);
   DCAACC_LAUNCH_CHECK();
-  buildPhaseOperandKernel<false><<<dim3(gridX(groups * s.D), a.n_sectors), 256, 0, stream>>>(
+  buildPhaseOperandKernel<false><<<dim3(gridX(groups * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
       d, a.sectors, a.Tc, orb_c, a.Fb, a.G0, w.eQ, s.D, s.Dp, s.Dq, s.Kr, static_cast<__half*>(w.bq));
   DCAACC_LAUNCH_CHECK();
   return launches + 3;
