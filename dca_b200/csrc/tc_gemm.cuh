@@ -286,6 +286,17 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         ar[i] = ai[i] = 0.f;
       const int rho = mt * kBM + row;
       const float* xinv = MODE == 1 ? p.xInv + (static_cast<long>(sec) * xtiles + nt) * kxc : nullptr;
+      // Column scales of this warp's 32 columns, one per lane, loaded now (their latency hides
+      // behind the chunk loop) and broadcast with shuffles in the epilogue.
+      float col_scale = 1.f;
+      if (MODE == 0) {
+        const int jl = nt * kBN + cg * 32 + lane;
+        col_scale = jl < p.Kr ? p.mInv[static_cast<long>(sec) * p.Kr + jl] : 1.f;
+      }
+      else if (MODE == 2) {
+        const int nl = nt * kBN + cg * 32 + lane;
+        col_scale = nl < p.Dp ? pow2f(-p.eV[static_cast<long>(sec) * p.Dp + nl]) : 1.f;
+      }
       for (int c = 0; c < chunks; ++c, ++g) {
         const int buf = g & 1;
         // Column step: the A rows of chunk c carry the scale 2^e of that X' row chunk; undo it.
@@ -327,10 +338,9 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         float mx = 0.f;
         if (live) {
           const float pinv = pow2f(-p.eP[sd.spin * p.Dp + rho]);
-          const float* minv = p.mInv + static_cast<long>(sec) * p.Kr + j0;
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
-            const float sc = pinv * minv[i];
+            const float sc = pinv * __shfl_sync(0xffffffffu, col_scale, i);
             ar[i] *= sc;
             ai[i] *= sc;
             mx = fmaxf(mx, fmaxf(fabsf(ar[i]), fabsf(ai[i])));
@@ -375,45 +385,52 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
       else if (MODE == 2) {
         // Lane row rho = m, columns n = 128 nt + 32 cg + i: disc[(problem M + n) M + m] =
         // acc 2^{-eU(m)} 2^{-eV(n)}; consecutive lanes store consecutive m.
-        if (rho < p.Md) {
-          const float uinv = pow2f(-p.eU[static_cast<long>(sec) * p.Dp + rho]);
-          const int* ev = p.eV + static_cast<long>(sec) * p.Dp;
-          const int n0 = nt * kBN + cg * 32;
-          float2* o = p.disc + static_cast<long>(sec) * p.Md * p.Md + rho;
+        const float uinv = rho < p.Md ? pow2f(-p.eU[static_cast<long>(sec) * p.Dp + rho]) : 0.f;
+        const int n0 = nt * kBN + cg * 32;
+        float2* o = p.disc + static_cast<long>(sec) * p.Md * p.Md + rho;
 #pragma unroll
-          for (int i = 0; i < 32; ++i)
-            if (n0 + i < p.Md) {
-              const float sc = uinv * pow2f(-ev[n0 + i]);
-              o[static_cast<long>(n0 + i) * p.Md] = make_float2(ar[i] * sc, ai[i] * sc);
-            }
+        for (int i = 0; i < 32; ++i) {
+          const float sc = uinv * __shfl_sync(0xffffffffu, col_scale, i);  // all lanes take part
+          if (rho < p.Md && n0 + i < p.Md)
+            o[static_cast<long>(n0 + i) * p.Md] = make_float2(ar[i] * sc, ai[i] * sc);
         }
       }
       else if (rho < p.D) {
         // Lane row rho = rho2 (a column of G), columns i -> rho1 = 128 nt + 32 cg + i (rows of G):
-        // G(rho1, rho2) = acc 2^{-eQ(rho2)} + beta G0 delta.
+        // G(rho1, rho2) = acc 2^{-eQ(rho2)} + beta G0 delta.  The delta term sits at the nb
+        // columns rho1 = R w2 + nb k2 + b1; the G offset of rho1 advances incrementally.
         const TpDims& d = p.dims;
         const int R = d.R, nb = d.nb, nc = d.nc, nw_ext = d.nw_ext;
         const int r2 = rho % R, w2 = rho / R, b2 = r2 % nb, k2 = r2 / nb;
         float2* gout = p.G + p.g_sector_stride * (2 * sd.slot + sd.spin) + static_cast<long>(w2) * R * R + r2;
-        const double2* g0s = p.G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
+        const double2* g0d = p.G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb +
+                             nb * (b2 + nb * (k2 + nc * w2));  // + b1 -> G0_s(b1, b2; k2, w2)
         const float qinv = pow2f(-p.eQ[sd.spin * p.Dp + rho]);
         const float beta = static_cast<float>(d.beta);
         const int rho0 = nt * kBN + cg * 32;
-        int r1 = rho0 % R, w1 = rho0 / R;
+        const int delta0 = R * w2 + nb * k2;
+        const int row_step = R, wrap_step = nw_ext * R * R - (R - 1) * R;
+        int r1 = rho0 % R;
+        int off = (rho0 / R) * nw_ext * R * R + r1 * R;
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
-          if (rho0 + i < p.D) {
+          const int rho1 = rho0 + i;
+          if (rho1 < p.D) {
             float2 v = make_float2(ar[i] * qinv, ai[i] * qinv);
-            if (w1 == w2 && r1 / nb == k2) {
-              const double2 g0 = g0s[r1 % nb + nb * (b2 + nb * (k2 + nc * w2))];
+            const unsigned b1 = static_cast<unsigned>(rho1 - delta0);
+            if (b1 < static_cast<unsigned>(nb)) {
+              const double2 g0 = g0d[b1];
               v.x += beta * static_cast<float>(g0.x);
               v.y += beta * static_cast<float>(g0.y);
             }
-            gout[static_cast<long>(w1) * nw_ext * R * R + static_cast<long>(r1) * R] = v;
+            gout[off] = v;
           }
           if (++r1 == R) {
             r1 = 0;
-            ++w1;
+            off += wrap_step;
+          }
+          else {
+            off += row_step;
           }
         }
       }
