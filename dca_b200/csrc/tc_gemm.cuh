@@ -109,11 +109,22 @@ struct GemmParams {
 // the tile has no work (row step: columns j beyond the sector's order).
 template <int MODE>
 __device__ inline void tileOf(const GemmParams& p, int t, int& sec, int& mt, int& nt, int& chunks) {
-  const int per = p.mt * p.nt;
-  sec = t / per;
-  const int rem = t % per;
-  mt = rem / p.nt;
-  nt = rem % p.nt;
+  if (MODE == 0) {
+    // Row step: column tiles (j) slowest.  Tiles with j beyond a sector's order are skipped, and
+    // with the column tile slowest they spread evenly over the persistent CTAs (with it fastest,
+    // a CTA would keep meeting the same column tile).
+    const int per = p.n_sectors * p.mt;
+    nt = t / per;
+    sec = (t % per) / p.mt;
+    mt = t % p.mt;
+  }
+  else {
+    const int per = p.mt * p.nt;
+    sec = t / per;
+    const int rem = t % per;
+    mt = rem / p.nt;
+    nt = rem % p.nt;
+  }
   if (MODE == 2) {
     chunks = (p.n_slots + kBK - 1) / kBK;
     return;
@@ -367,16 +378,21 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
           __half* o = p.ac + static_cast<long>(sec) * kPl * plane + static_cast<long>(rho) * kp + j0;
 #pragma unroll
           for (int g8 = 0; g8 < 4; ++g8) {
-            Pack8 hr, lr, hi, li;
+            Pack8 h, l;
 #pragma unroll
             for (int x = 0; x < 8; ++x) {
-              const Split2 a = split2f(ar[g8 * 8 + x], sc), b = split2f(ai[g8 * 8 + x], sc);
-              hr.v[x] = a.h, lr.v[x] = a.l, hi.v[x] = b.h, li.v[x] = b.l;
+              const Split2 a = split2f(ar[g8 * 8 + x], sc);
+              h.v[x] = a.h, l.v[x] = a.l;
             }
-            store8(o + g8 * 8, hr);
-            store8(o + plane + g8 * 8, lr);
-            store8(o + p.Kr + g8 * 8, hi);
-            store8(o + plane + p.Kr + g8 * 8, li);
+            store8(o + g8 * 8, h);
+            store8(o + plane + g8 * 8, l);
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+              const Split2 b = split2f(ai[g8 * 8 + x], sc);
+              h.v[x] = b.h, l.v[x] = b.l;
+            }
+            store8(o + p.Kr + g8 * 8, h);
+            store8(o + plane + p.Kr + g8 * 8, l);
           }
           if (quarter == 0 && lane == 0)
             p.xInv[(static_cast<long>(sec) * xtiles + mt) * kxc + j0 / kBK] = pow2f(-e);
