@@ -173,32 +173,23 @@ class ClockSampler:
 
 
 def dist_setup(n_gpus):
+    from dca_b200 import replicas
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import torch
-        import torch.distributed as dist
         torch.cuda.set_device(local)
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    return world, rank, local
+    return replicas.init_from_env("nccl")
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from dca_b200 import replicas
+    replicas.barrier()
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from dca_b200 import replicas
+    return replicas.max_over_ranks(x)
 
 
 # ------------------------------------------------------------------------------------------------
