@@ -365,11 +365,17 @@ def run_ours(args, world, rank, local):
     nwe = nw + 2 * w.ext()
     D = nb * nc * nwe
     n_g4 = nb ** 4 * nc ** 2 * nw ** 2 * len(w.exchange_momenta(nc)) * len(w.exchange_frequencies())
+    simt = os.environ.get("DCAACC_TP_SIMT_ONLY") == "1"
     if dom == "update_g4":
+        # Algorithmic bytes of one batch's update: the FP64 read-modify-write of every G4 entry of
+        # every channel, and one read of the batch's G (FP32 complex, both spins).
         alg_bytes = len(w.channels) * n_g4 * 32 + B * 2 * D * D * 8
-        roof = {"kernel": "updateG4Kernel<float2,float>", "bound": "hbm",
-                "achieved": alg_bytes / (per_launch_ms / 1e3) / 1e9, "peak": hbm_gbs, "unit": "GB/s",
-                "traffic": None, "peak_source": peak_src}
+        sec = dom_ms / args.steps / 1e3  # the stage's time per batch (its kernels run back to back)
+        roof = {"kernel": "update_g4 stage: discPlanesKernel + frontGemmKernel<2> (disconnected terms) + "
+                          "updateG4SinglebandOuter<16, 4, 4> (direct term, G4 flush)" if not simt else
+                          "updateG4SinglebandBatched", "bound": "hbm",
+                "achieved": alg_bytes / sec / 1e9, "peak": hbm_gbs, "unit": "GB/s",
+                "traffic": None, "peak_source": peak_src, "algorithmic_bytes": alg_bytes}
     elif dom in ("col_transform", "row_transform") and os.environ.get("DCAACC_TP_SIMT_ONLY") != "1":
         # Tensor-core front-end.  Algorithmic flops: the complex contractions themselves,
         # G = X' Q^H (8 D^2 n per sector) or X' = P M (4 D n^2, M real).  The split-FP16 products
@@ -410,6 +416,20 @@ def run_ours(args, world, rank, local):
                 "peak": hbm_gbs, "unit": "GB/s", "traffic": None, "peak_source": peak_src}
     roof["frac"] = roof["achieved"] / roof["peak"]
     roof["ms_per_launch"] = per_launch_ms
+    # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the stage's kernels from the
+    # committed ncu capture of this workload (one batch, cold caches), per launch of the stage.
+    stage_kernels = {"update_g4": ["discPlanesKernel", "frontGemmKernel<2>", "updateG4SinglebandOuter<16, 4, 4>"],
+                     "col_transform": ["frontGemmKernel<1>"], "row_transform": ["frontGemmKernel<0>"],
+                     "twiddle": ["twiddleWiKernel", "buildPhaseOperandKernel<0>", "buildPhaseOperandKernel<1>",
+                                 "buildMOperandKernel"]}.get(dom, [])
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            tk = json.load(f)["kernels"]
+        if w.name == "c3" and not simt and stage_kernels and all(k in tk for k in stage_kernels):
+            roof["traffic"] = sum(tk[k]["dram_read_bytes"] + tk[k]["dram_write_bytes"] for k in stage_kernels)
+            roof["traffic_unit"] = "bytes per launch of the stage (ncu, profiles/dram_traffic.json)"
+    except (OSError, ValueError, KeyError):
+        pass
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
