@@ -28,10 +28,16 @@ constexpr int kBK = 32;                           // K per chunk: one 64-byte sw
 constexpr uint32_t kBox = kBM * kBK * 2;          // one 128 x 32 FP16 box: 8 KB
 constexpr uint32_t kStageStride = 4 * kPl * kBox; // A re, A im, B re, B im (x planes): 64 KB
 constexpr int kStages = 3;
-constexpr size_t kGemmSmem = 1024 + kStages * kStageStride + 256;
 constexpr int kEpiWarps = 16;
+constexpr uint32_t kBarBytes = 256;  // barriers, tensor-memory slot, chunk maxima
+// Dynamic shared memory: alignment slack, operand stages, barriers.
+template <int MODE>
+__host__ __device__ constexpr size_t gemmSmem() {
+  return 1024 + kStages * kStageStride + kBarBytes;
+}
 constexpr int kGemmThreads = 32 * (2 + kEpiWarps);  // 576
 constexpr int kScaleTop = 14;  // scaled maxima land in [2^14, 2^15) (one binade lower for bounds)
+constexpr int kMaxDeltaBands = 1;  // bands whose delta-term G0 values the epilogue preloads (registers)
 
 // Offsets inside a stage.
 __host__ __device__ constexpr uint32_t boxOff(int part, int plane) {
@@ -104,6 +110,21 @@ struct GemmParams {
   const int* eV;        // [problem][Dp] row exponents of V
   float2* disc;         // [problem][n][m] FP32 result
 };
+
+// Column step, bands beyond those preloaded: adds beta G0_s(b1, b2; k2, w2) to v when column rho1
+// of G is a delta column of row rho2 = rho (rho < D).
+__device__ inline float2 addDeltaInPlace(const GemmParams& p, const SectorDesc& sd, int rho, int rho1, float2 v) {
+  const TpDims& d = p.dims;
+  const int r2 = rho % d.R, w2 = rho / d.R;
+  const int b1 = rho1 - (d.R * w2 + d.nb * (r2 / d.nb));
+  if (b1 >= 0 && b1 < d.nb) {
+    const double2 g0 = p.G0[static_cast<long>(sd.spin) * d.nw_ext * d.nc * d.nb * d.nb + b1 +
+                            d.nb * (r2 % d.nb + d.nb * (r2 / d.nb + d.nc * w2))];
+    v.x += static_cast<float>(d.beta) * static_cast<float>(g0.x);
+    v.y += static_cast<float>(d.beta) * static_cast<float>(g0.y);
+  }
+  return v;
+}
 
 // Tile t of the persistent schedule -> (sector, row tile, column tile, K chunks); chunks < 0 when
 // the tile has no work (row step: columns j beyond the sector's order).
@@ -308,6 +329,32 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const int nl = nt * kBN + cg * 32 + lane;
         col_scale = nl < p.Dp ? pow2f(-p.eV[static_cast<long>(sec) * p.Dp + nl]) : 1.f;
       }
+      // Row scale of this thread's row, and (column step) the beta G0 values of the row's delta
+      // columns when they fall in this warp's 32 columns: all loaded before the chunk loop.
+      float row_scale = 1.f;
+      float2 dterm[kMaxDeltaBands];
+      int dcol = -1;  // first delta column relative to this warp's columns, -1 if none here
+      if (MODE == 0)
+        row_scale = pow2f(-p.eP[sd.spin * p.Dp + rho]);
+      else if (MODE == 2)
+        row_scale = rho < p.Md ? pow2f(-p.eU[static_cast<long>(sec) * p.Dp + rho]) : 0.f;
+      else if (rho < p.D) {
+        row_scale = pow2f(-p.eQ[sd.spin * p.Dp + rho]);
+        const TpDims& d = p.dims;
+        const int r2 = rho % d.R, w2 = rho / d.R, b2 = r2 % d.nb, k2 = r2 / d.nb;
+        const int delta0 = d.R * w2 + d.nb * k2 - (nt * kBN + cg * 32);
+        if (delta0 + d.nb > 0 && delta0 < 32 && d.nb <= kMaxDeltaBands) {
+          dcol = delta0;
+          const double2* g0d = p.G0 + static_cast<long>(sd.spin) * d.nw_ext * d.nc * d.nb * d.nb +
+                               d.nb * (b2 + d.nb * (k2 + d.nc * w2));  // + b1 -> G0_s(b1, b2; k2, w2)
+          const float beta = static_cast<float>(d.beta);
+#pragma unroll
+          for (int b = 0; b < kMaxDeltaBands; ++b) {
+            const double2 g0 = b < d.nb ? g0d[b] : make_double2(0., 0.);
+            dterm[b] = make_float2(beta * static_cast<float>(g0.x), beta * static_cast<float>(g0.y));
+          }
+        }
+      }
       for (int c = 0; c < chunks; ++c, ++g) {
         const int buf = g & 1;
         // Column step: the A rows of chunk c carry the scale 2^e of that X' row chunk; undo it.
@@ -318,18 +365,16 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         tc::fenceAfterThreadSync();
         const uint32_t col = tmem + lane_addr + buf * 256 + cg * 32;
 #pragma unroll
-        for (int piece = 0; piece < 2; ++piece) {
-          float v[16];
-          tc::ld32x32bx16(col + piece * 16, v);
+        for (int piece = 0; piece < 2; ++piece) {  // real and imaginary loads share one wait
+          float vr[16], vi[16];
+          tc::ld32x32bx16(col + piece * 16, vr);
+          tc::ld32x32bx16(col + 128 + piece * 16, vi);
           tc::waitLd();
 #pragma unroll
-          for (int i = 0; i < 16; ++i)
-            ar[piece * 16 + i] = fmaf(v[i], f, ar[piece * 16 + i]);
-          tc::ld32x32bx16(col + 128 + piece * 16, v);
-          tc::waitLd();
-#pragma unroll
-          for (int i = 0; i < 16; ++i)
-            ai[piece * 16 + i] = fmaf(v[i], f, ai[piece * 16 + i]);
+          for (int i = 0; i < 16; ++i) {
+            ar[piece * 16 + i] = fmaf(vr[i], f, ar[piece * 16 + i]);
+            ai[piece * 16 + i] = fmaf(vi[i], f, ai[piece * 16 + i]);
+          }
         }
         tc::fenceBeforeThreadSync();
         __syncwarp();
@@ -348,10 +393,9 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const bool live = j0 < chunks * kBK;
         float mx = 0.f;
         if (live) {
-          const float pinv = pow2f(-p.eP[sd.spin * p.Dp + rho]);
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
-            const float sc = pinv * __shfl_sync(0xffffffffu, col_scale, i);
+            const float sc = row_scale * __shfl_sync(0xffffffffu, col_scale, i);
             ar[i] *= sc;
             ai[i] *= sc;
             mx = fmaxf(mx, fmaxf(fabsf(ar[i]), fabsf(ai[i])));
@@ -401,44 +445,39 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
       else if (MODE == 2) {
         // Lane row rho = m, columns n = 128 nt + 32 cg + i: disc[(problem M + n) M + m] =
         // acc 2^{-eU(m)} 2^{-eV(n)}; consecutive lanes store consecutive m.
-        const float uinv = rho < p.Md ? pow2f(-p.eU[static_cast<long>(sec) * p.Dp + rho]) : 0.f;
         const int n0 = nt * kBN + cg * 32;
         float2* o = p.disc + static_cast<long>(sec) * p.Md * p.Md + rho;
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
-          const float sc = uinv * __shfl_sync(0xffffffffu, col_scale, i);  // all lanes take part
+          const float sc = row_scale * __shfl_sync(0xffffffffu, col_scale, i);  // all lanes take part
           if (rho < p.Md && n0 + i < p.Md)
             o[static_cast<long>(n0 + i) * p.Md] = make_float2(ar[i] * sc, ai[i] * sc);
         }
       }
       else if (rho < p.D) {
         // Lane row rho = rho2 (a column of G), columns i -> rho1 = 128 nt + 32 cg + i (rows of G):
-        // G(rho1, rho2) = acc 2^{-eQ(rho2)} + beta G0 delta.  The delta term sits at the nb
-        // columns rho1 = R w2 + nb k2 + b1; the G offset of rho1 advances incrementally.
+        // G(rho1, rho2) = acc 2^{-eQ(rho2)} + beta G0 delta (preloaded: dterm at i = dcol + b1).
+        // The G offset of rho1 advances incrementally.
         const TpDims& d = p.dims;
-        const int R = d.R, nb = d.nb, nc = d.nc, nw_ext = d.nw_ext;
-        const int r2 = rho % R, w2 = rho / R, b2 = r2 % nb, k2 = r2 / nb;
+        const int R = d.R, nw_ext = d.nw_ext;
+        const int r2 = rho % R, w2 = rho / R;
         float2* gout = p.G + p.g_sector_stride * (2 * sd.slot + sd.spin) + static_cast<long>(w2) * R * R + r2;
-        const double2* g0d = p.G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb +
-                             nb * (b2 + nb * (k2 + nc * w2));  // + b1 -> G0_s(b1, b2; k2, w2)
-        const float qinv = pow2f(-p.eQ[sd.spin * p.Dp + rho]);
-        const float beta = static_cast<float>(d.beta);
         const int rho0 = nt * kBN + cg * 32;
-        const int delta0 = R * w2 + nb * k2;
         const int row_step = R, wrap_step = nw_ext * R * R - (R - 1) * R;
         int r1 = rho0 % R;
         int off = (rho0 / R) * nw_ext * R * R + r1 * R;
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
-          const int rho1 = rho0 + i;
-          if (rho1 < p.D) {
-            float2 v = make_float2(ar[i] * qinv, ai[i] * qinv);
-            const unsigned b1 = static_cast<unsigned>(rho1 - delta0);
-            if (b1 < static_cast<unsigned>(nb)) {
-              const double2 g0 = g0d[b1];
-              v.x += beta * static_cast<float>(g0.x);
-              v.y += beta * static_cast<float>(g0.y);
-            }
+          if (rho0 + i < p.D) {
+            float2 v = make_float2(ar[i] * row_scale, ai[i] * row_scale);
+#pragma unroll
+            for (int b = 0; b < kMaxDeltaBands; ++b)
+              if (i == dcol + b && b < d.nb) {
+                v.x += dterm[b].x;
+                v.y += dterm[b].y;
+              }
+            if (d.nb > kMaxDeltaBands)  // more bands than preloaded: load in place
+              v = addDeltaInPlace(p, sd, rho, rho0 + i, v);
             gout[off] = v;
           }
           if (++r1 == R) {
@@ -495,10 +534,12 @@ inline void makePlaneMap(CUtensorMap* map, void* base, long cols, long rows, lon
 template <int MODE>
 void launchGemm(const GemmParams& p, const CUtensorMap& ta, const CUtensorMap& tb, int n_sm, cudaStream_t stream) {
   auto k = frontGemmKernel<MODE>;
-  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGemmSmem)));
+  constexpr size_t smem = gemmSmem<MODE>();
+  static_assert(smem <= 227 * 1024, "shared memory per CTA");
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const long tiles = long(p.n_sectors) * p.mt * p.nt;
   const unsigned grid = static_cast<unsigned>(std::max(1L, std::min<long>(tiles, n_sm)));
-  k<<<grid, kGemmThreads, kGemmSmem, stream>>>(ta, tb, p);
+  k<<<grid, kGemmThreads, smem, stream>>>(ta, tb, p);
   DCAACC_LAUNCH_CHECK();
 }
 
