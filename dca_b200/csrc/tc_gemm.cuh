@@ -109,6 +109,7 @@ struct GemmParams {
   const int* eU;        // [problem][Dp] row exponents of U
   const int* eV;        // [problem][Dp] row exponents of V
   float2* disc;         // [problem][n][m] FP32 result
+  int* gmax;            // column step: [2 slot + spin] largest |G| of the sector (float bits), or null
 };
 
 // Column step, bands beyond those preloaded: adds beta G0_s(b1, b2; k2, w2) to v when column rho1
@@ -383,6 +384,7 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
       }
       if (!ok)
         break;
+      float gabs = 0.f;  // column step: largest |Re|, |Im| this thread stores
       if (MODE == 0) {
         // X'(rho, j) = acc 2^{-eP(rho)} 2^{-e_j}, j = 128 nt + 32 cg + i: one 32-wide K chunk of the
         // column step, whose B tile (128 rows rho of this tile) needs one scale for the whole
@@ -479,6 +481,7 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             if (d.nb > kMaxDeltaBands)  // more bands than preloaded: load in place
               v = addDeltaInPlace(p, sd, rho, rho0 + i, v);
             gout[off] = v;
+            gabs = fmaxf(gabs, fmaxf(fabsf(v.x), fabsf(v.y)));
           }
           if (++r1 == R) {
             r1 = 0;
@@ -488,6 +491,15 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             off += row_step;
           }
         }
+      }
+      if (MODE == 1 && p.gmax) {
+        // The sector's largest |G| (the G4 kernel scales its FP16 operands with it): warp maximum,
+        // then one atomic per warp and tile (non-negative floats order like their bit patterns).
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+          gabs = fmaxf(gabs, __shfl_xor_sync(0xffffffffu, gabs, off));
+        if (lane == 0 && gabs > 0.f)
+          atomicMax(p.gmax + 2 * sd.slot + sd.spin, __float_as_int(gabs));
       }
     }
   }

@@ -181,6 +181,7 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
       orb_r_d_.alloc(n_vtx);
       orb_c_d_.alloc(n_vtx);
+      gmax_d_.alloc(2 * size_t(max_batch_));
       if (discGemmApplies(dims_, max_batch_)) {
         disc_.alloc(discScratchBytes(dims_, max_batch_));
         discInit(disc_ws_, dims_, max_batch_, disc_.get(), disc_.bytes());
@@ -425,6 +426,8 @@ void TpAccumulator::process() {
     ga.q_all = distinct == dims_.nc && int(q_list_.size()) == dims_.nc;
   }
   ga.disc = have_disc_ ? &disc_ws_ : nullptr;
+  ga.gmax = tc_front_ ? gmax_d_.get() : nullptr;
+  ga.n_sm = ftc_.n_sm;
   cudaEvent_t b = nullptr;
   timeBegin(DCAACC_STAGE_ROW, &b);
   if (tc_front_)
@@ -436,7 +439,7 @@ void TpAccumulator::process() {
   timeEnd(DCAACC_STAGE_ROW, b, 1);
   timeBegin(DCAACC_STAGE_COL, &b);
   if (tc_front_)
-    launchFrontendTcCol(fa, ftc_, G32_.get(), g_sector_stride_, err_d_.get(), stream_);
+    launchFrontendTcCol(fa, ftc_, G32_.get(), g_sector_stride_, gmax_d_.get(), err_d_.get(), stream_);
   else if (mixed_)
     launchColTransform<float>(fa, X32_.get(), G32_.get(), g_sector_stride_, stream_);
   else

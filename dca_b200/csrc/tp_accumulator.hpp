@@ -160,6 +160,7 @@ private:
   DevBuf<unsigned char> ftc_mem_;
   FrontTcWorkspace ftc_{};
   DevBuf<int> orb_r_d_, orb_c_d_;
+  DevBuf<int> gmax_d_;  // [2 slot + spin] largest |G| per sector (column step -> G4 kernel)
   // Pinned staging of the batch being assembled, double-buffered: the host fills one set while the
   // uploads from the other (queued behind the previous batch's kernels) are still pending.
   struct HostStage {

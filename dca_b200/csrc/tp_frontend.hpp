@@ -75,7 +75,8 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
 // X' = P M (one launch).
 void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* err, cudaStream_t stream);
 // G = X' Q^H + beta G0 delta into the block-layout G (one launch).
+// gmax (or null): [2 slot + spin] set to each sector's largest |G| (float bits).
 void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
-                         int* err, cudaStream_t stream);
+                         int* gmax, int* err, cudaStream_t stream);
 
 }  // namespace dcaacc

@@ -354,11 +354,14 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
 }
 
 void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
-                         int* err, cudaStream_t stream) {
+                         int* gmax, int* err, cudaStream_t stream) {
   const FrontTcShape& s = w.shape;
   GemmParams p = gemmParams(a, w, err);
   p.G = G;
   p.g_sector_stride = g_sector_stride;
+  p.gmax = gmax;
+  if (gmax)
+    DCAACC_CUDA_CHECK(cudaMemsetAsync(gmax, 0, sizeof(int) * size_t(a.n_sectors), stream));
   p.mt = s.Dq / kBM;  // rows of G^T: rho2
   p.nt = s.Dp / kBN;  // columns of G^T: rho1
   launchGemm<1>(p, w.tm_bq, w.tm_ac, w.n_sm, stream);

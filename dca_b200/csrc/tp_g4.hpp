@@ -24,6 +24,8 @@ struct G4Args {
   int* err;             // device error word (async_copy.cuh kErr* bits)
   bool q_all = false;             // q_list is a permutation of all Nc cluster momenta
   const struct DiscWorkspace* disc = nullptr;  // tensor-core disconnected-term workspace (or null)
+  const int* gmax = nullptr;  // [2 slot + spin] largest |G| of each sector as float bits (or null)
+  int n_sm = 0;               // multiprocessors (persistent grids)
 };
 
 // Workspace of the tensor-core disconnected-term GEMM (tp_g4_disc.cu): U / V operand planes, their
@@ -58,6 +60,12 @@ bool discGemmApplies(const TpDims& d, int max_batch);
 size_t discScratchBytes(const TpDims& d, int max_batch);
 void discInit(DiscWorkspace& w, const TpDims& d, int max_batch, void* mem, size_t bytes);
 const float2* launchDiscGemm(const G4Args& a, const float2* G, long g_sector_stride, cudaStream_t stream);
+
+// Tensor-core direct term (tp_g4_mma.cu): one band, Nc = 16, all momentum transfers, with the
+// disconnected terms precomputed (disc) and the per-sector maxima of G recorded by the column step.
+bool directTcApplies(const G4Args& a);
+void launchDirectTc(const G4Args& a, const float2* G, long g_sector_stride, const float2* disc, int n_sm,
+                    cudaStream_t stream);
 
 // G: block-layout G of n_slots measurements, sector (slot, spin) at g_sector_stride * (2 slot + spin).
 // Returns the number of kernels launched.

@@ -662,7 +662,9 @@ void launchDirect(const G4Args& a, const float2* G, long stride, const float2* d
 template <int NC>
 int launchForNc(const G4Args& a, const float2* G, long stride, bool mag, bool charge, cudaStream_t s) {
   if (const float2* disc = launchDiscGemm(a, G, stride, s)) {
-    if (a.q_all)
+    if (NC == 16 && directTcApplies(a))
+      launchDirectTc(a, G, stride, disc, a.n_sm, s);
+    else if (a.q_all)
       launchOuter<NC>(a, G, stride, disc, s);
     else
       launchDirect<NC>(a, G, stride, disc, s);
