@@ -417,28 +417,39 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
           break;
         mx = fmaxf(fmaxf(rb[cg], rb[4 + cg]), fmaxf(rb[8 + cg], rb[12 + cg]));
         if (live) {
+          // The warp's 32 rows x 32 columns go out per part (re hi, re lo, im hi, im lo) through
+          // 2 KB of shared memory: lane = row writes its 64-byte row segment (16-byte chunk c at
+          // c ^ ((row >> 1) & 3), conflict-free), then each store instruction writes eight whole
+          // row segments (lane: row 8 pass + lane / 4, chunk lane % 4).  The staging lies in the
+          // B-imaginary part of stages 0 and 1, which the row step's loads never fill.
           const int e = scaleExp(mx);
           const float sc = pow2f(e);
           const long kp = 2L * p.Kr;
           const long plane = static_cast<long>(p.Dp) * kp;
-          __half* o = p.ac + static_cast<long>(sec) * kPl * plane + static_cast<long>(rho) * kp + j0;
+          const int ew = warp - 2;
+          unsigned char* stg = base + (ew >> 3) * kStageStride + boxOff(3, 0) + (ew & 7) * 2048;
+          __half* o = p.ac + static_cast<long>(sec) * kPl * plane + static_cast<long>(mt * kBM + quarter * 32) * kp + j0;
 #pragma unroll
-          for (int g8 = 0; g8 < 4; ++g8) {
-            Pack8 h, l;
+          for (int part = 0; part < 4; ++part) {
+            __syncwarp();  // the previous part's reads of the staging are done
 #pragma unroll
-            for (int x = 0; x < 8; ++x) {
-              const Split2 a = split2f(ar[g8 * 8 + x], sc);
-              h.v[x] = a.h, l.v[x] = a.l;
+            for (int c = 0; c < 4; ++c) {
+              Pack8 h;
+#pragma unroll
+              for (int x = 0; x < 8; ++x) {
+                const Split2 s2 = split2f(part < 2 ? ar[c * 8 + x] : ai[c * 8 + x], sc);
+                h.v[x] = (part & 1) ? s2.l : s2.h;
+              }
+              store8(reinterpret_cast<__half*>(stg + lane * 64 + ((c ^ ((lane >> 1) & 3)) * 16)), h);
             }
-            store8(o + g8 * 8, h);
-            store8(o + plane + g8 * 8, l);
+            __syncwarp();
+            __half* op = o + (part & 1) * plane + (part >> 1) * p.Kr;
 #pragma unroll
-            for (int x = 0; x < 8; ++x) {
-              const Split2 b = split2f(ai[g8 * 8 + x], sc);
-              h.v[x] = b.h, l.v[x] = b.l;
+            for (int pass = 0; pass < 4; ++pass) {
+              const int r = pass * 8 + lane / 4, ch = lane & 3;
+              const uint4 w = *reinterpret_cast<const uint4*>(stg + r * 64 + ((ch ^ ((r >> 1) & 3)) * 16));
+              *reinterpret_cast<uint4*>(op + static_cast<long>(r) * kp + ch * 8) = w;
             }
-            store8(o + p.Kr + g8 * 8, h);
-            store8(o + plane + p.Kr + g8 * 8, l);
           }
           if (quarter == 0 && lane == 0)
             p.xInv[(static_cast<long>(sec) * xtiles + mt) * kxc + j0 / kBK] = pow2f(-e);
