@@ -372,7 +372,7 @@ def run_ours(args, world, rank, local):
         alg_bytes = len(w.channels) * n_g4 * 32 + B * 2 * D * D * 8
         sec = dom_ms / args.steps / 1e3  # the stage's time per batch (its kernels run back to back)
         roof = {"kernel": "update_g4 stage: discPlanesKernel + frontGemmKernel<2> (disconnected terms) + "
-                          "updateG4SinglebandOuter<16, 4, 4> (direct term, G4 flush)" if not simt else
+                          "updateG4DirectMma (direct term, G4 flush)" if not simt else
                           "updateG4SinglebandBatched", "bound": "hbm",
                 "achieved": alg_bytes / sec / 1e9, "peak": hbm_gbs, "unit": "GB/s",
                 "traffic": None, "peak_source": peak_src, "algorithmic_bytes": alg_bytes}
@@ -418,7 +418,7 @@ def run_ours(args, world, rank, local):
     roof["ms_per_launch"] = per_launch_ms
     # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the stage's kernels from the
     # committed ncu capture of this workload (one batch, cold caches), per launch of the stage.
-    stage_kernels = {"update_g4": ["discPlanesKernel", "frontGemmKernel<2>", "updateG4SinglebandOuter<16, 4, 4>"],
+    stage_kernels = {"update_g4": ["discPlanesKernel", "frontGemmKernel<2>", "updateG4DirectMma"],
                      "col_transform": ["frontGemmKernel<1>"], "row_transform": ["frontGemmKernel<0>"],
                      "twiddle": ["twiddleWiKernel", "buildPhaseOperandKernel<0>", "buildPhaseOperandKernel<1>",
                                  "buildMOperandKernel"]}.get(dom, [])

@@ -100,45 +100,70 @@ class TpParameters:
         return (nb, nb, nb, nb, nc, nw, nc, nw, len(self.k_ex), len(self.w_ex))
 
 
-def _addr(a: np.ndarray) -> int:
-    return a.__array_interface__["data"][0]
+# dcaacc_sector as a numpy record (same layout as the C struct and _native.Sector), so that the
+# descriptors of a whole batch are filled with a few vectorised assignments.
+_SECTOR_FIELDS = ("n", "tau", "left_band", "right_band", "left_site", "right_site", "M", "ldm", "m_on_device")
+_SECTOR_DTYPE = np.dtype({
+    "names": list(_SECTOR_FIELDS),
+    "formats": ["<i4", "<u8", "<u8", "<u8", "<u8", "<u8", "<u8", "<i4", "<i4"],
+    "offsets": [getattr(N.Sector, f).offset for f in _SECTOR_FIELDS],
+    "itemsize": ctypes.sizeof(N.Sector),
+})
+_VERTEX_INTS = ("left_band", "right_band", "left_site", "right_site")
 
 
-def _fill_sector(sec, M, c, keep: list):
-    tau = np.ascontiguousarray(c.tau, np.float64)
-    n = int(tau.shape[0])
-    bands_sites = [np.ascontiguousarray(getattr(c, name), np.int32)
-                   for name in ("left_band", "right_band", "left_site", "right_site")]
-    keep.append(tau)
-    keep.extend(bands_sites)
-    sec.n = n
-    sec.tau = _addr(tau)
-    sec.left_band, sec.right_band, sec.left_site, sec.right_site = (_addr(a) for a in bands_sites)
-    if hasattr(M, "is_cuda") and M.is_cuda:
-        import torch
+def _device_matrix(M, n: int, keep: list):
+    """(pointer, ldm) of a device float64 matrix, made column major if needed."""
+    import torch
 
-        if M.dtype != torch.float64:
-            raise LogicError("device M must be float64")
-        if n and not (M.stride(0) == 1 and M.stride(1) >= max(n, 1)):
-            M = M.t().contiguous().t()  # column major
+    if M.dtype != torch.float64:
+        raise LogicError("device M must be float64")
+    if n and not (M.stride(0) == 1 and M.stride(1) >= max(n, 1)):
+        M = M.t().contiguous().t()  # column major
         keep.append(M)
-        sec.M = M.data_ptr()
-        sec.ldm = max(M.stride(1), 1) if n else 1
-        sec.m_on_device = 1
-    else:
-        Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
-        keep.append(Mh)
-        sec.M = _addr(Mh)
-        sec.ldm = max(n, 1)
-        sec.m_on_device = 0
+    return M.data_ptr(), (max(M.stride(1), 1) if n else 1)
 
 
 def _make_sectors(M_pair, configs, keep: list, count: int = 1):
-    """Sector descriptors for `count` measurements: M_pair / configs hold 2 * count entries."""
-    secs = (N.Sector * (2 * count))()
-    for s in range(2 * count):
-        _fill_sector(secs[s], M_pair[s], configs[s], keep)
-    return secs
+    """Sector descriptors for `count` measurements (M_pair / configs hold 2 * count entries), as a
+    pointer to dcaacc_sector records.  The vertex arrays of all sectors are packed into one
+    float64 and one int32 buffer; everything the pointers refer to is appended to `keep`."""
+    ns = 2 * count
+    taus = [c.tau for c in configs]
+    lens = np.fromiter((len(t) for t in taus), np.int64, ns)
+    offs = np.zeros(ns, np.int64)
+    np.cumsum(lens[:-1], out=offs[1:])
+    total = int(lens.sum())
+    width = max(total, 1)
+    tau_all = np.zeros(width, np.float64)
+    ints = np.zeros((len(_VERTEX_INTS), width), np.int32)
+    if total:
+        np.concatenate(taus, out=tau_all[:total], casting="unsafe")
+        for k, name in enumerate(_VERTEX_INTS):
+            np.concatenate([getattr(c, name) for c in configs], out=ints[k, :total], casting="unsafe")
+    rec = np.zeros(ns, _SECTOR_DTYPE)
+    rec["n"] = lens
+    rec["tau"] = tau_all.ctypes.data + 8 * offs
+    for k, name in enumerate(_VERTEX_INTS):
+        rec[name] = ints.ctypes.data + 4 * (k * width + offs)
+    ptr = np.zeros(ns, np.uint64)
+    ldm = np.ones(ns, np.int32)
+    dev = np.zeros(ns, np.int32)
+    for s in range(ns):
+        M, n = M_pair[s], int(lens[s])
+        if hasattr(M, "is_cuda") and M.is_cuda:
+            ptr[s], ldm[s] = _device_matrix(M, n, keep)
+            dev[s] = 1
+        else:
+            Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
+            keep.append(Mh)
+            ptr[s] = Mh.ctypes.data
+            ldm[s] = max(n, 1)
+    rec["M"] = ptr
+    rec["ldm"] = ldm
+    rec["m_on_device"] = dev
+    keep.extend((tau_all, ints, rec, M_pair))
+    return rec.ctypes.data_as(ctypes.POINTER(N.Sector))
 
 
 class TpAccumulator:

@@ -84,8 +84,11 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   DCAACC_CUDA_CHECK(cudaGetDevice(&device_));
   DCAACC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   own_stream_ = true;
+  DCAACC_CUDA_CHECK(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
   for (auto& h : hstage_)
     DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&h.uploaded, cudaEventDisableTiming));
+  for (auto& d : dstage_)
+    DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&d.consumed, cudaEventDisableTiming));
 
   // ---- G0 slice over the extended mesh (tp_accumulator_base.hpp:210-221) ----
   {
@@ -149,17 +152,19 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   const size_t n_sec = 2 * size_t(max_batch_);
   const size_t n_vtx = n_sec * max_order_;
   const size_t n_orb1 = dims_.n_orb + 1;
-  sectors_d_.alloc(n_sec);
-  tau_d_.alloc(n_vtx);
-  perm_r_d_.alloc(n_vtx);
-  perm_c_d_.alloc(n_vtx);
-  rstart_d_.alloc(n_sec * n_orb1);
-  cstart_d_.alloc(n_sec * n_orb1);
-  signs_d_.alloc(max_batch_);
+  for (auto& d : dstage_) {
+    d.sectors.alloc(n_sec);
+    d.tau.alloc(n_vtx);
+    d.perm_r.alloc(n_vtx);
+    d.perm_c.alloc(n_vtx);
+    d.rstart.alloc(n_sec * n_orb1);
+    d.cstart.alloc(n_sec * n_orb1);
+    d.signs.alloc(max_batch_);
+    d.M.alloc(n_sec * size_t(max_order_) * max_order_);
+  }
   Tr_d_.alloc(n_vtx * nw_ext);
   if (non_density_)
     Tc_d_.alloc(n_vtx * nw_ext);
-  M_d_.alloc(n_sec * size_t(max_order_) * max_order_);
   const size_t x_elems = n_sec * size_t(R) * max_order_ * nw_ext;
   const size_t g_elems = n_sec * size_t(g_sector_stride_);
   if (mixed_) {
@@ -179,8 +184,10 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
       // Padding rows stay zero; ordered before the scale kernel frontTcInit launches on stream_.
       DCAACC_CUDA_CHECK(cudaMemsetAsync(ftc_mem_.get(), 0, ftc_mem_.bytes(), stream_));
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
-      orb_r_d_.alloc(n_vtx);
-      orb_c_d_.alloc(n_vtx);
+      for (auto& d : dstage_) {
+        d.orb_r.alloc(n_vtx);
+        d.orb_c.alloc(n_vtx);
+      }
       gmax_d_.alloc(2 * size_t(max_batch_));
       if (discGemmApplies(dims_, max_batch_)) {
         disc_.alloc(discScratchBytes(dims_, max_batch_));
@@ -203,8 +210,10 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
     h.signs.alloc(max_batch_);
     h.orb_r.alloc(n_vtx);
     h.orb_c.alloc(n_vtx);
-    DCAACC_CUDA_CHECK(cudaEventRecord(h.uploaded, stream_));
+    DCAACC_CUDA_CHECK(cudaEventRecord(h.uploaded, copy_stream_));
   }
+  for (auto& d : dstage_)
+    DCAACC_CUDA_CHECK(cudaEventRecord(d.consumed, stream_));
 
   if (!tc_front_ && frontendSmemRequirement(dims_, max_order_, !mixed_) > 227 * 1024)
     invalid("max_order too large for the front-end's shared-memory tiles");
@@ -214,6 +223,8 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
 TpAccumulator::~TpAccumulator() {
   if (stream_)
     cudaStreamSynchronize(stream_);
+  if (copy_stream_)
+    cudaStreamSynchronize(copy_stream_);
   for (auto& t : timed_) {
     cudaEventDestroy(t.begin);
     cudaEventDestroy(t.end);
@@ -221,6 +232,11 @@ TpAccumulator::~TpAccumulator() {
   for (auto& h : hstage_)
     if (h.uploaded)
       cudaEventDestroy(h.uploaded);
+  for (auto& d : dstage_)
+    if (d.consumed)
+      cudaEventDestroy(d.consumed);
+  if (copy_stream_)
+    cudaStreamDestroy(copy_stream_);
   if (own_stream_ && stream_)
     cudaStreamDestroy(stream_);
 }
@@ -283,8 +299,11 @@ double TpAccumulator::flopEstimate(const dcaacc_sector* sec) const {
 }
 
 void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
-  if (slots_ == 0)
+  if (slots_ == 0) {
     DCAACC_CUDA_CHECK(cudaEventSynchronize(hs().uploaded));  // this staging set is free again
+    // Copies into this device set wait for the kernels of the batch that last used it.
+    DCAACC_CUDA_CHECK(cudaStreamWaitEvent(copy_stream_, dstage_[hset_].consumed, 0));
+  }
   const int slot = slots_;
   const int n_orb = dims_.n_orb;
   for (int s = 0; s < 2; ++s) {
@@ -332,9 +351,12 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
     const double* Mptr = x.M;
     int ldm = std::max(x.ldm, 1);
     if (n && !x.m_on_device) {
-      double* dst = M_d_.get() + size_t(sidx) * max_order_ * max_order_;
-      DCAACC_CUDA_CHECK(cudaMemcpy2DAsync(dst, sizeof(double) * n, x.M, sizeof(double) * x.ldm,
-                                          sizeof(double) * n, n, cudaMemcpyHostToDevice, stream_));
+      double* dst = dstage_[hset_].M.get() + size_t(sidx) * max_order_ * max_order_;
+      if (x.ldm == n)
+        DCAACC_CUDA_CHECK(cudaMemcpyAsync(dst, x.M, sizeof(double) * n * n, cudaMemcpyHostToDevice, copy_stream_));
+      else
+        DCAACC_CUDA_CHECK(cudaMemcpy2DAsync(dst, sizeof(double) * n, x.M, sizeof(double) * x.ldm,
+                                            sizeof(double) * n, n, cudaMemcpyHostToDevice, copy_stream_));
       Mptr = dst;
       ldm = n;
     }
@@ -361,34 +383,38 @@ void TpAccumulator::process() {
     return;
   const int n_sec = 2 * slots_;
   const int n_orb1 = dims_.n_orb + 1;
+  // Uploads on the copy stream (after the kernels that last read this device set, see stage());
+  // the kernels below wait for them.
+  DevStage& ds = dstage_[hset_];
   auto h2d = [&](void* dst, const void* src, size_t bytes) {
     if (bytes)
-      DCAACC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_));
+      DCAACC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, copy_stream_));
   };
-  h2d(sectors_d_.get(), hs().sectors.get(), sizeof(SectorDesc) * n_sec);
-  h2d(tau_d_.get(), hs().tau.get(), sizeof(double) * vtx_used_);
-  h2d(perm_r_d_.get(), hs().perm_r.get(), sizeof(int) * vtx_used_);
-  h2d(perm_c_d_.get(), hs().perm_c.get(), sizeof(int) * vtx_used_);
-  h2d(rstart_d_.get(), hs().rstart.get(), sizeof(int) * n_sec * n_orb1);
-  h2d(cstart_d_.get(), hs().cstart.get(), sizeof(int) * n_sec * n_orb1);
-  h2d(signs_d_.get(), hs().signs.get(), sizeof(int) * slots_);
+  h2d(ds.sectors.get(), hs().sectors.get(), sizeof(SectorDesc) * n_sec);
+  h2d(ds.tau.get(), hs().tau.get(), sizeof(double) * vtx_used_);
+  h2d(ds.perm_r.get(), hs().perm_r.get(), sizeof(int) * vtx_used_);
+  h2d(ds.perm_c.get(), hs().perm_c.get(), sizeof(int) * vtx_used_);
+  h2d(ds.rstart.get(), hs().rstart.get(), sizeof(int) * n_sec * n_orb1);
+  h2d(ds.cstart.get(), hs().cstart.get(), sizeof(int) * n_sec * n_orb1);
+  h2d(ds.signs.get(), hs().signs.get(), sizeof(int) * slots_);
   if (tc_front_) {
-    h2d(orb_r_d_.get(), hs().orb_r.get(), sizeof(int) * vtx_used_);
-    h2d(orb_c_d_.get(), (non_density_ ? hs().orb_c : hs().orb_r).get(), sizeof(int) * vtx_used_);
+    h2d(ds.orb_r.get(), hs().orb_r.get(), sizeof(int) * vtx_used_);
+    h2d(ds.orb_c.get(), (non_density_ ? hs().orb_c : hs().orb_r).get(), sizeof(int) * vtx_used_);
   }
-  DCAACC_CUDA_CHECK(cudaEventRecord(hs().uploaded, stream_));
+  DCAACC_CUDA_CHECK(cudaEventRecord(hs().uploaded, copy_stream_));
+  DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, hs().uploaded, 0));
   hset_ ^= 1;
 
   FrontendArgs fa{};
   fa.dims = dims_;
-  fa.sectors = sectors_d_.get();
+  fa.sectors = ds.sectors.get();
   fa.n_sectors = n_sec;
   fa.n_max = n_max_batch_;
-  fa.tau = tau_d_.get();
-  fa.perm_r = perm_r_d_.get();
-  fa.perm_c = non_density_ ? perm_c_d_.get() : perm_r_d_.get();
-  fa.row_start = rstart_d_.get();
-  fa.col_start = non_density_ ? cstart_d_.get() : rstart_d_.get();
+  fa.tau = ds.tau.get();
+  fa.perm_r = ds.perm_r.get();
+  fa.perm_c = non_density_ ? ds.perm_c.get() : ds.perm_r.get();
+  fa.row_start = ds.rstart.get();
+  fa.col_start = non_density_ ? ds.cstart.get() : ds.rstart.get();
   fa.Tr = Tr_d_.get();
   fa.Tc = non_density_ ? Tc_d_.get() : Tr_d_.get();
   fa.Fb = Fb_.get();
@@ -398,7 +424,7 @@ void TpAccumulator::process() {
     timeBegin(DCAACC_STAGE_TWIDDLE, &b);
     int n_prep;
     if (tc_front_) {
-      n_prep = launchFrontendTcPrep(fa, ftc_, orb_r_d_.get(), orb_c_d_.get(), stream_);
+      n_prep = launchFrontendTcPrep(fa, ftc_, ds.orb_r.get(), ds.orb_c.get(), stream_);
     }
     else {
       launchTwiddles(fa, stream_);
@@ -409,7 +435,7 @@ void TpAccumulator::process() {
   }
   G4Args ga{};
   ga.dims = dims_;
-  ga.signs = signs_d_.get();
+  ga.signs = ds.signs.get();
   ga.n_slots = slots_;
   ga.k_add = k_add_d_.get();
   ga.k_sub = k_sub_d_.get();
@@ -450,6 +476,7 @@ void TpAccumulator::process() {
                                  : launchUpdateG4<double2>(ga, G64_.get(), g_sector_stride_, stream_);
   timeEnd(DCAACC_STAGE_G4, b, g4_launches);
   launches_ += 2 + g4_launches;
+  DCAACC_CUDA_CHECK(cudaEventRecord(ds.consumed, stream_));
   have_g_ = !mixed_;
   slots_ = 0;
   vtx_used_ = 0;
@@ -635,18 +662,20 @@ void TpAccumulator::setStream(cudaStream_t s) {
 }
 
 void TpAccumulator::synchronize() {
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(copy_stream_));  // host M copies of a pending batch
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
   checkDeviceError();
 }
 
 size_t TpAccumulator::deviceFingerprint() const {
   size_t b = G0_.bytes() + Fb_.bytes() + k_add_d_.bytes() + k_sub_d_.bytes() + q_d_.bytes() +
-             wex_d_.bytes() + G4_ptrs_.bytes() + sectors_d_.bytes() + tau_d_.bytes() +
-             M_d_.bytes() + perm_r_d_.bytes() + perm_c_d_.bytes() + rstart_d_.bytes() +
-             cstart_d_.bytes() + signs_d_.bytes() + Tr_d_.bytes() + Tc_d_.bytes() + X64_.bytes() +
+             wex_d_.bytes() + G4_ptrs_.bytes() + Tr_d_.bytes() + Tc_d_.bytes() + X64_.bytes() +
              G64_.bytes() + X32_.bytes() + G32_.bytes() + err_d_.bytes();
   for (const auto& g : G4_)
     b += g.bytes();
+  for (const auto& d : dstage_)
+    b += d.sectors.bytes() + d.tau.bytes() + d.M.bytes() + d.perm_r.bytes() + d.perm_c.bytes() +
+         d.rstart.bytes() + d.cstart.bytes() + d.signs.bytes() + d.orb_r.bytes() + d.orb_c.bytes();
   return b;
 }
 

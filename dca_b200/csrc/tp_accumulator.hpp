@@ -145,9 +145,16 @@ private:
   DevBuf<double2*> G4_ptrs_;
   DevBuf<int> err_d_;  // kernels' error word (async_copy.cuh kErr* bits)
   // Batch workspace.
-  DevBuf<SectorDesc> sectors_d_;
-  DevBuf<double> tau_d_, M_d_;
-  DevBuf<int> perm_r_d_, perm_c_d_, rstart_d_, cstart_d_, signs_d_;
+  // Per-batch device inputs, double-buffered like the pinned staging below: batch k + 1 is uploaded
+  // on copy_stream_ while batch k's kernels run on stream_ (events order the reuse of a set).
+  struct DevStage {
+    DevBuf<SectorDesc> sectors;
+    DevBuf<double> tau, M;  // M: host-resident sectors' matrices, copied in
+    DevBuf<int> perm_r, perm_c, rstart, cstart, signs, orb_r, orb_c;
+    cudaEvent_t consumed = nullptr;  // the kernels that read this set have completed
+  };
+  DevStage dstage_[2];
+  cudaStream_t copy_stream_ = nullptr;
   DevBuf<double2> Tr_d_, Tc_d_;
   DevBuf<double2> X64_, G64_;  // FP64 mode
   DevBuf<float2> X32_, G32_;   // mixed mode
@@ -159,7 +166,6 @@ private:
   bool tc_front_ = false;
   DevBuf<unsigned char> ftc_mem_;
   FrontTcWorkspace ftc_{};
-  DevBuf<int> orb_r_d_, orb_c_d_;
   DevBuf<int> gmax_d_;  // [2 slot + spin] largest |G| per sector (column step -> G4 kernel)
   // Pinned staging of the batch being assembled, double-buffered: the host fills one set while the
   // uploads from the other (queued behind the previous batch's kernels) are still pending.
