@@ -115,10 +115,13 @@ EXTRA_WORKLOADS = {"sq2_allq": _small_all_transfers(("square", 2), 1),
 @pytest.mark.parametrize("wname,n_meas,max_batch", [("c1", 6, 4), ("sq2_allq", 5, 4), ("betts8_allq", 5, 4),
                                                      ("c3", 9, 4), ("c3", 70, 72)])
 def test_tensor_core_disconnected_terms_match_oracle(oracle_lib, monkeypatch, wname, n_meas, max_batch):
-    """The one-band PH update with its disconnected terms on tcgen05 (split BF16, FP32 accumulate)
+    """The one-band PH update with its disconnected terms on tcgen05 (split FP16, FP32 accumulate)
     against the all-SIMT update and an FP64 reference: the oracle for c1, the FP64 GPU path (pinned
-    to the oracle above) for c3.  (c3, 70, 72) takes two K chunks in the GEMM (batch padded to
-    128); c1 (M = 64) pads the rows to one 128-row tile."""
+    to the oracle above) for c3.  (c3, 70, 72) takes three K chunks in the GEMM and, in the
+    tensor-core direct term (Nc = 16), eight full 8-measurement steps and a partial one, with the
+    G4 flush of each tile spread over the next tile's steps; (c3, 9, 4) runs single partial steps
+    (batches of 4 and 1), whose flush chunks outnumber the steps.  c1 (M = 64) pads the rows to
+    one 128-row tile."""
     case = case_from_workload(EXTRA_WORKLOADS.get(wname) or W.WORKLOADS[wname], n_meas)
     tc = _run_timed(case, False, monkeypatch, max_batch=max_batch)
     simt = _run_timed(case, True, monkeypatch, max_batch=max_batch)
