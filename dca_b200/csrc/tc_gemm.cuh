@@ -132,12 +132,13 @@ __device__ inline float2 addDeltaInPlace(const GemmParams& p, const SectorDesc& 
 template <int MODE>
 __device__ inline void tileOf(const GemmParams& p, int t, int& sec, int& mt, int& nt, int& chunks) {
   if (MODE == 0) {
-    // Row step: column tiles (j) slowest.  Tiles with j beyond a sector's order are skipped, and
-    // with the column tile slowest they spread evenly over the persistent CTAs (with it fastest,
-    // a CTA would keep meeting the same column tile).
-    const int per = p.n_sectors * p.mt;
-    nt = t / per;
-    sec = (t % per) / p.mt;
+    // Row step: (sector, column tile, row tile), row tiles fastest.  The eight row tiles that
+    // share an M tile run at once, and the few column tiles of a sector, which re-read its P row
+    // tiles, follow each other closely enough for those reads to hit L2.  Tiles with j beyond a
+    // sector's order are skipped; a CTA's tiles (stride = grid) still visit every column tile.
+    const int per = p.mt * p.nt;
+    sec = t / per;
+    nt = (t % per) / p.mt;
     mt = t % p.mt;
   }
   else {
