@@ -66,22 +66,30 @@ struct Split2 {
 };
 // y = x * 2^e (scale given as the exact power of two) = h + l with |y - h - l| <= 2^-22 |y|,
 // both parts rounded to nearest.
-__device__ inline Split2 split2d(double x, double scale) {
-  const double y = x * scale;
-  const __half h = __double2half(y);
-  return {h, __double2half(y - static_cast<double>(__half2float(h)))};
-}
 __device__ inline Split2 split2f(float x, float scale) {
   const float y = x * scale;
   const __half h = __float2half_rn(y);
   return {h, __float2half_rn(y - __half2float(h))};
 }
 
-struct Pack8 {
+struct alignas(16) Pack8 {
   __half v[8];
 };
 __device__ inline void store8(__half* dst, const Pack8& p) {
   *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(&p);
+}
+
+// Eight values already scaled into FP16 range, y = hi + lo with both parts rounded to nearest
+// (|y - hi - lo| <= 2^-22 |y|): one packed conversion per pair for hi, one for lo.
+__device__ inline void split8(const float (&y)[8], Pack8& hi, Pack8& lo) {
+  __half2* h = reinterpret_cast<__half2*>(hi.v);
+  __half2* l = reinterpret_cast<__half2*>(lo.v);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    h[q] = __floats2half2_rn(y[2 * q], y[2 * q + 1]);
+    const float2 f = __half22float2(h[q]);
+    l[q] = __floats2half2_rn(y[2 * q] - f.x, y[2 * q + 1] - f.y);
+  }
 }
 
 __device__ inline double2 zmul(double2 a, double2 b) {

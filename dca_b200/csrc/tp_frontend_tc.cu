@@ -165,6 +165,7 @@ buildPhaseOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sector
       const int rho = r + R * w;
       const double sc = pow2d(es[rho]);
       Pack8 re[kPl], im[kPl];
+      float yr[8], yi[8];  // the FP64 products, scaled, rounded once to FP32 and then split
 #pragma unroll
       for (int x = 0; x < 8; ++x) {
         const double2 ph = zmul(Fb[(bv[x] * nc + k) * nc + xv[x]], tv[x]);
@@ -176,10 +177,11 @@ buildPhaseOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sector
           const double2 g = g0s[bv[x] + nb * (b + nb * (k + nc * w))];
           z = zmul(ph, make_double2(g.x * qscale, -g.y * qscale));
         }
-        const Split2 a = split2d(z.x, sc), c = split2d(z.y, sc);
-        re[0].v[x] = a.h, re[1].v[x] = a.l;
-        im[0].v[x] = c.h, im[1].v[x] = c.l;
+        yr[x] = static_cast<float>(z.x * sc);
+        yi[x] = static_cast<float>(z.y * sc);
       }
+      split8(yr, re[0], re[1]);
+      split8(yi, im[0], im[1]);
 #pragma unroll
       for (int pl = 0; pl < kPl; ++pl) {
         __half* op = o + pl * plane + static_cast<long>(rho) * kp + grp * 8;
@@ -218,13 +220,13 @@ buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restric
     const double sc = pow2d(e);
     for (int grp = lane; grp < groups; grp += 32) {
       Pack8 v[kPl];
+      float y[8];
 #pragma unroll
       for (int x = 0; x < 8; ++x) {
         const int i = grp * 8 + x;
-        const double m = (col && i < n) ? col[perm_r[sd.vtx_off + i]] : 0.;
-        const Split2 s = split2d(m, sc);
-        v[0].v[x] = s.h, v[1].v[x] = s.l;
+        y[x] = static_cast<float>(((col && i < n) ? col[perm_r[sd.vtx_off + i]] : 0.) * sc);
       }
+      split8(y, v[0], v[1]);
 #pragma unroll
       for (int pl = 0; pl < kPl; ++pl)
         store8(o + pl * plane + static_cast<long>(j) * Kr + grp * 8, v[pl]);
