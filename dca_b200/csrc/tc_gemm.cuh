@@ -102,6 +102,7 @@ struct GemmParams {
   int n_sectors;
   int D, Dp, Kr;
   int mt, nt;           // row and column tiles per sector
+  int mt0, nt0;         // index of the first row / column tile
   const int* eP;        // [spin][Dp] row exponents of P
   const int* eQ;        // [spin][Dp] row exponents of Q
   const float* mInv;    // [sector][Kr] 2^-e of M's rows j (row step's output columns)
@@ -147,14 +148,14 @@ __device__ inline void tileOf(const GemmParams& p, int t, int& sec, int& mt, int
     const int per = p.mt * p.nt;
     sec = t / per;
     nt = (t % per) / p.mt;
-    mt = t % p.mt;
+    mt = p.mt0 + t % p.mt;
   }
   else {
     const int per = p.mt * p.nt;
     sec = t / per;
     const int rem = t % per;
     mt = rem / p.nt;
-    nt = rem % p.nt;
+    nt = p.nt0 + rem % p.nt;
   }
   if (MODE == 2) {
     chunks = (p.n_slots + kBK - 1) / kBK;

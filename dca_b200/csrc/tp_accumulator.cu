@@ -78,6 +78,21 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   q_list_.assign(c.k_ex, c.k_ex + c.n_k_ex);
   wex_list_.assign(c.w_ex, c.w_ex + c.n_w_ex);
   g4_size_ = size_t(nb) * nb * nb * nb * nc * nc * nw * nw * c.n_k_ex * c.n_w_ex;
+  // -k for the mirror-symmetric G of the mixed path: the identity z of the momentum group
+  // (k_add[z + Nc k] = k for all k), then -k = z - k = k_sub[k + Nc z].
+  std::vector<int> kneg;
+  if (nc <= kMaxMirrorNc)
+    for (int z = 0; z < nc && kneg.empty(); ++z) {
+      bool id = true;
+      for (int k = 0; k < nc; ++k)
+        id = id && k_add_[z + nc * k] == k;
+      if (id)
+        for (int k = 0; k < nc; ++k)
+          kneg.push_back(k_sub_[k + nc * z]);
+    }
+  bool mirror_ok = !kneg.empty();
+  for (size_t k = 0; k < kneg.size(); ++k)
+    mirror_ok = mirror_ok && kneg[kneg[k]] == int(k);
   const long R = dims_.R;
   g_sector_stride_ = long(nw_ext) * nw_ext * R * R;
 
@@ -106,6 +121,22 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
             }
     G0_.alloc(g0.size());
     DCAACC_CUDA_CHECK(cudaMemcpy(G0_.get(), g0.data(), G0_.bytes(), cudaMemcpyHostToDevice));
+    // Mirror symmetry G0(-k, -w) = conj G0(k, w) (one band; time-reversal symmetric models).
+    if (mirror_ok && nb == 1) {
+      double mx = 0, dev = 0;
+      for (int s = 0; s < 2; ++s)
+        for (int w = 0; w < nw_ext; ++w)
+          for (int k = 0; k < nc; ++k) {
+            const double2 a = g0[k + size_t(nc) * (w + size_t(nw_ext) * s)];
+            const double2 b = g0[kneg[k] + size_t(nc) * (nw_ext - 1 - w + size_t(nw_ext) * s)];
+            mx = std::max(mx, std::hypot(a.x, a.y));
+            dev = std::max(dev, std::hypot(a.x - b.x, a.y + b.y));
+          }
+      mirror_ok = dev <= 1e-12 * mx;
+    }
+    else {
+      mirror_ok = false;
+    }
   }
   // ---- cluster transform with band phases: Fb(r, k, b) = e^{i k.r} e^{i k.a_b}
   // (space_transform_2D.hpp:93-140) ----
@@ -125,6 +156,13 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
       }
     Fb_.alloc(fb.size());
     DCAACC_CUDA_CHECK(cudaMemcpy(Fb_.get(), fb.data(), Fb_.bytes(), cudaMemcpyHostToDevice));
+    // The cluster transform must map -k to the conjugate phases as well.
+    if (mirror_ok)
+      for (int k = 0; k < nc; ++k)
+        for (int r = 0; r < nc; ++r) {
+          const double2 a = fb[size_t(k) * nc + r], b = fb[size_t(kneg[k]) * nc + r];
+          mirror_ok = mirror_ok && std::hypot(a.x - b.x, a.y + b.y) <= 1e-12;
+        }
   }
   auto upload_ints = [](DevBuf<int>& d, const std::vector<int>& h) {
     d.alloc(h.size());
@@ -193,6 +231,22 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
         disc_.alloc(discScratchBytes(dims_, max_batch_));
         discInit(disc_ws_, dims_, max_batch_, disc_.get(), disc_.bytes());
         have_disc_ = true;
+      }
+      // Half G (mirror symmetry) when the tensor-core direct term reads every G of the batch:
+      // one band, Nc = 16, all momentum transfers, and half of D a whole number of 128-row tiles.
+      // DCAACC_TP_FULL_G=1 computes the whole of G instead (for comparisons).
+      std::vector<int> seen(nc, 0);
+      int distinct = 0;
+      for (int q : q_list_)
+        distinct += seen[q]++ == 0;
+      const bool q_all = distinct == nc && int(q_list_.size()) == nc;
+      const char* full_env = std::getenv("DCAACC_TP_FULL_G");
+      const bool full_g = full_env && std::strcmp(full_env, "1") == 0;
+      if (have_disc_ && mirror_ok && !full_g && nb == 1 && nc == kMaxMirrorNc && q_all && c.n_channels <= 2 &&
+          nw_ext % 2 == 0 && (long(R) * nw_ext / 2) % 128 == 0) {
+        dims_.half_g = 1;
+        for (int k = 0; k < nc; ++k)
+          dims_.kneg[k] = static_cast<unsigned char>(kneg[k]);
       }
     }
   }

@@ -145,10 +145,11 @@ buildPhaseOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sector
   const double2* Ts = T + static_cast<long>(sd.vtx_off) * nw_ext;
   const int* es = eRow + sd.spin * Dp;
   const double qscale = -1.0 / nc;
-  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * nw_ext;
+  const int w_lo = ROW && dims.half_g ? nw_ext / 2 : 0;  // half G: P rows of the upper half only
+  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * (nw_ext - w_lo);
        idx += long(gridDim.x) * blockDim.x) {
     const int grp = static_cast<int>(idx % groups);
-    const int w = static_cast<int>(idx / groups);
+    const int w = w_lo + static_cast<int>(idx / groups);
     double2 tv[8];
     int bv[8], xv[8];
 #pragma unroll
@@ -350,7 +351,8 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
   if (a.n_max == 0)
     return;
   GemmParams p = gemmParams(a, w, err);
-  p.mt = s.Dp / kBM;
+  p.mt0 = a.dims.half_g ? s.D / 2 / kBM : 0;  // half G: X' rows of the upper frequency half only
+  p.mt = s.Dp / kBM - p.mt0;
   p.nt = (a.n_max + kBN - 1) / kBN;
   launchGemm<0>(p, w.tm_pr, w.tm_mb, w.n_sm, stream);
 }
@@ -364,8 +366,9 @@ void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float
   p.gmax = gmax;
   if (gmax)
     DCAACC_CUDA_CHECK(cudaMemsetAsync(gmax, 0, sizeof(int) * size_t(a.n_sectors), stream));
-  p.mt = s.Dq / kBM;  // rows of G^T: rho2
-  p.nt = s.Dp / kBN;  // columns of G^T: rho1
+  p.mt = s.Dq / kBM;                          // rows of G^T: rho2
+  p.nt0 = a.dims.half_g ? s.D / 2 / kBN : 0;  // columns of G^T: rho1 (half G: the upper half)
+  p.nt = s.Dp / kBN - p.nt0;
   launchGemm<1>(p, w.tm_bq, w.tm_ac, w.n_sm, stream);
 }
 

@@ -60,7 +60,7 @@ discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_
                  const int* __restrict__ signs, int n_slots, int Kb, int Mp, const int* __restrict__ k_add,
                  const int* __restrict__ q_list, const int* __restrict__ wex_list, __half* __restrict__ Up,
                  __half* __restrict__ Vp, int* __restrict__ eU, int* __restrict__ eV) {
-  const int nc = dims.nc, nw_ext = dims.nw_ext, ext = dims.ext, R = dims.R;
+  const int nc = dims.nc, ext = dims.ext;
   const int M = nc * dims.nw;
   const int p = blockIdx.y;
   const int ch = blockIdx.z;
@@ -79,13 +79,14 @@ discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_
     const int row = static_cast<int>(idx / groups);
     const int slot0 = grp * 8;
     long bc = 0, be = 0;
+    bool cc = false, ce = false;  // read from the conjugated mirror (half G)
     const bool in_row = row < M;
     if (in_row) {
       const int k = row % nc, w = row / nc;
       const int kq = k_add[k + nc * q];
       const int we = w + ext, wx = we + wex;
-      bc = (static_cast<long>(we) * nw_ext + wx) * R * R + static_cast<long>(k) * R + kq;
-      be = (static_cast<long>(wx) * nw_ext + we) * R * R + static_cast<long>(kq) * R + k;
+      bc = gIndexMirrored(dims, we, wx, k, kq, cc);
+      be = gIndexMirrored(dims, wx, we, kq, k, ce);
     }
     float2 u[8], v[8];
     float mu = 0.f, mv = 0.f;
@@ -97,7 +98,15 @@ discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_
         const float hs = 0.5f * static_cast<float>(signs[slot]);
         const float2* G0s = G + g_sector_stride * (2 * slot);
         const float2* G1s = G0s + g_sector_stride;
-        const float2 c0 = G0s[bc], c1 = G1s[bc], e0 = G0s[be], e1 = G1s[be];
+        float2 c0 = G0s[bc], c1 = G1s[bc], e0 = G0s[be], e1 = G1s[be];
+        if (cc) {
+          c0.y = -c0.y;
+          c1.y = -c1.y;
+        }
+        if (ce) {
+          e0.y = -e0.y;
+          e1.y = -e1.y;
+        }
         u[e] = make_float2(hs * (c0.x + sg * c1.x), hs * (c0.y + sg * c1.y));
         v[e] = make_float2(e0.x + sg * e1.x, e0.y + sg * e1.y);
       }

@@ -30,6 +30,12 @@
 // (conflict-free both ways) so that consecutive threads touch consecutive k1 of G4 and of the
 // disconnected terms, as in the SIMT kernel.
 //
+// Half G (dims.half_g): a block whose row frequency lies in the lower half is not stored; the
+// producer copies its mirror (w' = NwExt - 1 - w on both frequencies) and the consumers read
+// element (k1, k2) as the conjugate of the mirror's (-k1, -k2).  So that the gathers stay
+// conflict-free, a mirrored A block takes MMA row i as k2 = -i and a mirrored B block takes MMA
+// column n as l1 = -n (the mirror's element then sits in column i / n again).
+//
 // Every mbarrier wait is bounded (async_copy.cuh); after a timeout a warp stops waiting and
 // computing but still takes part in the two named barriers per tile, so no thread can be left
 // waiting, and the host reports the error word.
@@ -63,7 +69,8 @@ constexpr uint32_t kOffExp = kOffBars + 2 * kStages * 8;
 constexpr uint32_t kOffKplus = kOffExp + 4 * kMaxSteps;
 constexpr uint32_t kOffKsub = kOffKplus + kBlk;
 constexpr uint32_t kOffQinv = kOffKsub + kBlk;
-constexpr uint32_t kOffSigns = kOffQinv + 16;
+constexpr uint32_t kOffKneg = kOffQinv + 16;
+constexpr uint32_t kOffSigns = kOffKneg + 16;
 constexpr size_t kSmem = kOffSigns + kMaxSteps * kMeasPerStep;
 constexpr int kExpMax = 60;  // |e| <= 60 keeps 2^{+-2e} a normal FP32 number
 constexpr int kMaxCh = 2;    // PH-magnetic and PH-charge
@@ -97,7 +104,8 @@ __device__ inline void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t 
 // split into FP16 hi / lo.  FULL: all eight measurements of the step exist (no predicates).
 template <bool FULL>
 __device__ __forceinline__ void buildFragments(const float2* S, const int (&oa)[2], const int (&ob)[2], int t4,
-                                               int m0, int n_slots, const signed char* sgn, float sc,
+                                               int m0, int n_slots, const signed char* sgn, float sc, float ca,
+                                               float cb,
                                                uint32_t (&arh)[4], uint32_t (&arl)[4], uint32_t (&aih)[4],
                                                uint32_t (&ail)[4], uint32_t (&brh)[2][2], uint32_t (&brl)[2][2],
                                                uint32_t (&bih)[2][2], uint32_t (&bil)[2][2]) {
@@ -107,6 +115,7 @@ __device__ __forceinline__ void buildFragments(const float2* S, const int (&oa)[
     const bool valid = FULL || m0 + mi < n_slots;
     const float fa = valid ? -0.5f * static_cast<float>(sgn[m0 + mi]) * sc : 0.f;
     const float fb = valid ? sc : 0.f;
+    const float fai = fa * ca, fbi = fb * cb;  // imaginary parts (conjugated mirrors: negated)
     const float2* slot = S + mi * (kSlotBytes / sizeof(float2));
     const float2 z = make_float2(0.f, 0.f);
 #pragma unroll
@@ -114,11 +123,11 @@ __device__ __forceinline__ void buildFragments(const float2* S, const int (&oa)[
       const float2 a0 = valid ? slot[oa[r]] : z;
       const float2 a1 = valid ? slot[2 * kBlk + oa[r]] : z;
       splitPair(a0.x * fa, a1.x * fa, arh[2 * j + r], arl[2 * j + r]);
-      splitPair(a0.y * fa, a1.y * fa, aih[2 * j + r], ail[2 * j + r]);
+      splitPair(a0.y * fai, a1.y * fai, aih[2 * j + r], ail[2 * j + r]);
       const float2 b0 = valid ? slot[kBlk + ob[r]] : z;
       const float2 b1 = valid ? slot[3 * kBlk + ob[r]] : z;
       splitPair(b0.x * fb, b1.x * fb, brh[r][j], brl[r][j]);
-      splitPair(b0.y * fb, b1.y * fb, bih[r][j], bil[r][j]);
+      splitPair(b0.y * fbi, b1.y * fbi, bih[r][j], bil[r][j]);
     }
   }
 }
@@ -168,6 +177,7 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
   unsigned char* kplus = smem + kOffKplus;  // [d][i] -> k1 with k1 - d = i
   unsigned char* ksub = smem + kOffKsub;    // [a + 16 b] = b - a
   unsigned char* qinv = smem + kOffQinv;    // q -> its position in q_list
+  unsigned char* kneg = smem + kOffKneg;    // k -> -k (half G)
   signed char* sgn = reinterpret_cast<signed char*>(smem + kOffSigns);  // [m] measurement signs
 
   const int t = threadIdx.x, warp = t / 32, lane = t % 32;
@@ -181,8 +191,10 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
     ksub[e] = static_cast<unsigned char>(s);
     kplus[a * kNc + s] = static_cast<unsigned char>(b);  // d = a, k1 = b, i = b - d
   }
-  for (int e = t; e < kNc; e += kThreads)
+  for (int e = t; e < kNc; e += kThreads) {
     qinv[q_list[e]] = static_cast<unsigned char>(e);
+    kneg[e] = dims.half_g ? dims.kneg[e] : static_cast<unsigned char>(e);
+  }
   for (int m = t; m < n_slots; m += kThreads)
     sgn[m] = static_cast<signed char>(signs[m]);
   for (int step = warp; step < n_steps; step += kThreads / 32) {
@@ -212,8 +224,12 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
       tilePair(tile % (nw * nw), nw, w1, w2);
       const int wex = wex_list[tile / (nw * nw)];
       const int w1e = w1 + dims.ext, w2e = w2 + dims.ext, w1x = w1e + wex, w2x = w2e + wex;
-      const long b_A = (static_cast<long>(w1e) * nw_ext + w2e) * kBlk;
-      const long b_B = (static_cast<long>(w2x) * nw_ext + w1x) * kBlk;
+      // A = block (w1e, w2e), B = block (w2x, w1x), or their mirrors (half G).
+      const bool mir_a = dims.half_g && 2 * w1e < nw_ext, mir_b = dims.half_g && 2 * w2x < nw_ext;
+      const long b_A = mir_a ? (static_cast<long>(nw_ext - 1 - w1e) * nw_ext + nw_ext - 1 - w2e) * kBlk
+                             : (static_cast<long>(w1e) * nw_ext + w2e) * kBlk;
+      const long b_B = mir_b ? (static_cast<long>(nw_ext - 1 - w2x) * nw_ext + nw_ext - 1 - w1x) * kBlk
+                             : (static_cast<long>(w2x) * nw_ext + w1x) * kBlk;
       for (int step = 0; step < n_steps; ++step, ++gs) {
         const int st = gs % kStages, use = gs / kStages;
         if (use > 0 && !__all_sync(0xffffffffu, mbarWait(&empty[st], (use - 1) & 1, err))) {
@@ -243,15 +259,6 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
   // ---- consumer warps: warp d = warp
   const int d = warp;
   const int g = lane >> 2, t4 = lane & 3;
-  // Fragment gathers (float2 offsets inside a staged block).
-  int oa[2], ob[2];
-#pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int i = g + 8 * r;                 // MMA row: k2 = i, k1 = i + d
-    oa[r] = kplus[d * kNc + i] * kNc + i;    // A[k1][k2]
-    const int l1 = g + 8 * r;                // MMA column (N tile r): l1
-    ob[r] = ksub[d + kNc * l1] * kNc + l1;   // B[l1 - d][l1]
-  }
   const long M = static_cast<long>(kNc) * nw;
   const long s_w1 = kNc, s_k2 = s_w1 * nw, s_w2 = s_k2 * kNc, s_q = s_w2 * nw, s_wq = s_q * nq;
   const int n_ch = dims.n_channels;
@@ -301,6 +308,21 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
     int w1, w2;
     tilePair(tile % (nw * nw), nw, w1, w2);
     const int iwq = tile / (nw * nw);
+    const int w1e = w1 + dims.ext, w2x = w2 + dims.ext + wex_list[iwq];
+    const bool mir_a = dims.half_g && 2 * w1e < nw_ext, mir_b = dims.half_g && 2 * w2x < nw_ext;
+    // Fragment gathers (float2 offsets inside a staged block).  MMA row i: k2 = i (mirrored: -i),
+    // k1 = k2 + d, element A[k1][k2] (mirrored: A'[-k1][i]); MMA column n (N tile r): l1 = n
+    // (mirrored: -n), element B[l1 - d][l1] (mirrored: B'[-(l1 - d)][n]).
+    int oa[2], ob[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int i = g + 8 * r;
+      const int k2 = mir_a ? kneg[i] : i, k1 = kplus[d * kNc + k2];
+      oa[r] = (mir_a ? kneg[k1] : k1) * kNc + i;
+      const int l1 = mir_b ? kneg[i] : i, lr = ksub[d + kNc * l1];
+      ob[r] = (mir_b ? kneg[lr] : lr) * kNc + i;
+    }
+    const float ca = mir_a ? -1.f : 1.f, cb = mir_b ? -1.f : 1.f;  // conjugation of the mirrors
     float acc_re[2][4], acc_im[2][4];
 #pragma unroll
     for (int n = 0; n < 2; ++n)
@@ -329,9 +351,11 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
         uint32_t arh[4], arl[4], aih[4], ail[4];
         uint32_t brh[2][2], brl[2][2], bih[2][2], bil[2][2];
         if (m0 + kMeasPerStep <= n_slots)
-          buildFragments<true>(S, oa, ob, t4, m0, n_slots, sgn, sc, arh, arl, aih, ail, brh, brl, bih, bil);
+          buildFragments<true>(S, oa, ob, t4, m0, n_slots, sgn, sc, ca, cb, arh, arl, aih, ail, brh, brl, bih,
+                               bil);
         else
-          buildFragments<false>(S, oa, ob, t4, m0, n_slots, sgn, sc, arh, arl, aih, ail, brh, brl, bih, bil);
+          buildFragments<false>(S, oa, ob, t4, m0, n_slots, sgn, sc, ca, cb, arh, arl, aih, ail, brh, brl, bih,
+                                bil);
         uint32_t naih[4], nail[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -404,10 +428,11 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
       for (int n = 0; n < 2; ++n)
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          const int i = g + 8 * (k >> 1), l1 = 8 * n + 2 * t4 + (k & 1);
-          const int k1 = kplus[d * kNc + i];
+          const int i = g + 8 * (k >> 1), nn = 8 * n + 2 * t4 + (k & 1);
+          const int k2 = mir_a ? kneg[i] : i, k1 = kplus[d * kNc + k2];
+          const int l1 = mir_b ? kneg[nn] : nn;
           const int qi = qinv[ksub[k1 + kNc * l1]];
-          table[(qi * kNc + i) * kNc + (k1 ^ qi)] = make_float2(acc_re[n][k], acc_im[n][k]);
+          table[(qi * kNc + k2) * kNc + (k1 ^ qi)] = make_float2(acc_re[n][k], acc_im[n][k]);
         }
     }
     namedSync();  // the table is complete

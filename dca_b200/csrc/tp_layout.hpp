@@ -26,7 +26,26 @@ struct TpDims {
   int n_channels;
   int channels[kMaxChannels];
   double beta;
+  // Mixed path, one band, Nc <= kMaxMirrorNc: G rows of the lower frequency half (w1 < nw_ext / 2)
+  // are not computed; G(k1 w1; k2 w2) = conj G(-k1 w1'; -k2 w2') with w' = nw_ext - 1 - w (real M
+  // and G0(-k, -w) = conj G0(k, w)), and the consumers read that mirror instead.
+  int half_g;
+  unsigned char kneg[16];  // index of -k (half_g only)
 };
+constexpr int kMaxMirrorNc = 16;
+
+// Index of element (k1 w1; k2 w2) of a one-band block-layout G (R = Nc) and whether it is stored
+// conjugated there (half_g: the lower-half rows are read from their mirror).
+__host__ __device__ inline long gIndexMirrored(const TpDims& d, int w1, int w2, int k1, int k2, bool& conj) {
+  conj = d.half_g && 2 * w1 < d.nw_ext;
+  if (conj) {
+    w1 = d.nw_ext - 1 - w1;
+    w2 = d.nw_ext - 1 - w2;
+    k1 = d.kneg[k1];
+    k2 = d.kneg[k2];
+  }
+  return ((static_cast<long>(w1) * d.nw_ext + w2) * d.R + k1) * d.R + k2;
+}
 
 // One spin sector of one measurement, as the kernels see it after host-side sorting.
 struct SectorDesc {

@@ -135,6 +135,24 @@ def test_tensor_core_disconnected_terms_match_oracle(oracle_lib, monkeypatch, wn
         assert rel_err(ref, want) <= MIXED_TOL
 
 
+@pytest.mark.parametrize("n_meas,max_batch", [(9, 8), (3, 4)])
+def test_half_g_matches_full_g(monkeypatch, n_meas, max_batch):
+    """c3 (Nc = 16, all transfers, one band, G0(-k, -w) = conj G0(k, w)) computes only the upper
+    frequency half of G and reads the rest as its conjugated mirror; DCAACC_TP_FULL_G=1 computes
+    all of G.  Both against the FP64 path, and against each other."""
+    case = case_from_workload(W.WORKLOADS["c3"], n_meas)
+    monkeypatch.setenv("DCAACC_TP_FULL_G", "0")
+    half = _run_timed(case, False, monkeypatch, max_batch=max_batch)
+    monkeypatch.setenv("DCAACC_TP_FULL_G", "1")
+    full = _run_timed(case, False, monkeypatch, max_batch=max_batch)
+    exact = run_gpu(case, precision=0, max_batch=1)
+    for h, f, want in zip(half.get_G4(), full.get_G4(), exact.get_G4()):
+        print("half / full G relative errors:", rel_err(h, want), rel_err(f, want))
+        assert rel_err(h, want) <= MIXED_TOL
+        assert rel_err(f, want) <= MIXED_TOL
+        assert rel_err(h, f) <= MIXED_TOL
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_sum_to_equals_single_accumulator(precision):
     case, _ = golden("sq2_all")
