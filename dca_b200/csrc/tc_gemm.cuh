@@ -154,7 +154,7 @@ __device__ inline void tileOf(const GemmParams& p, int t, int& sec, int& mt, int
     const int per = p.mt * p.nt;
     sec = t / per;
     const int rem = t % per;
-    mt = rem / p.nt;
+    mt = p.mt0 + rem / p.nt;
     nt = p.nt0 + rem % p.nt;
   }
   if (MODE == 2) {

@@ -247,6 +247,45 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
         dims_.half_g = 1;
         for (int k = 0; k < nc; ++k)
           dims_.kneg[k] = static_cast<unsigned char>(kneg[k]);
+        // Half G4 when the transfer lists are closed under negation.
+        std::vector<int> qm(q_list_.size(), -1), wm(wex_list_.size(), -1);
+        for (size_t i = 0; i < q_list_.size(); ++i)
+          for (size_t j = 0; j < q_list_.size(); ++j)
+            if (q_list_[j] == kneg[q_list_[i]])
+              qm[i] = int(j);
+        for (size_t i = 0; i < wex_list_.size(); ++i)
+          for (size_t j = 0; j < wex_list_.size(); ++j)
+            if (wex_list_[j] == -wex_list_[i])
+              wm[i] = int(j);
+        const bool closed = std::count(qm.begin(), qm.end(), -1) == 0 && std::count(wm.begin(), wm.end(), -1) == 0;
+        if (closed && nw % 2 == 0 && (nc * nw / 2) % 128 == 0) {
+          dims_.half_g4 = 1;
+          upload_ints(q_mirror_d_, qm);
+          upload_ints(wq_mirror_d_, wm);
+          // Tiles (w1, w2) with w1 >= Nw / 2, each next to the tile that reads its B block as A:
+          // (w2, w1) if w2 >= Nw / 2, else the mirror (Nw - 1 - w2, Nw - 1 - w1).
+          std::vector<char> seen(size_t(nw) * nw, 0);
+          std::vector<unsigned> order;
+          auto push = [&](int a, int b) {
+            if (!seen[size_t(a) * nw + b]) {
+              seen[size_t(a) * nw + b] = 1;
+              order.push_back(unsigned(a) | (unsigned(b) << 16));
+            }
+          };
+          for (int a = nw / 2; a < nw; ++a)
+            for (int b = 0; b < nw; ++b) {
+              if (seen[size_t(a) * nw + b])
+                continue;
+              push(a, b);
+              if (2 * b >= nw)
+                push(b, a);
+              else
+                push(nw - 1 - b, nw - 1 - a);
+            }
+          tile_order_d_.alloc(order.size());
+          DCAACC_CUDA_CHECK(cudaMemcpy(tile_order_d_.get(), order.data(), tile_order_d_.bytes(),
+                                       cudaMemcpyHostToDevice));
+        }
       }
     }
   }
@@ -507,6 +546,7 @@ void TpAccumulator::process() {
   }
   ga.disc = have_disc_ ? &disc_ws_ : nullptr;
   ga.gmax = tc_front_ ? gmax_d_.get() : nullptr;
+  ga.tile_order = dims_.half_g4 ? tile_order_d_.get() : nullptr;
   ga.n_sm = ftc_.n_sm;
   cudaEvent_t b = nullptr;
   timeBegin(DCAACC_STAGE_ROW, &b);
@@ -566,6 +606,8 @@ void TpAccumulator::finalize() {
     return;
   process();
   for (size_t c = 0; c < G4_.size(); ++c) {
+    if (dims_.half_g4)  // the entries with w1 < Nw / 2 from their mirrors
+      launchG4Mirror(G4_[c].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), stream_);
     G4_host_[c].resize(g4_size_);
     DCAACC_CUDA_CHECK(cudaMemcpyAsync(G4_host_[c].data(), G4_[c].get(), G4_[c].bytes(),
                                       cudaMemcpyDeviceToHost, stream_));
@@ -702,8 +744,15 @@ void TpAccumulator::peekG4(int channel, size_t offset, size_t count, double* out
   if (offset > g4_size_ || count > g4_size_ - offset)
     invalid("window outside G4");
   process();
-  DCAACC_CUDA_CHECK(cudaMemcpyAsync(out, G4_[channel].get() + offset, 16 * count,
-                                    cudaMemcpyDeviceToHost, stream_));
+  const double2* src = G4_[channel].get() + offset;
+  if (dims_.half_g4) {  // entries with w1 < Nw / 2 come from their mirrors
+    if (peek_d_.size() < count)
+      peek_d_.alloc(count);
+    launchG4Window(G4_[channel].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), offset, count, peek_d_.get(),
+                   stream_);
+    src = peek_d_.get();
+  }
+  DCAACC_CUDA_CHECK(cudaMemcpyAsync(out, src, 16 * count, cudaMemcpyDeviceToHost, stream_));
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 

@@ -167,6 +167,11 @@ private:
   DevBuf<unsigned char> ftc_mem_;
   FrontTcWorkspace ftc_{};
   DevBuf<int> gmax_d_;  // [2 slot + spin] largest |G| per sector (column step -> G4 kernel)
+  // Half G4 (dims_.half_g4): positions of -q / -wq in the transfer lists, the tiles the update
+  // runs, and a device window for peeks.
+  DevBuf<int> q_mirror_d_, wq_mirror_d_;
+  DevBuf<unsigned> tile_order_d_;
+  DevBuf<double2> peek_d_;
   // Pinned staging of the batch being assembled, double-buffered: the host fills one set while the
   // uploads from the other (queued behind the previous batch's kernels) are still pending.
   struct HostStage {

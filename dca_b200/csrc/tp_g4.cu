@@ -464,6 +464,78 @@ __global__ void addAndClearKernel(double2* __restrict__ dst, double2* __restrict
 }
 }  // namespace
 
+namespace {
+
+// G4 entry index (one band: k1 + Nc (w1 + Nw (k2 + Nc (w2 + Nw (iq + Nq iwq))))) of the mirror of
+// entry e, and whether e lies in the lower half (w1 < Nw / 2) that the mirror provides.
+__device__ inline bool g4Mirror(const TpDims& d, const int* q_mirror, const int* wq_mirror, size_t e, size_t& m) {
+  const int nc = d.nc, nw = d.nw;
+  size_t r = e;
+  const int k1 = static_cast<int>(r % nc);
+  r /= nc;
+  const int w1 = static_cast<int>(r % nw);
+  r /= nw;
+  const int k2 = static_cast<int>(r % nc);
+  r /= nc;
+  const int w2 = static_cast<int>(r % nw);
+  r /= nw;
+  const int iq = static_cast<int>(r % d.nq);
+  const int iwq = static_cast<int>(r / d.nq);
+  if (2 * w1 >= nw)
+    return false;
+  m = d.kneg[k1] + nc * (nw - 1 - w1 + size_t(nw) * (d.kneg[k2] + nc * (nw - 1 - w2 +
+      size_t(nw) * (q_mirror[iq] + size_t(d.nq) * wq_mirror[iwq]))));
+  return true;
+}
+
+__global__ void g4MirrorKernel(double2* __restrict__ G4, const TpDims d, const int* __restrict__ q_mirror,
+                               const int* __restrict__ wq_mirror, size_t n) {
+  for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
+    size_t m;
+    if (g4Mirror(d, q_mirror, wq_mirror, e, m)) {
+      const double2 v = G4[m];
+      G4[e] = make_double2(v.x, -v.y);
+    }
+  }
+}
+
+__global__ void g4WindowKernel(const double2* __restrict__ G4, const TpDims d, const int* __restrict__ q_mirror,
+                               const int* __restrict__ wq_mirror, size_t offset, size_t count,
+                               double2* __restrict__ out) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x) {
+    size_t m;
+    if (d.half_g4 && g4Mirror(d, q_mirror, wq_mirror, offset + i, m)) {
+      const double2 v = G4[m];
+      out[i] = make_double2(v.x, -v.y);
+    }
+    else {
+      out[i] = G4[offset + i];
+    }
+  }
+}
+
+size_t g4Entries(const TpDims& d) {
+  return size_t(d.nb) * d.nb * d.nb * d.nb * d.nc * d.nc * d.nw * d.nw * d.nq * d.nwq;
+}
+
+}  // namespace
+
+void launchG4Mirror(double2* G4, const TpDims& d, const int* q_mirror, const int* wq_mirror, cudaStream_t stream) {
+  const size_t n = g4Entries(d);
+  const int blocks = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16));
+  g4MirrorKernel<<<blocks, 256, 0, stream>>>(G4, d, q_mirror, wq_mirror, n);
+  DCAACC_LAUNCH_CHECK();
+}
+
+void launchG4Window(const double2* G4, const TpDims& d, const int* q_mirror, const int* wq_mirror, size_t offset,
+                    size_t count, double2* out, cudaStream_t stream) {
+  if (!count)
+    return;
+  const int blocks = static_cast<int>(std::min<size_t>((count + 255) / 256, 148 * 16));
+  g4WindowKernel<<<blocks, 256, 0, stream>>>(G4, d, q_mirror, wq_mirror, offset, count, out);
+  DCAACC_LAUNCH_CHECK();
+}
+
 void launchAddAndClear(double2* dst, double2* src, size_t n, cudaStream_t stream) {
   if (!n)
     return;

@@ -26,6 +26,7 @@ struct G4Args {
   const struct DiscWorkspace* disc = nullptr;  // tensor-core disconnected-term workspace (or null)
   const int* gmax = nullptr;  // [2 slot + spin] largest |G| of each sector as float bits (or null)
   int n_sm = 0;               // multiprocessors (persistent grids)
+  const unsigned* tile_order = nullptr;  // half_g4: the (w1 | w2 << 16) tiles to update, mirror pairs adjacent
 };
 
 // Workspace of the tensor-core disconnected-term GEMM (tp_g4_disc.cu): U / V operand planes, their
@@ -66,6 +67,13 @@ const float2* launchDiscGemm(const G4Args& a, const float2* G, long g_sector_str
 bool directTcApplies(const G4Args& a);
 void launchDirectTc(const G4Args& a, const float2* G, long g_sector_stride, const float2* disc, int n_sm,
                     cudaStream_t stream);
+
+// half_g4: G4 entries with w1 < Nw / 2 := conj of their mirror (-k1 w1', -k2 w2', -q, -wq);
+// q_mirror[iq] / wq_mirror[iwq] are the positions of -q / -wq in the transfer lists.
+void launchG4Mirror(double2* G4, const TpDims& d, const int* q_mirror, const int* wq_mirror, cudaStream_t stream);
+// Entries [offset, offset + count) of G4 with the mirror applied (half_g4) into out (device).
+void launchG4Window(const double2* G4, const TpDims& d, const int* q_mirror, const int* wq_mirror, size_t offset,
+                    size_t count, double2* out, cudaStream_t stream);
 
 // G: block-layout G of n_slots measurements, sector (slot, spin) at g_sector_stride * (2 slot + spin).
 // Returns the number of kernels launched.

@@ -200,7 +200,8 @@ const float2* launchDiscGemm(const G4Args& a, const float2* G, long g_sector_str
   p.D = s.M;
   p.Dp = s.Mp;
   p.Kr = s.Kb;
-  p.mt = s.Mp / kBM;
+  p.mt0 = d.half_g4 ? s.M / 2 / kBM : 0;  // half G4: the rows (k1, w1) with w1 >= Nw / 2 only
+  p.mt = s.Mp / kBM - p.mt0;
   p.nt = s.Mp / kBN;
   p.err = a.err;
   p.n_slots = a.n_slots;

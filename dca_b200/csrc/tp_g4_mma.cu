@@ -167,8 +167,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
                   const int* __restrict__ signs, int n_slots, const int* __restrict__ k_sub,
                   const int* __restrict__ q_list, const int* __restrict__ wex_list,
-                  const int* __restrict__ gmax, const float2* __restrict__ disc, double2* const* __restrict__ G4,
-                  bool atomic, int* __restrict__ err) {
+                  const int* __restrict__ gmax, const unsigned* __restrict__ tile_order,
+                  const float2* __restrict__ disc, double2* const* __restrict__ G4, bool atomic,
+                  int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem[];
   float2* table = reinterpret_cast<float2*>(smem + kOffTable);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOffBars);
@@ -182,7 +183,18 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
 
   const int t = threadIdx.x, warp = t / 32, lane = t % 32;
   const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq;
-  const int n_tiles = nw * nw * dims.nwq;
+  const int per_wq = dims.half_g4 ? nw * nw / 2 : nw * nw;  // half G4: the tiles with w1 >= Nw / 2
+  const int n_tiles = per_wq * dims.nwq;
+  auto tileOf = [&](int tile, int& w1, int& w2) {
+    if (dims.half_g4) {
+      const unsigned v = tile_order[tile % per_wq];
+      w1 = static_cast<int>(v & 0xffffu);
+      w2 = static_cast<int>(v >> 16);
+    }
+    else {
+      tilePair(tile % per_wq, nw, w1, w2);
+    }
+  };
   const int n_steps = (n_slots + kMeasPerStep - 1) / kMeasPerStep;
 
   for (int e = t; e < kBlk; e += kThreads) {
@@ -221,8 +233,8 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
     bool ok = true;
     for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
       int w1, w2;
-      tilePair(tile % (nw * nw), nw, w1, w2);
-      const int wex = wex_list[tile / (nw * nw)];
+      tileOf(tile, w1, w2);
+      const int wex = wex_list[tile / per_wq];
       const int w1e = w1 + dims.ext, w2e = w2 + dims.ext, w1x = w1e + wex, w2x = w2e + wex;
       // A = block (w1e, w2e), B = block (w2x, w1x), or their mirrors (half G).
       const bool mir_a = dims.half_g && 2 * w1e < nw_ext, mir_b = dims.half_g && 2 * w2x < nw_ext;
@@ -306,8 +318,8 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
   bool ok = true;
   for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     int w1, w2;
-    tilePair(tile % (nw * nw), nw, w1, w2);
-    const int iwq = tile / (nw * nw);
+    tileOf(tile, w1, w2);
+    const int iwq = tile / per_wq;
     const int w1e = w1 + dims.ext, w2x = w2 + dims.ext + wex_list[iwq];
     const bool mir_a = dims.half_g && 2 * w1e < nw_ext, mir_b = dims.half_g && 2 * w2x < nw_ext;
     // Fragment gathers (float2 offsets inside a staged block).  MMA row i: k2 = i (mirrored: -i),
@@ -460,10 +472,11 @@ void launchDirectTc(const G4Args& a, const float2* G, long g_sector_stride, cons
   const TpDims& d = a.dims;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(updateG4DirectMma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(kSmem)));
-  const long tiles = long(d.nw) * d.nw * d.nwq;
+  const long tiles = long(d.nw) * d.nw * d.nwq / (d.half_g4 ? 2 : 1);
   const unsigned grid = static_cast<unsigned>(std::max(1L, std::min<long>(tiles, n_sm)));
   updateG4DirectMma<<<grid, kThreads, kSmem, stream>>>(d, G, g_sector_stride, a.signs, a.n_slots, a.k_sub,
-                                                       a.q_list, a.wex_list, a.gmax, disc, a.G4, a.atomic, a.err);
+                                                       a.q_list, a.wex_list, a.gmax, a.tile_order, disc, a.G4,
+                                                       a.atomic, a.err);
   DCAACC_LAUNCH_CHECK();
 }
 

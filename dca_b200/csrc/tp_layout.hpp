@@ -31,6 +31,11 @@ struct TpDims {
   // and G0(-k, -w) = conj G0(k, w)), and the consumers read that mirror instead.
   int half_g;
   unsigned char kneg[16];  // index of -k (half_g only)
+  // With half_g, and momentum and frequency transfers closed under negation, G4 itself obeys
+  // G4(-k1 w1', -k2 w2', -q, -wq) = conj G4(k1 w1, k2 w2, q, wq) (w' = Nw - 1 - w): the update
+  // accumulates the frequency tiles with w1 >= Nw / 2 only and the rest is filled from them when
+  // G4 is read (finalize, peek).
+  int half_g4;
 };
 constexpr int kMaxMirrorNc = 16;
 
