@@ -113,6 +113,7 @@ def _load():
         "dcaacc_tp_synchronize": (i, [p]),
         "dcaacc_tp_device_fingerprint": (sz, [p]),
         "dcaacc_tp_kernel_launches": (c_uint64, [p]),
+        "dcaacc_tp_mirror_mode": (i, [p]),
         "dcaacc_tp_enable_timing": (i, [p, i]),
         "dcaacc_tp_stage_times": (i, [p, POINTER(c_double), POINTER(c_uint64), i]),
         "dcaacc_tp_peek_g4": (i, [p, i, sz, sz, POINTER(c_double)]),

@@ -281,6 +281,10 @@ class TpAccumulator:
     def kernel_launches(self) -> int:
         return N.lib.dcaacc_tp_kernel_launches(self._h)
 
+    def mirror_mode(self) -> int:
+        """Bit 0: half of G computed (mirror symmetry); bit 1: half of the G4 tiles accumulated."""
+        return N.lib.dcaacc_tp_mirror_mode(self._h)
+
     STAGES = ("twiddle", "row_transform", "col_transform", "update_g4")
 
     def enable_timing(self, on: bool = True):

@@ -154,6 +154,10 @@ size_t dcaacc_tp_device_fingerprint(const dcaacc_tp* acc) {
   return acc ? acc->impl.deviceFingerprint() : 0;
 }
 
+int32_t dcaacc_tp_mirror_mode(const dcaacc_tp* acc) {
+  return acc ? acc->impl.mirrorMode() : 0;
+}
+
 uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc) {
   return acc ? acc->impl.kernelLaunches() : 0;
 }

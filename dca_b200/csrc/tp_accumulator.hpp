@@ -108,6 +108,9 @@ public:
   }
   void synchronize();
   size_t deviceFingerprint() const;
+  int mirrorMode() const {
+    return (dims_.half_g ? 1 : 0) | (dims_.half_g4 ? 2 : 0);
+  }
   uint64_t kernelLaunches() const {
     return launches_;
   }

@@ -164,6 +164,11 @@ size_t dcaacc_tp_device_fingerprint(const dcaacc_tp* acc);
 /* Number of this library's kernels launched by the handle since creation. */
 uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc);
 
+/* Which mirror symmetries the mixed path uses (no reference counterpart; monitoring): bit 0, only
+ * the upper frequency half of G is computed (real M and G0(-k,-w) = conj G0(k,w)); bit 1, only
+ * the G4 tiles with w1 >= Nw/2 are accumulated and the rest is their conjugated mirror. */
+int32_t dcaacc_tp_mirror_mode(const dcaacc_tp* acc);
+
 /* Stage timers, the counterpart of the reference's Profiler scopes in the accumulator
  * ("Frequency FT", "Space FT", "ComputeG", "updateG4": tp_accumulator_cpu.hpp:236-280,
  * tp_accumulator_gpu_base.hpp:214-219).  When enabled, CUDA events bracket each launch on the

@@ -138,14 +138,17 @@ def test_tensor_core_disconnected_terms_match_oracle(oracle_lib, monkeypatch, wn
 @pytest.mark.parametrize("n_meas,max_batch", [(9, 8), (3, 4)])
 def test_half_g_matches_full_g(monkeypatch, n_meas, max_batch):
     """c3 (Nc = 16, all transfers, one band, G0(-k, -w) = conj G0(k, w)) computes only the upper
-    frequency half of G and reads the rest as its conjugated mirror; DCAACC_TP_FULL_G=1 computes
-    all of G.  Both against the FP64 path, and against each other."""
+    frequency half of G and reads the rest as its conjugated mirror, and accumulates only the G4
+    tiles with w1 >= Nw/2 (the rest is their mirror, filled at finalize); DCAACC_TP_FULL_G=1
+    computes all of G and G4.  Both against the FP64 path, and against each other (with exactly
+    conjugate-symmetric inputs the two agree to the last bit)."""
     case = case_from_workload(W.WORKLOADS["c3"], n_meas)
     monkeypatch.setenv("DCAACC_TP_FULL_G", "0")
     half = _run_timed(case, False, monkeypatch, max_batch=max_batch)
     monkeypatch.setenv("DCAACC_TP_FULL_G", "1")
     full = _run_timed(case, False, monkeypatch, max_batch=max_batch)
     exact = run_gpu(case, precision=0, max_batch=1)
+    assert half.mirror_mode() == 3 and full.mirror_mode() == 0 and exact.mirror_mode() == 0
     for h, f, want in zip(half.get_G4(), full.get_G4(), exact.get_G4()):
         print("half / full G relative errors:", rel_err(h, want), rel_err(f, want))
         assert rel_err(h, want) <= MIXED_TOL
