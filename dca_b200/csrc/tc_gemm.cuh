@@ -79,6 +79,19 @@ __device__ inline void store8(__half* dst, const Pack8& p) {
   *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(&p);
 }
 
+// Four values already scaled into FP16 range, y = hi + lo (as split8), packed as 4 halves each.
+__device__ inline void split4(const float (&y)[4], uint2& hi, uint2& lo) {
+  __half2 h[2], l[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    h[q] = __floats2half2_rn(y[2 * q], y[2 * q + 1]);
+    const float2 f = __half22float2(h[q]);
+    l[q] = __floats2half2_rn(y[2 * q] - f.x, y[2 * q + 1] - f.y);
+  }
+  hi = make_uint2(*reinterpret_cast<uint32_t*>(&h[0]), *reinterpret_cast<uint32_t*>(&h[1]));
+  lo = make_uint2(*reinterpret_cast<uint32_t*>(&l[0]), *reinterpret_cast<uint32_t*>(&l[1]));
+}
+
 // Eight values already scaled into FP16 range, y = hi + lo with both parts rounded to nearest
 // (|y - hi - lo| <= 2^-22 |y|): one packed conversion per pair for hi, one for lo.
 __device__ inline void split8(const float (&y)[8], Pack8& hi, Pack8& lo) {

@@ -193,6 +193,82 @@ buildPhaseOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sector
   }
 }
 
+// Density-density models (the same vertex order on both sides): P and Q from one pass, sharing
+// the phase product Fb(b_i, k, x_i) T(w, i).  Thread per (w, 4 vertices) (4 rather than 8 keeps the
+// FP64 state small enough for 4 blocks per SM); Q for every row, P for the rows the row step reads
+// (half G: the upper frequency half).
+__global__ void __launch_bounds__(256)
+buildPhasePairKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, const double2* __restrict__ T,
+                     const int* __restrict__ orb, const double2* __restrict__ Fb, const double2* __restrict__ G0,
+                     const int* __restrict__ eP, const int* __restrict__ eQ, int Dp, int Dq, int Kr,
+                     __half* __restrict__ outP, __half* __restrict__ outQ) {
+  const SectorDesc sd = sectors[blockIdx.y];
+  const int n = sd.n;
+  const int groups = (n + kBK - 1) / kBK * (kBK / 4);
+  const int nb = dims.nb, nc = dims.nc, R = dims.R, nw_ext = dims.nw_ext;
+  const long kp = 2L * Kr;
+  const long planeP = static_cast<long>(Dp) * kp, planeQ = static_cast<long>(Dq) * kp;
+  __half* oP = outP + static_cast<long>(blockIdx.y) * kPl * planeP;
+  __half* oQ = outQ + static_cast<long>(blockIdx.y) * kPl * planeQ;
+  const double2* g0s = G0 + static_cast<long>(sd.spin) * nw_ext * nc * nb * nb;
+  const double2* Ts = T + static_cast<long>(sd.vtx_off) * nw_ext;
+  const int* esP = eP + sd.spin * Dp;
+  const int* esQ = eQ + sd.spin * Dp;
+  const double qscale = -1.0 / nc;
+  const int w_lo = dims.half_g ? nw_ext / 2 : 0;
+  for (long idx = blockIdx.x * long(blockDim.x) + threadIdx.x; idx < long(groups) * nw_ext;
+       idx += long(gridDim.x) * blockDim.x) {
+    const int grp = static_cast<int>(idx % groups);
+    const int w = static_cast<int>(idx / groups);
+    const bool doP = w >= w_lo;
+    double2 tv[4];
+    int bv[4], xv[4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+      const int v = grp * 4 + x;
+      const bool in = v < n;
+      tv[x] = in ? Ts[static_cast<long>(w) * n + v] : make_double2(0., 0.);
+      const int ov = in ? orb[sd.vtx_off + v] : 0;
+      bv[x] = ov % nb;
+      xv[x] = ov / nb;
+    }
+    for (int r = 0; r < R; ++r) {
+      const int b = r % nb, k = r / nb;
+      const int rho = r + R * w;
+      const double scQ = pow2d(esQ[rho]) * qscale, scP = pow2d(esP[rho]);
+      float qr[4], qi[4], pr[4], pi[4];
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        const double2 ph = zmul(Fb[(bv[x] * nc + k) * nc + xv[x]], tv[x]);
+        const double2 gq = g0s[bv[x] + nb * (b + nb * (k + nc * w))];  // G0(b_j, b2; k2, w2), conjugated
+        const double2 zq = zmul(ph, make_double2(gq.x, -gq.y));
+        qr[x] = static_cast<float>(zq.x * scQ);
+        qi[x] = static_cast<float>(zq.y * scQ);
+        const double2 zp = zmul(g0s[b + nb * (bv[x] + nb * (k + nc * w))], ph);  // G0(b1, b_i; k1, w1)
+        pr[x] = static_cast<float>(zp.x * scP);
+        pi[x] = static_cast<float>(zp.y * scP);
+      }
+      uint2 h, l;
+      __half* q = oQ + static_cast<long>(rho) * kp + grp * 4;
+      split4(qr, h, l);
+      *reinterpret_cast<uint2*>(q) = h;
+      *reinterpret_cast<uint2*>(q + planeQ) = l;
+      split4(qi, h, l);
+      *reinterpret_cast<uint2*>(q + Kr) = h;
+      *reinterpret_cast<uint2*>(q + planeQ + Kr) = l;
+      if (doP) {
+        __half* pp = oP + static_cast<long>(rho) * kp + grp * 4;
+        split4(pr, h, l);
+        *reinterpret_cast<uint2*>(pp) = h;
+        *reinterpret_cast<uint2*>(pp + planeP) = l;
+        split4(pi, h, l);
+        *reinterpret_cast<uint2*>(pp + Kr) = h;
+        *reinterpret_cast<uint2*>(pp + planeP + Kr) = l;
+      }
+    }
+  }
+}
+
 // M operand, planes [sector][plane][Kr rows j][Kr columns i]: M(perm_r[i], perm_c[j]) * 2^{e_j}
 // for i, j < n, zero up to i < roundup(n, 32) and j < min(roundup(n, 128), Kr).  One warp per
 // row j: the first pass finds the row's maximum, the second writes the scaled planes; 2^{-e_j}
@@ -332,13 +408,21 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
     DCAACC_LAUNCH_CHECK();
     ++launches;
   }
-  const long groups = (a.n_max + kBK - 1) / kBK * (kBK / 8);
-  buildPhaseOperandKernel<true><<<dim3(gridX(groups * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
-      d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, s.D, s.Dp, s.Dp, s.Kr, static_cast<__half*>(w.pr));
-  DCAACC_LAUNCH_CHECK();
   const long mrows = std::min<long>((a.n_max + kBN - 1) / kBN * kBN, s.Kr);
   buildMOperandKernel<<<dim3(static_cast<unsigned>((mrows + 7) / 8), a.n_sectors), 256, 0, stream>>>(
       a.sectors, a.perm_r, a.perm_c, s.Kr, static_cast<__half*>(w.mb), w.mInv);
+  DCAACC_LAUNCH_CHECK();
+  if (a.Tc == a.Tr && orb_c == orb_r) {  // density-density: one pass for P and Q
+    const long groups4 = (a.n_max + kBK - 1) / kBK * (kBK / 4);
+    buildPhasePairKernel<<<dim3(gridX(groups4 * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
+        d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, w.eQ, s.Dp, s.Dq, s.Kr, static_cast<__half*>(w.pr),
+        static_cast<__half*>(w.bq));
+    DCAACC_LAUNCH_CHECK();
+    return launches + 2;
+  }
+  const long groups = (a.n_max + kBK - 1) / kBK * (kBK / 8);
+  buildPhaseOperandKernel<true><<<dim3(gridX(groups * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
+      d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, s.D, s.Dp, s.Dp, s.Kr, static_cast<__half*>(w.pr));
   DCAACC_LAUNCH_CHECK();
   buildPhaseOperandKernel<false><<<dim3(gridX(groups * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
       d, a.sectors, a.Tc, orb_c, a.Fb, a.G0, w.eQ, s.D, s.Dp, s.Dq, s.Kr, static_cast<__half*>(w.bq));
