@@ -517,7 +517,8 @@ void TpAccumulator::process() {
     timeBegin(DCAACC_STAGE_TWIDDLE, &b);
     int n_prep;
     if (tc_front_) {
-      n_prep = launchFrontendTcPrep(fa, ftc_, ds.orb_r.get(), ds.orb_c.get(), stream_);
+      n_prep = launchFrontendTcPrep(fa, ftc_, ds.orb_r.get(), non_density_ ? ds.orb_c.get() : ds.orb_r.get(),
+                                    stream_);
     }
     else {
       launchTwiddles(fa, stream_);
