@@ -432,8 +432,7 @@ def run_ours(args, world, rank, local):
     # committed ncu capture of this workload (one batch, cold caches), per launch of the stage.
     stage_kernels = {"update_g4": ["discPlanesKernel", "frontGemmKernel<2>", "updateG4DirectMma"],
                      "col_transform": ["frontGemmKernel<1>"], "row_transform": ["frontGemmKernel<0>"],
-                     "twiddle": ["twiddleWiKernel", "buildPhaseOperandKernel<0>", "buildPhaseOperandKernel<1>",
-                                 "buildMOperandKernel"]}.get(dom, [])
+                     "twiddle": ["twiddleWiKernel", "buildMOperandKernel", "buildPhasePairKernel"]}.get(dom, [])
     try:
         with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
             tk = json.load(f)["kernels"]
