@@ -196,7 +196,9 @@ buildPhaseOperandKernel(const TpDims dims, const SectorDesc* __restrict__ sector
 // Density-density models (the same vertex order on both sides): P and Q from one pass, sharing
 // the phase product Fb(b_i, k, x_i) T(w, i).  Thread per (w, 4 vertices) (4 rather than 8 keeps the
 // FP64 state small enough for 4 blocks per SM); Q for every row, P for the rows the row step reads
-// (half G: the upper frequency half).
+// (half G: the upper frequency half).  NB1: one band, where G0 depends on (k, w) only and the
+// row scales fold into it once per row.
+template <bool NB1>
 __global__ void __launch_bounds__(256)
 buildPhasePairKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, const double2* __restrict__ T,
                      const int* __restrict__ orb, const double2* __restrict__ Fb, const double2* __restrict__ G0,
@@ -237,16 +239,32 @@ buildPhasePairKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, 
       const int rho = r + R * w;
       const double scQ = pow2d(esQ[rho]) * qscale, scP = pow2d(esP[rho]);
       float qr[4], qi[4], pr[4], pi[4];
+      if (NB1) {
+        const double2 g = g0s[k + nc * w];
+        const double2 gq = make_double2(g.x * scQ, -g.y * scQ), gp = make_double2(g.x * scP, g.y * scP);
+        const double2* fbk = Fb + k * nc;
 #pragma unroll
-      for (int x = 0; x < 4; ++x) {
-        const double2 ph = zmul(Fb[(bv[x] * nc + k) * nc + xv[x]], tv[x]);
-        const double2 gq = g0s[bv[x] + nb * (b + nb * (k + nc * w))];  // G0(b_j, b2; k2, w2), conjugated
-        const double2 zq = zmul(ph, make_double2(gq.x, -gq.y));
-        qr[x] = static_cast<float>(zq.x * scQ);
-        qi[x] = static_cast<float>(zq.y * scQ);
-        const double2 zp = zmul(g0s[b + nb * (bv[x] + nb * (k + nc * w))], ph);  // G0(b1, b_i; k1, w1)
-        pr[x] = static_cast<float>(zp.x * scP);
-        pi[x] = static_cast<float>(zp.y * scP);
+        for (int x = 0; x < 4; ++x) {
+          const double2 ph = zmul(fbk[xv[x]], tv[x]);
+          const double2 zq = zmul(ph, gq), zp = zmul(gp, ph);
+          qr[x] = static_cast<float>(zq.x);
+          qi[x] = static_cast<float>(zq.y);
+          pr[x] = static_cast<float>(zp.x);
+          pi[x] = static_cast<float>(zp.y);
+        }
+      }
+      else {
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+          const double2 ph = zmul(Fb[(bv[x] * nc + k) * nc + xv[x]], tv[x]);
+          const double2 gq = g0s[bv[x] + nb * (b + nb * (k + nc * w))];  // G0(b_j, b2; k2, w2), conjugated
+          const double2 zq = zmul(ph, make_double2(gq.x, -gq.y));
+          qr[x] = static_cast<float>(zq.x * scQ);
+          qi[x] = static_cast<float>(zq.y * scQ);
+          const double2 zp = zmul(g0s[b + nb * (bv[x] + nb * (k + nc * w))], ph);  // G0(b1, b_i; k1, w1)
+          pr[x] = static_cast<float>(zp.x * scP);
+          pi[x] = static_cast<float>(zp.y * scP);
+        }
       }
       uint2 h, l;
       __half* q = oQ + static_cast<long>(rho) * kp + grp * 4;
@@ -271,11 +289,13 @@ buildPhasePairKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, 
 
 // M operand, planes [sector][plane][Kr rows j][Kr columns i]: M(perm_r[i], perm_c[j]) * 2^{e_j}
 // for i, j < n, zero up to i < roundup(n, 32) and j < min(roundup(n, 128), Kr).  One warp per
-// row j: the first pass finds the row's maximum, the second writes the scaled planes; 2^{-e_j}
-// goes to mInv[sector][j].
+// row j: the column perm_c[j] of M is read contiguously into the warp's shared-memory row (its
+// maximum on the way), then the permuted entries come from there; 2^{-e_j} goes to
+// mInv[sector][j].  Dynamic shared memory: Kr doubles per warp.
 __global__ void __launch_bounds__(256)
 buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restrict__ perm_r,
                     const int* __restrict__ perm_c, int Kr, __half* __restrict__ out, float* __restrict__ mInv) {
+  extern __shared__ double mrow_all[];
   const SectorDesc sd = sectors[blockIdx.y];
   const int n = sd.n;
   const int groups = (n + kBK - 1) / kBK * (kBK / 8);
@@ -283,16 +303,32 @@ buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restric
   const long plane = static_cast<long>(Kr) * Kr;
   __half* o = out + static_cast<long>(blockIdx.y) * kPl * plane;
   const int lane = threadIdx.x % 32;
+  double* mrow = mrow_all + static_cast<long>(threadIdx.x / 32) * Kr;
+  const int* pr = perm_r + sd.vtx_off;
   const int warps = gridDim.x * (blockDim.x / 32);
   for (int j = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; j < rows; j += warps) {
     const double* col = j < n ? sd.M + static_cast<long>(sd.ldm) * perm_c[sd.vtx_off + j] : nullptr;
     double mx = 0;
-    if (col)
-      for (int i = lane; i < n; i += 32)
-        mx = fmax(mx, fabs(col[perm_r[sd.vtx_off + i]]));
+    __syncwarp();  // the previous row's reads of mrow are done
+    for (int i0 = 0; i0 < n; i0 += 128) {  // four loads in flight per lane
+      double m[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + 32 * u + lane;
+        m[u] = (col && i < n) ? col[i] : 0.;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + 32 * u + lane;
+        if (i < n)
+          mrow[i] = m[u];
+        mx = fmax(mx, fabs(m[u]));
+      }
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
       mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    __syncwarp();
     const int e = scaleExp(mx);
     const double sc = pow2d(e);
     for (int grp = lane; grp < groups; grp += 32) {
@@ -301,7 +337,7 @@ buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restric
 #pragma unroll
       for (int x = 0; x < 8; ++x) {
         const int i = grp * 8 + x;
-        y[x] = static_cast<float>(((col && i < n) ? col[perm_r[sd.vtx_off + i]] : 0.) * sc);
+        y[x] = static_cast<float>((i < n ? mrow[pr[i]] : 0.) * sc);
       }
       split8(y, v[0], v[1]);
 #pragma unroll
@@ -409,12 +445,18 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
     ++launches;
   }
   const long mrows = std::min<long>((a.n_max + kBN - 1) / kBN * kBN, s.Kr);
-  buildMOperandKernel<<<dim3(static_cast<unsigned>((mrows + 7) / 8), a.n_sectors), 256, 0, stream>>>(
-      a.sectors, a.perm_r, a.perm_c, s.Kr, static_cast<__half*>(w.mb), w.mInv);
+  // Up to 8 warps per block, as many as their Kr-double rows fit in 200 KB of shared memory.
+  const int mwarps = static_cast<int>(std::max<long>(1, std::min<long>(8, 200L * 1024 / (8L * s.Kr))));
+  const size_t msmem = sizeof(double) * mwarps * size_t(s.Kr);
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(buildMOperandKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(msmem)));
+  buildMOperandKernel<<<dim3(static_cast<unsigned>((mrows + mwarps - 1) / mwarps), a.n_sectors), 32 * mwarps, msmem,
+                        stream>>>(a.sectors, a.perm_r, a.perm_c, s.Kr, static_cast<__half*>(w.mb), w.mInv);
   DCAACC_LAUNCH_CHECK();
   if (a.Tc == a.Tr && orb_c == orb_r) {  // density-density: one pass for P and Q
     const long groups4 = (a.n_max + kBK - 1) / kBK * (kBK / 4);
-    buildPhasePairKernel<<<dim3(gridX(groups4 * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
+    auto k = d.nb == 1 ? buildPhasePairKernel<true> : buildPhasePairKernel<false>;
+    k<<<dim3(gridX(groups4 * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
         d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, w.eQ, s.Dp, s.Dq, s.Kr, static_cast<__half*>(w.pr),
         static_cast<__half*>(w.bq));
     DCAACC_LAUNCH_CHECK();
