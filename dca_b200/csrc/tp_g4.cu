@@ -179,6 +179,234 @@ updateG4Kernel(const TpDims dims, const GT* __restrict__ G, long g_sector_stride
 }
 
 
+// Any number of bands, at most two channels: the same entries and formulas as updateG4Kernel,
+// with the G blocks a tile reads (A, B, C, E, P below, per channel set) staged in shared memory
+// for each measurement by the bulk-copy engine (two-stage ring) instead of gathered from L2 per
+// entry and measurement.  A thread keeps EPT entries; their block offsets are computed once per
+// chunk of entries, the measurement loop then reads shared memory only.  The (chunk, measurement)
+// steps form one sequence, so the ring keeps running across chunks.
+//   A = G(w1; w2)  B = G(w2+x; w1+x)  C = G(w1; w1+x)  E = G(w2+x; w2)  P = G(m1; m2)
+constexpr int kStagedMaxCh = 2;
+constexpr int kStagedEpt = 4;
+
+template <typename GT, typename AT>
+__global__ void __launch_bounds__(256)
+updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_stride,
+                     const int* __restrict__ signs, int n_slots, const int* __restrict__ k_add,
+                     const int* __restrict__ k_sub, const int* __restrict__ q_list,
+                     const int* __restrict__ wex_list, double2* const* __restrict__ G4, bool atomic,
+                     int* __restrict__ err) {
+  using C = cplx_t<AT>;
+  constexpr int EPT = kStagedEpt;
+  const int nb = dims.nb, nc = dims.nc, nw = dims.nw, nw_ext = dims.nw_ext, R = dims.R;
+  const int w1 = blockIdx.x, w2 = blockIdx.y, iwq = blockIdx.z;
+  const int wex = wex_list[iwq];
+  const int ext = dims.ext;
+  const int nb2 = nb * nb, nb4 = nb2 * nb2;
+  const int inner = nb4 * nc;
+  const long per_tile = static_cast<long>(inner) * nc * dims.nq;
+  const long blk = static_cast<long>(R) * R;
+  const int n_ch = dims.n_channels;
+
+  // Blocks of this tile: slot index in the stage (-1: not needed).
+  bool need[5] = {false, false, false, false, false};  // A B C E P
+  for (int c = 0; c < n_ch; ++c) {
+    const int ch = dims.channels[c];
+    need[0] = true;
+    if (ch == 1 || ch == 2 || ch == 3)
+      need[1] = true;
+    if (ch == 2 || ch == 3)
+      need[2] = need[3] = true;
+    if (ch == 4)
+      need[4] = true;
+  }
+  const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
+  const int m1 = wex + nw - 1 - w1 + ext, m2 = wex + nw - 1 - w2 + ext;
+  auto blkOff = [&](int wr, int wc) { return (static_cast<long>(wr) * nw_ext + wc) * blk; };
+  const long boffAll[5] = {blkOff(w1e, w2e), blkOff(w2x, w1x), blkOff(w1e, w1x), blkOff(w2x, w2e), blkOff(m1, m2)};
+  int sidx[5];
+  long boff[5];
+  int nblk = 0;
+  for (int b = 0; b < 5; ++b) {
+    sidx[b] = need[b] ? nblk : -1;
+    if (need[b])
+      boff[nblk++] = boffAll[b];
+  }
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);  // [2]
+  GT* stage = reinterpret_cast<GT*>(smem_raw + 16);       // [2][2 spins][nblk][R*R]
+  const long stage_elems = 2L * nblk * blk;
+  const uint32_t blk_bytes = static_cast<uint32_t>(blk * sizeof(GT));
+  const long n_chunks = (per_tile + static_cast<long>(EPT) * blockDim.x - 1) / (static_cast<long>(EPT) * blockDim.x);
+  const long n_steps = n_chunks * n_slots;
+  auto issue = [&](long step) {
+    const int st = static_cast<int>(step & 1);
+    const int slot = static_cast<int>(step % n_slots);
+    GT* dst = stage + st * stage_elems;
+    mbarArriveExpectTx(&bar[st], 2 * nblk * blk_bytes);
+    for (int s = 0; s < 2; ++s) {
+      const GT* src = G + g_sector_stride * (2 * slot + s);
+      for (int b = 0; b < nblk; ++b)
+        bulkCopyG2S(dst + (s * nblk + b) * blk, src + boff[b], blk_bytes, &bar[st]);
+    }
+  };
+  const int t = threadIdx.x;
+  if (t == 0) {
+    mbarInit(&bar[0], 1);
+    mbarInit(&bar[1], 1);
+    fenceBarrierInit();
+  }
+  __syncthreads();
+  if (t == 0) {
+    issue(0);
+    if (n_steps > 1)
+      issue(1);
+  }
+
+  const long s_w1 = inner, s_k2 = s_w1 * nw, s_w2 = s_k2 * nc, s_q = s_w2 * nw, s_wq = s_q * dims.nq;
+  const long tile_base = w1 * s_w1 + w2 * s_w2 + iwq * s_wq;
+  long step = 0;
+  for (long chunk = 0; chunk < n_chunks; ++chunk) {
+    // This chunk's entries: G4 index and, per channel, the shared-memory offsets of the two G
+    // elements of the second-order term (id in A, ie in B or P) and, for PH magnetic / charge,
+    // of the disconnected-term elements (iu in C, iv in E).
+    long g4i[EPT];
+    int id[EPT][kStagedMaxCh], ie[EPT][kStagedMaxCh], iu[EPT], iv[EPT];
+    bool live[EPT];
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      const long idx = chunk * EPT * blockDim.x + t + static_cast<long>(e) * blockDim.x;
+      live[e] = idx < per_tile;
+      const long ii = live[e] ? idx : 0;
+      const int in = static_cast<int>(ii % inner);
+      const int outer = static_cast<int>(ii / inner);
+      const int b1 = in % nb, b2 = (in / nb) % nb, b3 = (in / nb2) % nb, b4 = (in / (nb2 * nb)) % nb;
+      const int k1 = in / nb4;
+      const int k2 = outer % nc, iq = outer / nc;
+      const int q = q_list[iq];
+      const int k1q = k_add[k1 + nc * q], k2q = k_add[k2 + nc * q];
+      auto rc = [&](int b, int k) { return b + nb * k; };
+      g4i[e] = tile_base + in + k2 * s_k2 + iq * s_q;
+      iu[e] = rc(b1, k1) * R + rc(b2, k1q);
+      iv[e] = rc(b4, k2q) * R + rc(b3, k2);
+#pragma unroll
+      for (int c = 0; c < kStagedMaxCh; ++c) {
+        const int ch = c < n_ch ? dims.channels[c] : 0;
+        if (ch == 2) {
+          id[e][c] = rc(b1, k1) * R + rc(b3, k2);
+          ie[e][c] = rc(b4, k2q) * R + rc(b2, k1q);
+        }
+        else if (ch == 3) {
+          id[e][c] = rc(b4, k1) * R + rc(b1, k2);
+          ie[e][c] = rc(b3, k2q) * R + rc(b2, k1q);
+        }
+        else if (ch == 1) {
+          id[e][c] = rc(b4, k1) * R + rc(b2, k2);
+          ie[e][c] = rc(b1, k2q) * R + rc(b3, k1q);
+        }
+        else {
+          const int qk1 = k_sub[k1 + nc * q], qk2 = k_sub[k2 + nc * q];
+          id[e][c] = rc(b3, k1) * R + rc(b1, k2);
+          ie[e][c] = rc(b4, qk1) * R + rc(b2, qk2);
+        }
+      }
+    }
+    C acc[EPT][kStagedMaxCh];
+#pragma unroll
+    for (int e = 0; e < EPT; ++e)
+#pragma unroll
+      for (int c = 0; c < kStagedMaxCh; ++c)
+        acc[e][c] = mk(AT(0), AT(0));
+
+    for (int slot = 0; slot < n_slots; ++slot, ++step) {
+      const int st = static_cast<int>(step & 1);
+      const bool ok = mbarWait(&bar[st], static_cast<uint32_t>((step >> 1) & 1), err);
+      if (!__syncthreads_and(ok))
+        return;  // uniform bail-out; the host reports the error word
+      const GT* S0 = stage + st * stage_elems;
+      const GT* S1 = S0 + nblk * blk;
+      auto ld = [](const GT* p) { return mk(static_cast<AT>(p->x), static_cast<AT>(p->y)); };
+      const AT half_sign = AT(0.5) * static_cast<AT>(signs[slot]);
+#pragma unroll
+      for (int e = 0; e < EPT; ++e) {
+        if (!live[e])
+          continue;
+#pragma unroll
+        for (int c = 0; c < kStagedMaxCh; ++c) {
+          if (c >= n_ch)
+            break;
+          const int ch = dims.channels[c];
+          C v;
+          if (ch == 2 || ch == 3) {
+            const GT* Cb0 = S0 + sidx[2] * blk;
+            const GT* Cb1 = S1 + sidx[2] * blk;
+            const GT* Eb0 = S0 + sidx[3] * blk;
+            const GT* Eb1 = S1 + sidx[3] * blk;
+            const C a0 = ld(Cb0 + iu[e]), a1 = ld(Cb1 + iu[e]), e0 = ld(Eb0 + iv[e]), e1 = ld(Eb1 + iv[e]);
+            const AT sg = ch == 2 ? AT(-1) : AT(1);
+            v = cmul(mk(a0.x + sg * a1.x, a0.y + sg * a1.y), mk(e0.x + sg * e1.x, e0.y + sg * e1.y));
+            const GT* Ab0 = S0 + sidx[0] * blk;
+            const GT* Ab1 = S1 + sidx[0] * blk;
+            const GT* Bb0 = S0 + sidx[1] * blk;
+            const GT* Bb1 = S1 + sidx[1] * blk;
+            C d = cmul(ld(Ab0 + id[e][c]), ld(Bb0 + ie[e][c]));
+            cfma(d, ld(Ab1 + id[e][c]), ld(Bb1 + ie[e][c]));
+            v = csub(v, d);
+          }
+          else if (ch == 1) {
+            const GT* Ab0 = S0 + sidx[0] * blk;
+            const GT* Ab1 = S1 + sidx[0] * blk;
+            const GT* Bb0 = S0 + sidx[1] * blk;
+            const GT* Bb1 = S1 + sidx[1] * blk;
+            C d = cmul(ld(Ab0 + id[e][c]), ld(Bb1 + ie[e][c]));
+            cfma(d, ld(Ab1 + id[e][c]), ld(Bb0 + ie[e][c]));
+            v = mk(-d.x, -d.y);
+          }
+          else {
+            const GT* Ab0 = S0 + sidx[0] * blk;
+            const GT* Ab1 = S1 + sidx[0] * blk;
+            const GT* Pb0 = S0 + sidx[4] * blk;
+            const GT* Pb1 = S1 + sidx[4] * blk;
+            v = cmul(ld(Ab0 + id[e][c]), ld(Pb1 + ie[e][c]));
+            cfma(v, ld(Ab1 + id[e][c]), ld(Pb0 + ie[e][c]));
+          }
+          acc[e][c].x = fma(half_sign, v.x, acc[e][c].x);
+          acc[e][c].y = fma(half_sign, v.y, acc[e][c].y);
+        }
+      }
+      __syncthreads();  // stage st is free again
+      if (t == 0 && step + 2 < n_steps) {
+        fenceProxyAsync();
+        issue(step + 2);
+      }
+    }
+
+    // One read-modify-write of the FP64 running sum per entry and channel.
+#pragma unroll
+    for (int e = 0; e < EPT; ++e) {
+      if (!live[e])
+        continue;
+#pragma unroll
+      for (int c = 0; c < kStagedMaxCh; ++c) {
+        if (c >= n_ch)
+          break;
+        double2* p = G4[c] + g4i[e];
+        if (atomic) {
+          atomicAdd(&p->x, static_cast<double>(acc[e][c].x));
+          atomicAdd(&p->y, static_cast<double>(acc[e][c].y));
+        }
+        else {
+          double2 old = *p;
+          old.x += static_cast<double>(acc[e][c].x);
+          old.y += static_cast<double>(acc[e][c].y);
+          *p = old;
+        }
+      }
+    }
+  }
+}
+
 // Single-band PH-magnetic / PH-charge update with the G blocks staged in shared memory.
 //
 // CTA = one (w1, w2, wq) tile and a chunk of momentum transfers q; thread = (k1, q, k2-chunk),
@@ -394,7 +622,7 @@ static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_strid
   const TpDims& d = a.dims;
   const int n_kc = (d.nc + KT - 1) / KT;
   const int per_q = d.nc * n_kc;
-  if (per_q > 1024)
+  if (per_q > MAXT)  // one q per CTA must fit the kernel's launch bound
     return false;
   const int q_chunk = std::max(1, std::min(d.nq, std::min(target_threads, MAXT) / per_q));
   const int threads = per_q * q_chunk;
@@ -429,6 +657,29 @@ int launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStrea
       return 1;
   }
   const dim3 grid(a.dims.nw, a.dims.nw, a.dims.nwq);
+  // Batches: the staged kernel (a single measurement reads each block element a few times only, and
+  // the direct gathers of updateG4Kernel cost less than staging).
+  if (a.n_slots >= 2 && a.dims.n_channels <= kStagedMaxCh && (size_t(a.dims.R) * a.dims.R * sizeof(GT)) % 16 == 0) {
+    int nblk = 1;  // A, and B / C, E / P as the channels need them
+    bool needB = false, needCE = false, needP = false;
+    for (int c = 0; c < a.dims.n_channels; ++c) {
+      const int ch = a.dims.channels[c];
+      needB |= ch == 1 || ch == 2 || ch == 3;
+      needCE |= ch == 2 || ch == 3;
+      needP |= ch == 4;
+    }
+    nblk += needB + 2 * needCE + needP;
+    const size_t smem = 16 + 2 * 2 * size_t(nblk) * a.dims.R * a.dims.R * sizeof(GT);
+    if (smem <= 200 * 1024) {
+      using AT = std::conditional_t<std::is_same_v<GT, double2>, double, float>;
+      auto k = updateG4StagedKernel<GT, AT>;
+      DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      k<<<grid, 256, smem, stream>>>(a.dims, G, g_sector_stride, a.signs, a.n_slots, a.k_add, a.k_sub, a.q_list,
+                                     a.wex_list, a.G4, a.atomic, a.err);
+      DCAACC_LAUNCH_CHECK();
+      return 1;
+    }
+  }
   if constexpr (std::is_same_v<GT, double2>) {
     updateG4Kernel<double2, double, 4><<<grid, 256, 0, stream>>>(
         a.dims, G, g_sector_stride, a.signs, a.n_slots, a.k_add, a.k_sub, a.q_list, a.wex_list,
