@@ -156,6 +156,38 @@ def test_half_g_matches_full_g(monkeypatch, n_meas, max_batch):
         assert rel_err(h, f) <= MIXED_TOL
 
 
+def _small(wname, **kw):
+    import dataclasses
+    return dataclasses.replace(W.WORKLOADS[wname], **kw)
+
+
+def test_large_cluster_fp64_matches_oracle(oracle_lib):
+    """6x6 single band (Nc = 36): one momentum transfer's k1 x k2 block does not fit the tuned
+    single-band kernel's thread block, so the FP64 update takes the general kernel."""
+    w = _small("c5", nw_half=2, n_sp=64, n_range=(20, 40))
+    case = case_from_workload(w, 2)
+    acc = run_gpu(case)
+    ora = run_oracle(oracle_lib, case)
+    for got, want in zip(acc.get_G4(), ora.get_G4()):
+        assert rel_err(got, want) <= FP64_TOL
+
+
+@pytest.mark.parametrize("channels", [(4,), (2, 3)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_multiband_batched_matches_oracle(oracle_lib, channels, precision):
+    """Three bands on the Betts 8 cluster, batches of 3: the staged multi-band update (the G blocks
+    of each measurement in shared memory), particle-particle and the two PH channels, in FP64 and
+    in the mixed path."""
+    w = _small("c4", nw_half=4, n_sp=64, n_range=(20, 40), channels=channels, freq_transfer=1)
+    case = case_from_workload(w, 4)
+    acc = run_gpu(case, precision=precision, max_batch=3)
+    ora = run_oracle(oracle_lib, case)
+    tol = FP64_TOL if precision == 0 else MIXED_TOL
+    for got, want in zip(acc.get_G4(), ora.get_G4()):
+        print("multiband", channels, precision, rel_err(got, want))
+        assert rel_err(got, want) <= tol
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_sum_to_equals_single_accumulator(precision):
     case, _ = golden("sq2_all")
