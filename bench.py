@@ -266,14 +266,26 @@ def run_ours(args, world, rank, local):
     configs = [list(m.sectors) for m in pool]
     signs = [m.sign for m in pool]
     dev_M = [[torch.from_numpy(np.ascontiguousarray(s.M.T)).cuda().t() for s in m.sectors] for m in pool]
+    # Host-resident M for the end-to-end leg: each batch's matrices in one pinned buffer, packed in
+    # the order they are accumulated (column major, n x n each), as a caller with a pinned arena
+    # per batch holds them; the accumulator then copies a batch in one piece.
     pinned = []
-    for m in pool:
-        pair = []
-        for s in m.sectors:
-            t = torch.empty((s.n, s.n), dtype=torch.float64, pin_memory=True)
-            t.copy_(torch.from_numpy(np.ascontiguousarray(s.M.T)))
-            pair.append(t.numpy().T)  # column-major view of pinned memory
-        pinned.append(pair)
+    arenas = []
+    for b0 in range(0, len(pool), B):
+        mats = [s.M for m in pool[b0:b0 + B] for s in m.sectors]
+        arena = torch.empty(max(1, sum(M.shape[0] ** 2 for M in mats)), dtype=torch.float64, pin_memory=True)
+        arenas.append(arena)
+        flat = arena.numpy()
+        off = 0
+        for m in pool[b0:b0 + B]:
+            pair = []
+            for sec in m.sectors:
+                n = sec.n
+                view = flat[off:off + n * n].reshape(n, n)  # row-major M^T = column-major M
+                view[...] = sec.M.T
+                pair.append(view.T)
+                off += n * n
+            pinned.append(pair)
 
     params = TpParameters.from_workload(w, cl, precision=1, max_batch=B)
     acc = TpAccumulator(g0, params)

@@ -341,6 +341,8 @@ void TpAccumulator::reset() {
   slots_ = 0;
   vtx_used_ = 0;
   x_used_ = 0;
+  m_used_ = 0;
+  mcopy_bytes_ = 0;  // a copy of a discarded batch is not issued
   n_max_batch_ = 0;
   for (auto& g : G4_)
     DCAACC_CUDA_CHECK(cudaMemsetAsync(g.get(), 0, g.bytes(), stream_));
@@ -444,12 +446,28 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
     const double* Mptr = x.M;
     int ldm = std::max(x.ldm, 1);
     if (n && !x.m_on_device) {
-      double* dst = dstage_[hset_].M.get() + size_t(sidx) * max_order_ * max_order_;
-      if (x.ldm == n)
-        DCAACC_CUDA_CHECK(cudaMemcpyAsync(dst, x.M, sizeof(double) * n * n, cudaMemcpyHostToDevice, copy_stream_));
-      else
+      double* dst = dstage_[hset_].M.get() + m_used_;
+      m_used_ += size_t(n) * n;
+      const size_t bytes = sizeof(double) * n * n;
+      if (x.ldm == n) {
+        if (mcopy_bytes_ && reinterpret_cast<const char*>(mcopy_src_) + mcopy_bytes_ == reinterpret_cast<const char*>(x.M) &&
+            reinterpret_cast<char*>(mcopy_dst_) + mcopy_bytes_ == reinterpret_cast<char*>(dst)) {
+          mcopy_bytes_ += bytes;  // contiguous on both sides: one larger copy
+          if (mcopy_bytes_ >= (size_t(8) << 20))
+            flushMCopy();  // in pieces of about 8 MB, overlapping the staging of the rest
+        }
+        else {
+          flushMCopy();
+          mcopy_src_ = x.M;
+          mcopy_dst_ = dst;
+          mcopy_bytes_ = bytes;
+        }
+      }
+      else {
+        flushMCopy();
         DCAACC_CUDA_CHECK(cudaMemcpy2DAsync(dst, sizeof(double) * n, x.M, sizeof(double) * x.ldm,
                                             sizeof(double) * n, n, cudaMemcpyHostToDevice, copy_stream_));
+      }
       Mptr = dst;
       ldm = n;
     }
@@ -471,9 +489,16 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
   ++slots_;
 }
 
+void TpAccumulator::flushMCopy() {
+  if (mcopy_bytes_)
+    DCAACC_CUDA_CHECK(cudaMemcpyAsync(mcopy_dst_, mcopy_src_, mcopy_bytes_, cudaMemcpyHostToDevice, copy_stream_));
+  mcopy_bytes_ = 0;
+}
+
 void TpAccumulator::process() {
   if (slots_ == 0)
     return;
+  flushMCopy();
   const int n_sec = 2 * slots_;
   const int n_orb1 = dims_.n_orb + 1;
   // Uploads on the copy stream (after the kernels that last read this device set, see stage());
@@ -576,6 +601,7 @@ void TpAccumulator::process() {
   slots_ = 0;
   vtx_used_ = 0;
   x_used_ = 0;
+  m_used_ = 0;
   n_max_batch_ = 0;
 }
 
@@ -766,6 +792,7 @@ void TpAccumulator::setStream(cudaStream_t s) {
 }
 
 void TpAccumulator::synchronize() {
+  flushMCopy();
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(copy_stream_));  // host M copies of a pending batch
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
   checkDeviceError();

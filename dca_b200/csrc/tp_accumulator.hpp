@@ -193,6 +193,13 @@ private:
   int slots_ = 0;         // measurements staged
   int vtx_used_ = 0;      // packed vertices staged
   long x_used_ = 0;       // X' elements reserved
+  size_t m_used_ = 0;     // host-resident M copied into the device set, packed n x n per sector
+  // Host -> device M copy being extended: a sector whose host M directly follows the previous
+  // one's (a caller keeping a batch's matrices in one pinned buffer) joins the same copy.
+  const double* mcopy_src_ = nullptr;
+  double* mcopy_dst_ = nullptr;
+  size_t mcopy_bytes_ = 0;
+  void flushMCopy();
   int n_max_batch_ = 0;   // largest order staged
   bool ready_ = false;    // reset() called since the last finalize
   bool finalized_ = false;
