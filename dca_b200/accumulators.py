@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import sys
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -146,22 +147,41 @@ def _make_sectors(M_pair, configs, keep: list, count: int = 1):
     rec["tau"] = tau_all.ctypes.data + 8 * offs
     for k, name in enumerate(_VERTEX_INTS):
         rec[name] = ints.ctypes.data + 4 * (k * width + offs)
-    ptr = np.zeros(ns, np.uint64)
-    ldm = np.ones(ns, np.int32)
-    dev = np.zeros(ns, np.int32)
-    for s in range(ns):
-        M, n = M_pair[s], int(lens[s])
-        if hasattr(M, "is_cuda") and M.is_cuda:
-            ptr[s], ldm[s] = _device_matrix(M, n, keep)
-            dev[s] = 1
-        else:
-            Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
-            keep.append(Mh)
-            ptr[s] = Mh.ctypes.data
-            ldm[s] = max(n, 1)
-    rec["M"] = ptr
-    rec["ldm"] = ldm
-    rec["m_on_device"] = dev
+    torch = sys.modules.get("torch")
+    if torch is not None and all(type(M) is torch.Tensor and M.is_cuda for M in M_pair):
+        # Device matrices (the walkers' M): one pass of attribute reads; a matrix that is not
+        # column major float64 goes through _device_matrix.
+        f64 = torch.float64
+        ptrs, lds = [], []
+        for M, n in zip(M_pair, lens.tolist()):
+            st = M.stride()
+            if M.dtype is f64 and (n == 0 or (st[0] == 1 and st[1] >= n)):
+                ptrs.append(M.data_ptr())
+                lds.append(max(st[1], 1) if n else 1)
+            else:
+                p_, l_ = _device_matrix(M, n, keep)
+                ptrs.append(p_)
+                lds.append(l_)
+        rec["M"] = ptrs
+        rec["ldm"] = lds
+        rec["m_on_device"] = 1
+    else:
+        ptr = np.zeros(ns, np.uint64)
+        ldm = np.ones(ns, np.int32)
+        dev = np.zeros(ns, np.int32)
+        for s in range(ns):
+            M, n = M_pair[s], int(lens[s])
+            if hasattr(M, "is_cuda") and M.is_cuda:
+                ptr[s], ldm[s] = _device_matrix(M, n, keep)
+                dev[s] = 1
+            else:
+                Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
+                keep.append(Mh)
+                ptr[s] = Mh.ctypes.data
+                ldm[s] = max(n, 1)
+        rec["M"] = ptr
+        rec["ldm"] = ldm
+        rec["m_on_device"] = dev
     keep.extend((tau_all, ints, rec, M_pair))
     return rec.ctypes.data_as(ctypes.POINTER(N.Sector))
 

@@ -81,6 +81,8 @@ discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_
     long bc = 0, be = 0;
     bool cc = false, ce = false;  // read from the conjugated mirror (half G)
     const bool in_row = row < M;
+    // Half G4: the GEMM reads U only for the rows (k1, w1) with w1 >= Nw / 2.
+    const bool need_u = in_row && !(dims.half_g4 && 2 * (row / nc) < dims.nw);
     if (in_row) {
       const int k = row % nc, w = row / nc;
       const int kq = k_add[k + nc * q];
@@ -98,7 +100,12 @@ discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_
         const float hs = 0.5f * static_cast<float>(signs[slot]);
         const float2* G0s = G + g_sector_stride * (2 * slot);
         const float2* G1s = G0s + g_sector_stride;
-        float2 c0 = G0s[bc], c1 = G1s[bc], e0 = G0s[be], e1 = G1s[be];
+        float2 c0 = make_float2(0.f, 0.f), c1 = c0;
+        if (need_u) {
+          c0 = G0s[bc];
+          c1 = G1s[bc];
+        }
+        float2 e0 = G0s[be], e1 = G1s[be];
         if (cc) {
           c0.y = -c0.y;
           c1.y = -c1.y;
@@ -132,8 +139,10 @@ discPlanesKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_
     const long o = static_cast<long>(row) * kp + slot0;
 #pragma unroll
     for (int pl = 0; pl < kPl; ++pl) {
-      store8(U + pl * plane + o, ur[pl]);
-      store8(U + pl * plane + o + Kb, ui[pl]);
+      if (need_u || !dims.half_g4) {
+        store8(U + pl * plane + o, ur[pl]);
+        store8(U + pl * plane + o + Kb, ui[pl]);
+      }
       store8(V + pl * plane + o, vr[pl]);
       store8(V + pl * plane + o + Kb, vi[pl]);
     }
