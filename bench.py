@@ -8,10 +8,13 @@ per-spin expansion orders n ~ U[50, 400], batches of 64 measurements, synthetic 
 (twiddles, NDFT + cluster transform + G, G4 update); G4 (2 x 268 MB FP64) and each batch's G
 (1 GB) exceed the 126 MB L2, so no L2 flush is needed between steps.
 
-  value      measurements/s with M already resident in HBM (device pointers), CUDA-event timed
+  value      measurements/s with M already resident in HBM (device pointers), CUDA-event timed;
+             each batch's kernels are replayed from the accumulator's CUDA graph of that batch
+             shape (captured during the warm-up, which runs at least four batches)
   e2e        the same through the public API with M in pinned host memory (host->device copies
              inside the timed region) and a 4 KiB G4 read-back per step, wall-clock timed
-  roofline   the dominant stage, timed with CUDA events on the accumulator's stream
+  roofline   the dominant stage, timed with CUDA events on the accumulator's stream around each
+             stage's launches, in a second pass over the same steps (eager launches)
   cpu_baseline  the reference's own CPU TpAccumulator (oracle/_ref/tp_ref, FP64) on a bounded
              sample, one single-threaded process per core
 
@@ -297,11 +300,14 @@ def run_ours(args, world, rank, local):
         acc.accumulate_batch(M_src[base:base + B], configs[base:base + B], signs[base:base + B])
         acc.flush()
 
-    for i in range(args.warmup):
+    # Warm-up: at least four batches, so that both device input sets have their CUDA graph
+    # (captured on a batch shape's second batch) before the timed region.
+    warmup = max(args.warmup, 4)
+    for i in range(warmup):
         step(i, dev_M)
     torch.cuda.synchronize()
-    acc.enable_timing(True)
     launches0 = acc.kernel_launches()
+    graphs0 = acc.graph_stats()
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
     barrier(world)
@@ -316,7 +322,15 @@ def run_ours(args, world, rank, local):
     clk = clocks.stop()
     ms_local = ev0.elapsed_time(ev1)
     launches = acc.kernel_launches() - launches0
+    graphs1 = acc.graph_stats()
+    graph_info = {"captured": graphs1[0] - graphs0[0], "batches_replayed": graphs1[1] - graphs0[1]}
+    # Stage breakdown: the same steps once more with CUDA events around each stage's launches on
+    # the accumulator's stream (eager launches: the events sit between the kernels).
+    acc.enable_timing(True)
+    for i in range(args.steps):
+        step(i, dev_M)
     stages = acc.stage_times()
+    acc.enable_timing(False)
     mirror = acc.mirror_mode()
     ms = max_over_ranks(ms_local, world)
     n_meas_total = world * args.steps * B
@@ -456,7 +470,7 @@ def run_ours(args, world, rank, local):
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (G, G4 partials) + fp64 (running G4)",
         "data": "synthetic (seeded; dca_b200.workloads)",
         "config": {"workload": f"{w.name}: single-band Hubbard 4x4 (Nc=16), Nw=64, 16 q x 1 wq, "
@@ -465,6 +479,7 @@ def run_ours(args, world, rank, local):
                    "l2": "inputs larger than L2 (G4 537 MB, G 1 GB per batch)"},
         "e2e": e2e,
         "gpu_launches": int(launches),
+        "cuda_graphs": graph_info,
         "mirror_mode": {"half_g": bool(mirror & 1), "half_g4": bool(mirror & 2)},
         "roofline": roof,
         "update_g4_roofline": g4_roof,

@@ -317,6 +317,16 @@ class TpAccumulator:
         _check(N.lib.dcaacc_tp_stage_times(self._h, ms, cnt, 4))
         return {name: (ms[i], cnt[i]) for i, name in enumerate(self.STAGES)}
 
+    def set_graphs(self, on: bool = True):
+        """Replay each batch shape's kernel sequence from a CUDA graph (mixed path; on by default)."""
+        _check(N.lib.dcaacc_tp_set_graphs(self._h, int(on)))
+
+    def graph_stats(self):
+        """(graphs captured, batches replayed from a graph) since creation."""
+        cap, rep = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(N.lib.dcaacc_tp_graph_stats(self._h, ctypes.byref(cap), ctypes.byref(rep)))
+        return cap.value, rep.value
+
     def peek_G4(self, channel: int, offset: int, count: int) -> np.ndarray:
         out = np.empty(count, np.complex128)
         _check(N.lib.dcaacc_tp_peek_g4(self._h, channel, offset, count, _dptr(out.view(np.float64))))

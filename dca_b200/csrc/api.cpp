@@ -174,6 +174,18 @@ int dcaacc_tp_stage_times(dcaacc_tp* acc, double* ms, uint64_t* launches, int32_
   return guard([&] { acc->impl.stageTimes(ms, launches, n_stages); });
 }
 
+int dcaacc_tp_set_graphs(dcaacc_tp* acc, int32_t on) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.setGraphs(on != 0); });
+}
+
+int dcaacc_tp_graph_stats(const dcaacc_tp* acc, uint64_t* captures, uint64_t* replays) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.graphStats(captures, replays); });
+}
+
 int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out) {
   if (!acc || !out)
     return null_handle();

@@ -209,6 +209,8 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
     // The mixed path runs its front-end and the disconnected terms of the one-band PH channels on
     // the tensor cores, unless DCAACC_TP_SIMT_ONLY=1 selects the all-SIMT kernels (kept to compare
     // both paths).
+    const char* graphs_env = std::getenv("DCAACC_TP_GRAPHS");
+    graphs_on_ = !(graphs_env && std::strcmp(graphs_env, "0") == 0);
     const char* simt_env = std::getenv("DCAACC_TP_SIMT_ONLY");
     const bool simt_only = simt_env && std::strcmp(simt_env, "1") == 0;
     G32_.alloc(g_elems);
@@ -322,6 +324,7 @@ TpAccumulator::~TpAccumulator() {
     cudaEventDestroy(t.begin);
     cudaEventDestroy(t.end);
   }
+  releaseGraphs();
   for (auto& h : hstage_)
     if (h.uploaded)
       cudaEventDestroy(h.uploaded);
@@ -521,6 +524,7 @@ void TpAccumulator::process() {
   }
   DCAACC_CUDA_CHECK(cudaEventRecord(hs().uploaded, copy_stream_));
   DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, hs().uploaded, 0));
+  const int set = hset_;
   hset_ ^= 1;
 
   FrontendArgs fa{};
@@ -537,21 +541,11 @@ void TpAccumulator::process() {
   fa.Tc = non_density_ ? Tc_d_.get() : Tr_d_.get();
   fa.Fb = Fb_.get();
   fa.G0 = G0_.get();
-  if (n_max_batch_ > 0) {
-    cudaEvent_t b = nullptr;
-    timeBegin(DCAACC_STAGE_TWIDDLE, &b);
-    int n_prep;
-    if (tc_front_) {
-      n_prep = launchFrontendTcPrep(fa, ftc_, ds.orb_r.get(), non_density_ ? ds.orb_c.get() : ds.orb_r.get(),
-                                    stream_);
-    }
-    else {
-      launchTwiddles(fa, stream_);
-      n_prep = non_density_ ? 2 : 1;
-    }
-    launches_ += n_prep;
-    timeEnd(DCAACC_STAGE_TWIDDLE, b, n_prep);
-  }
+  // Tensor-core path: the launch shapes take the order bound in steps of 128 (the GEMM tile);
+  // every kernel reads each sector's own order, so the results do not depend on it, and batches
+  // of similar orders share one captured graph.
+  if (tc_front_ && n_max_batch_ > 0)
+    fa.n_max = (n_max_batch_ + 127) / 128 * 128;
   G4Args ga{};
   ga.dims = dims_;
   ga.signs = ds.signs.get();
@@ -574,7 +568,40 @@ void TpAccumulator::process() {
   ga.gmax = tc_front_ ? gmax_d_.get() : nullptr;
   ga.tile_order = dims_.half_g4 ? tile_order_d_.get() : nullptr;
   ga.n_sm = ftc_.n_sm;
+
+  const bool graphable = graphs_on_ && tc_front_ && !timing_ && n_max_batch_ > 0 && stream_ != nullptr &&
+                         stream_ != cudaStreamLegacy && stream_ != cudaStreamPerThread;
+  if (graphable)
+    launches_ += launchBatchGraph(set, fa, ga, ds);
+  else
+    launches_ += launchBatch(fa, ga, ds);
+  DCAACC_CUDA_CHECK(cudaEventRecord(ds.consumed, stream_));
+  have_g_ = !mixed_;
+  slots_ = 0;
+  vtx_used_ = 0;
+  x_used_ = 0;
+  m_used_ = 0;
+  n_max_batch_ = 0;
+}
+
+// The kernels of one batch, all on stream_ and nothing else (the sequence a graph captures).
+int TpAccumulator::launchBatch(const FrontendArgs& fa, const G4Args& ga, DevStage& ds) {
+  int launched = 0;
   cudaEvent_t b = nullptr;
+  if (fa.n_max > 0) {
+    timeBegin(DCAACC_STAGE_TWIDDLE, &b);
+    int n_prep;
+    if (tc_front_) {
+      n_prep = launchFrontendTcPrep(fa, ftc_, ds.orb_r.get(), non_density_ ? ds.orb_c.get() : ds.orb_r.get(),
+                                    stream_);
+    }
+    else {
+      launchTwiddles(fa, stream_);
+      n_prep = non_density_ ? 2 : 1;
+    }
+    launched += n_prep;
+    timeEnd(DCAACC_STAGE_TWIDDLE, b, n_prep);
+  }
   timeBegin(DCAACC_STAGE_ROW, &b);
   if (tc_front_)
     launchFrontendTcRow(fa, ftc_, err_d_.get(), stream_);
@@ -595,14 +622,80 @@ void TpAccumulator::process() {
   const int g4_launches = mixed_ ? launchUpdateG4<float2>(ga, G32_.get(), g_sector_stride_, stream_)
                                  : launchUpdateG4<double2>(ga, G64_.get(), g_sector_stride_, stream_);
   timeEnd(DCAACC_STAGE_G4, b, g4_launches);
-  launches_ += 2 + g4_launches;
-  DCAACC_CUDA_CHECK(cudaEventRecord(ds.consumed, stream_));
-  have_g_ = !mixed_;
-  slots_ = 0;
-  vtx_used_ = 0;
-  x_used_ = 0;
-  m_used_ = 0;
-  n_max_batch_ = 0;
+  return launched + 2 + g4_launches;
+}
+
+// Replays the batch's kernel sequence from a CUDA graph keyed by (device input set, batch size,
+// order bound): the launch shapes and every pointer the kernels receive depend on nothing else
+// (per-batch data reaches them through the device input set).  A key's first batch runs eagerly
+// (lazy setup such as shared-memory attributes happens outside any capture), its second is
+// captured and instantiated, later ones replay.  At most kMaxGraphs executables are kept.
+int TpAccumulator::launchBatchGraph(int set, const FrontendArgs& fa, const G4Args& ga, DevStage& ds) {
+  constexpr size_t kMaxGraphs = 32;
+  BatchGraph* g = nullptr;
+  for (auto& x : graphs_)
+    if (x.set == set && x.slots == ga.n_slots && x.n_max == fa.n_max)
+      g = &x;
+  if (!g) {
+    if (graphs_.size() >= kMaxGraphs) {
+      auto lru = std::min_element(graphs_.begin(), graphs_.end(),
+                                  [](const BatchGraph& a, const BatchGraph& b) { return a.last < b.last; });
+      if (lru->exec)
+        cudaGraphExecDestroy(lru->exec);
+      graphs_.erase(lru);
+    }
+    graphs_.push_back(BatchGraph{set, ga.n_slots, fa.n_max, 0, nullptr, 0, 0});
+    g = &graphs_.back();
+  }
+  g->last = ++graph_stamp_;
+  if (g->uses++ == 0)
+    return launchBatch(fa, ga, ds);
+  if (!g->exec) {
+    DCAACC_CUDA_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+    int n = 0;
+    cudaGraph_t graph = nullptr;
+    try {
+      n = launchBatch(fa, ga, ds);
+    }
+    catch (...) {
+      if (cudaStreamEndCapture(stream_, &graph) == cudaSuccess && graph)
+        cudaGraphDestroy(graph);
+      cudaGetLastError();
+      throw;
+    }
+    DCAACC_CUDA_CHECK(cudaStreamEndCapture(stream_, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      g->exec = nullptr;
+      DCAACC_CUDA_CHECK(e);
+    }
+    g->launches = n;
+    ++graph_captures_;
+  }
+  DCAACC_CUDA_CHECK(cudaGraphLaunch(g->exec, stream_));
+  ++graph_replays_;
+  return g->launches;
+}
+
+void TpAccumulator::releaseGraphs() {
+  for (auto& g : graphs_)
+    if (g.exec)
+      cudaGraphExecDestroy(g.exec);
+  graphs_.clear();
+}
+
+void TpAccumulator::setGraphs(bool on) {
+  if (!on)
+    releaseGraphs();
+  graphs_on_ = on;
+}
+
+void TpAccumulator::graphStats(uint64_t* captures, uint64_t* replays) const {
+  if (captures)
+    *captures = graph_captures_;
+  if (replays)
+    *replays = graph_replays_;
 }
 
 double TpAccumulator::accumulate(const dcaacc_sector* sectors, int sign) {

@@ -119,6 +119,8 @@ public:
   }
   void enableTiming(bool on);
   void stageTimes(double* ms, uint64_t* launches, int n);
+  void setGraphs(bool on);
+  void graphStats(uint64_t* captures, uint64_t* replays) const;
   void peekG4(int channel, size_t offset, size_t count, double* out);
 
 private:
@@ -158,6 +160,20 @@ private:
   };
   DevStage dstage_[2];
   cudaStream_t copy_stream_ = nullptr;
+  int launchBatch(const FrontendArgs& fa, const G4Args& ga, DevStage& ds);
+  int launchBatchGraph(int set, const FrontendArgs& fa, const G4Args& ga, DevStage& ds);
+  // CUDA graphs of the tensor-core path's batch sequence (launchBatchGraph).
+  struct BatchGraph {
+    int set, slots, n_max;  // key: device input set, batch size, order bound
+    int uses;               // batches seen with this key
+    cudaGraphExec_t exec;   // instantiated on the key's second batch
+    int launches;           // kernels in the graph
+    uint64_t last;          // least-recently-used stamp
+  };
+  std::vector<BatchGraph> graphs_;
+  bool graphs_on_ = true;
+  uint64_t graph_stamp_ = 0, graph_captures_ = 0, graph_replays_ = 0;
+  void releaseGraphs();
   DevBuf<double2> Tr_d_, Tc_d_;
   DevBuf<double2> X64_, G64_;  // FP64 mode
   DevBuf<float2> X32_, G32_;   // mixed mode

@@ -180,6 +180,15 @@ enum { DCAACC_STAGE_TWIDDLE = 0, DCAACC_STAGE_ROW = 1, DCAACC_STAGE_COL = 2, DCA
 int dcaacc_tp_enable_timing(dcaacc_tp* acc, int32_t on);
 int dcaacc_tp_stage_times(dcaacc_tp* acc, double* ms, uint64_t* launches, int32_t n_stages);
 
+/* CUDA graphs of the mixed path's per-batch kernel sequence (no reference counterpart; the
+ * reference launches each kernel from the host per measurement).  On by default (environment
+ * DCAACC_TP_GRAPHS=0 turns them off at creation); used only on a non-default stream and while
+ * stage timing is off.  A batch shape's first batch runs eagerly, its second is captured, later
+ * ones replay the graph; the results are the same either way.  graph_stats reports the graphs
+ * captured and the batches replayed from one since creation (either pointer may be null). */
+int dcaacc_tp_set_graphs(dcaacc_tp* acc, int32_t on);
+int dcaacc_tp_graph_stats(const dcaacc_tp* acc, uint64_t* captures, uint64_t* replays);
+
 /* Reads count complex entries of one channel's running G4 starting at offset, without finalizing
  * (processes queued measurements first, then a synchronous device-to-host copy).  For monitoring
  * an accumulation in progress. */

@@ -161,6 +161,33 @@ def _small(wname, **kw):
     return dataclasses.replace(W.WORKLOADS[wname], **kw)
 
 
+def test_graph_replay_matches_eager(monkeypatch):
+    """The mixed path replays each batch shape's kernel sequence from a CUDA graph (captured on the
+    shape's second batch): the G4 equals, bit for bit, that of eager launches, and of a handle
+    created with DCAACC_TP_GRAPHS=0."""
+    from dca_b200.accumulators import TpAccumulator
+    w = _small("c3", n_range=(40, 120))
+    case = case_from_workload(w, 24)  # 6 batches of 4, three per device input set
+
+    def run(graphs, env="1"):
+        monkeypatch.setenv("DCAACC_TP_GRAPHS", env)
+        acc = TpAccumulator(case.G0, case.tp_params(precision=1, max_batch=4))
+        if not graphs:
+            acc.set_graphs(False)
+        acc.resetAccumulation(0)
+        for m in case.measurements:
+            acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+        acc.finalize()
+        return acc
+
+    graph, eager, off = run(True), run(False), run(True, env="0")
+    assert graph.graph_stats() == (2, 4)
+    assert eager.graph_stats() == (0, 0) and off.graph_stats() == (0, 0)
+    assert graph.kernel_launches() == eager.kernel_launches()
+    for g, e, o in zip(graph.get_G4(), eager.get_G4(), off.get_G4()):
+        assert np.array_equal(g, e) and np.array_equal(g, o)
+
+
 def test_large_cluster_fp64_matches_oracle(oracle_lib):
     """6x6 single band (Nc = 36): one momentum transfer's k1 x k2 block does not fit the tuned
     single-band kernel's thread block, so the FP64 update takes the general kernel."""
