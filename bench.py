@@ -300,11 +300,13 @@ def run_ours(args, world, rank, local):
         acc.accumulate_batch(M_src[base:base + B], configs[base:base + B], signs[base:base + B])
         acc.flush()
 
-    # Warm-up: at least four batches, so that both device input sets have their CUDA graph
-    # (captured on a batch shape's second batch) before the timed region.
-    warmup = max(args.warmup, 4)
-    for i in range(warmup):
-        step(i, dev_M)
+    # Warm-up: at least W batches, until the launch-shape tuner has chosen every tuned launch's
+    # shape (each candidate timed three times on real batches) and until both device input sets
+    # have their CUDA graph (captured after a batch of the shape ran without tuning probes).
+    warmup = 0
+    while warmup < args.warmup or ((not acc.tuning_settled() or acc.graph_stats()[0] < 2) and warmup < 64):
+        step(warmup, dev_M)
+        warmup += 1
     torch.cuda.synchronize()
     launches0 = acc.kernel_launches()
     graphs0 = acc.graph_stats()
@@ -358,8 +360,10 @@ def run_ours(args, world, rank, local):
         n_cmp = B
         ref_acc = TpAccumulator(g0, TpParameters.from_workload(w, cl, precision=0, max_batch=1))
         ref_acc.resetAccumulation(0)
-        for j in range(2):  # warm-up
-            ref_acc.accumulate(dev_M[j], configs[j], signs[j])
+        j = 0
+        while j < 2 or (not ref_acc.tuning_settled() and j < 256):  # warm-up, launch shapes tuned
+            ref_acc.accumulate(dev_M[j % len(dev_M)], configs[j % len(dev_M)], signs[j % len(dev_M)])
+            j += 1
         torch.cuda.synchronize()
         ref_acc.resetAccumulation(0)
         ref_acc.enable_timing(True)
@@ -480,6 +484,7 @@ def run_ours(args, world, rank, local):
         "e2e": e2e,
         "gpu_launches": int(launches),
         "cuda_graphs": graph_info,
+        "launch_tuning": [line for line in acc.tuning_report().splitlines() if line],
         "mirror_mode": {"half_g": bool(mirror & 1), "half_g4": bool(mirror & 2)},
         "roofline": roof,
         "update_g4_roofline": g4_roof,

@@ -118,6 +118,8 @@ def _load():
         "dcaacc_tp_stage_times": (i, [p, POINTER(c_double), POINTER(c_uint64), i]),
         "dcaacc_tp_set_graphs": (i, [p, i]),
         "dcaacc_tp_graph_stats": (i, [p, POINTER(c_uint64), POINTER(c_uint64)]),
+        "dcaacc_tp_tuning_settled": (i, [p]),
+        "dcaacc_tp_tuning_report": (i, [p, ctypes.c_char_p, sz, POINTER(sz)]),
         "dcaacc_tp_peek_g4": (i, [p, i, sz, sz, POINTER(c_double)]),
         "dcaacc_tp_compute_g_noalloc": (i, [POINTER(TpConfig), p, POINTER(Sector), p, p]),
         "dcaacc_sp_create": (i, [POINTER(SpConfig), POINTER(p)]),

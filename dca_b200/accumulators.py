@@ -327,6 +327,18 @@ class TpAccumulator:
         _check(N.lib.dcaacc_tp_graph_stats(self._h, ctypes.byref(cap), ctypes.byref(rep)))
         return cap.value, rep.value
 
+    def tuning_settled(self) -> bool:
+        """No problem shape is still being explored by the launch-shape tuner."""
+        return bool(N.lib.dcaacc_tp_tuning_settled(self._h))
+
+    def tuning_report(self) -> str:
+        """One line per tuned launch: key, candidates, choice, median ms per candidate."""
+        n = ctypes.c_size_t()
+        _check(N.lib.dcaacc_tp_tuning_report(self._h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        _check(N.lib.dcaacc_tp_tuning_report(self._h, buf, n.value + 1, ctypes.byref(n)))
+        return buf.value.decode()
+
     def peek_G4(self, channel: int, offset: int, count: int) -> np.ndarray:
         out = np.empty(count, np.complex128)
         _check(N.lib.dcaacc_tp_peek_g4(self._h, channel, offset, count, _dptr(out.view(np.float64))))

@@ -1,6 +1,8 @@
 // The C ABI (include/dcaacc.h): status codes around the accumulator objects.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
 #include <new>
 #include <string>
 
@@ -184,6 +186,25 @@ int dcaacc_tp_graph_stats(const dcaacc_tp* acc, uint64_t* captures, uint64_t* re
   if (!acc)
     return null_handle();
   return guard([&] { acc->impl.graphStats(captures, replays); });
+}
+
+int32_t dcaacc_tp_tuning_settled(const dcaacc_tp* acc) {
+  return acc ? acc->impl.tuningSettled() : 0;
+}
+
+int dcaacc_tp_tuning_report(dcaacc_tp* acc, char* buf, size_t cap, size_t* len) {
+  if (!acc)
+    return null_handle();
+  return guard([&] {
+    const std::string r = acc->impl.tuningReport();
+    if (len)
+      *len = r.size();
+    if (buf && cap) {
+      const size_t n = std::min(cap - 1, r.size());
+      std::memcpy(buf, r.data(), n);
+      buf[n] = '\0';
+    }
+  });
 }
 
 int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out) {

@@ -203,6 +203,9 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   Tr_d_.alloc(n_vtx * nw_ext);
   if (non_density_)
     Tc_d_.alloc(n_vtx * nw_ext);
+  // Launch-shape tuning (launch_tuner.hpp), unless DCAACC_TUNE=0 keeps the built-in shapes.
+  const char* tune_env = std::getenv("DCAACC_TUNE");
+  tuner_.setEnabled(!(tune_env && std::strcmp(tune_env, "0") == 0));
   const size_t x_elems = n_sec * size_t(R) * max_order_ * nw_ext;
   const size_t g_elems = n_sec * size_t(g_sector_stride_);
   if (mixed_) {
@@ -541,6 +544,7 @@ void TpAccumulator::process() {
   fa.Tc = non_density_ ? Tc_d_.get() : Tr_d_.get();
   fa.Fb = Fb_.get();
   fa.G0 = G0_.get();
+  fa.tuner = &tuner_;
   // Tensor-core path: the launch shapes take the order bound in steps of 128 (the GEMM tile);
   // every kernel reads each sector's own order, so the results do not depend on it, and batches
   // of similar orders share one captured graph.
@@ -568,6 +572,7 @@ void TpAccumulator::process() {
   ga.gmax = tc_front_ ? gmax_d_.get() : nullptr;
   ga.tile_order = dims_.half_g4 ? tile_order_d_.get() : nullptr;
   ga.n_sm = ftc_.n_sm;
+  ga.tuner = &tuner_;
 
   const bool graphable = graphs_on_ && tc_front_ && !timing_ && n_max_batch_ > 0 && stream_ != nullptr &&
                          stream_ != cudaStreamLegacy && stream_ != cudaStreamPerThread;
@@ -627,9 +632,10 @@ int TpAccumulator::launchBatch(const FrontendArgs& fa, const G4Args& ga, DevStag
 
 // Replays the batch's kernel sequence from a CUDA graph keyed by (device input set, batch size,
 // order bound): the launch shapes and every pointer the kernels receive depend on nothing else
-// (per-batch data reaches them through the device input set).  A key's first batch runs eagerly
-// (lazy setup such as shared-memory attributes happens outside any capture), its second is
-// captured and instantiated, later ones replay.  At most kMaxGraphs executables are kept.
+// (per-batch data reaches them through the device input set).  A key's batches run eagerly until
+// one has run without launch-shape probes (so lazy setup such as shared-memory attributes happens
+// outside any capture, and the tuned shapes are final); the next is captured and instantiated,
+// later ones replay.  At most kMaxGraphs executables are kept.
 int TpAccumulator::launchBatchGraph(int set, const FrontendArgs& fa, const G4Args& ga, DevStage& ds) {
   constexpr size_t kMaxGraphs = 32;
   BatchGraph* g = nullptr;
@@ -644,12 +650,16 @@ int TpAccumulator::launchBatchGraph(int set, const FrontendArgs& fa, const G4Arg
         cudaGraphExecDestroy(lru->exec);
       graphs_.erase(lru);
     }
-    graphs_.push_back(BatchGraph{set, ga.n_slots, fa.n_max, 0, nullptr, 0, 0});
+    graphs_.push_back(BatchGraph{set, ga.n_slots, fa.n_max, false, nullptr, 0, 0});
     g = &graphs_.back();
   }
   g->last = ++graph_stamp_;
-  if (g->uses++ == 0)
-    return launchBatch(fa, ga, ds);
+  if (!g->clean) {
+    const uint64_t p0 = tuner_.probes();
+    const int n = launchBatch(fa, ga, ds);
+    g->clean = tuner_.probes() == p0;
+    return n;
+  }
   if (!g->exec) {
     DCAACC_CUDA_CHECK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
     int n = 0;

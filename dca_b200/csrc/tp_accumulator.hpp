@@ -12,6 +12,7 @@
 
 #include <complex>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../include/dcaacc.h"
@@ -121,6 +122,12 @@ public:
   void stageTimes(double* ms, uint64_t* launches, int n);
   void setGraphs(bool on);
   void graphStats(uint64_t* captures, uint64_t* replays) const;
+  bool tuningSettled() const {
+    return tuner_.settled();
+  }
+  std::string tuningReport() {
+    return tuner_.report();
+  }
   void peekG4(int channel, size_t offset, size_t count, double* out);
 
 private:
@@ -165,12 +172,13 @@ private:
   // CUDA graphs of the tensor-core path's batch sequence (launchBatchGraph).
   struct BatchGraph {
     int set, slots, n_max;  // key: device input set, batch size, order bound
-    int uses;               // batches seen with this key
-    cudaGraphExec_t exec;   // instantiated on the key's second batch
+    bool clean;             // a batch of this key ran eagerly without launch-shape probes
+    cudaGraphExec_t exec;   // instantiated on the batch after the first clean one
     int launches;           // kernels in the graph
     uint64_t last;          // least-recently-used stamp
   };
   std::vector<BatchGraph> graphs_;
+  LaunchTuner tuner_;
   bool graphs_on_ = true;
   uint64_t graph_stamp_ = 0, graph_captures_ = 0, graph_replays_ = 0;
   void releaseGraphs();

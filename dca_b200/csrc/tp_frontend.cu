@@ -321,10 +321,10 @@ void launchTwiddles(const FrontendArgs& a, cudaStream_t stream) {
 
 constexpr int kRowJC = 32, kRowWC = 8, kRowIB = 64, kColJB = 64;
 
-template <typename Real>
+template <typename Real, int JC = kRowJC, int WC = kRowWC, int IB = kRowIB>
 static size_t rowSmem(const TpDims& d) {
-  return sizeof(cplx_t<Real>) * (kRowJC * kRowWC * d.n_orb + d.nb * d.nc * d.nc + kRowIB * kRowWC) +
-         sizeof(Real) * kRowJC * (kRowIB + 1) + sizeof(int) * (d.n_orb + 1);
+  return sizeof(cplx_t<Real>) * (JC * WC * d.n_orb + d.nb * d.nc * d.nc + IB * WC) +
+         sizeof(Real) * JC * (IB + 1) + sizeof(int) * (d.n_orb + 1);
 }
 
 template <typename Real>
@@ -344,25 +344,49 @@ static size_t colSmem(const TpDims& d, int wc2) {
          sizeof(int) * (d.n_orb + 1);
 }
 
+template <typename Real, int JC, int WC>
+static void launchRowTile(const FrontendArgs& a, cplx_t<Real>* Xp, cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  const size_t smem = rowSmem<Real, JC, WC>(d);
+  auto k = rowTransformKernel<Real, JC, WC, kRowIB>;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const dim3 grid(ceil_div(a.n_max, JC), ceil_div(d.nw_ext, WC), a.n_sectors);
+  k<<<grid, JC * WC, smem, stream>>>(d, a.sectors, a.perm_r, a.perm_c, a.row_start, a.Tr, a.Fb, Xp);
+  DCAACC_LAUNCH_CHECK();
+}
+
+// Tile shapes (vertices JC x frequencies WC per CTA, 256 threads) the tuner chooses among: each
+// X' element is the same sum in the same order whatever the tile.
 template <typename Real>
 void launchRowTransform(const FrontendArgs& a, cplx_t<Real>* Xp, cudaStream_t stream) {
   const TpDims& d = a.dims;
   if (a.n_max == 0)
     return;
-  const size_t smem = rowSmem<Real>(d);
-  auto k = rowTransformKernel<Real, kRowJC, kRowWC, kRowIB>;
-  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const dim3 grid(ceil_div(a.n_max, kRowJC), ceil_div(d.nw_ext, kRowWC), a.n_sectors);
-  k<<<grid, kRowJC * kRowWC, smem, stream>>>(d, a.sectors, a.perm_r, a.perm_c, a.row_start, a.Tr, a.Fb,
-                                             Xp);
-  DCAACC_LAUNCH_CHECK();
+  const size_t lim = 227 * 1024;
+  const bool fit16 = rowSmem<Real, 16, 16>(d) <= lim, fit64 = rowSmem<Real, 64, 4>(d) <= lim;
+  const int n_cand = fit16 ? (fit64 ? 3 : 2) : 1;
+  const auto pk = tunePick(a.tuner, tuneKey("row", d.nb, d.nc, d.nw_ext, a.n_max, a.n_sectors, sizeof(Real)),
+                           n_cand, stream);
+  if (pk.choice == 1)
+    launchRowTile<Real, 16, 16>(a, Xp, stream);
+  else if (pk.choice == 2)
+    launchRowTile<Real, 64, 4>(a, Xp, stream);
+  else
+    launchRowTile<Real, kRowJC, kRowWC>(a, Xp, stream);
+  tuneEnd(a.tuner, pk, stream);
 }
 
 template <typename Real>
 void launchColTransform(const FrontendArgs& a, const cplx_t<Real>* Xp, cplx_t<Real>* G,
                         long g_sector_stride, cudaStream_t stream) {
   const TpDims& d = a.dims;
-  const int wc2 = pickWC2<Real>(d);
+  // Candidates: the heuristic's column-frequency width and the next two halvings (each G element
+  // is the same sum in the same order whatever the width).
+  const int wc2_max = pickWC2<Real>(d);
+  const int n_cand = wc2_max >= 4 ? 3 : wc2_max == 2 ? 2 : 1;
+  const auto pk = tunePick(a.tuner, tuneKey("col", d.nb, d.nc, d.nw_ext, a.n_max, a.n_sectors, sizeof(Real)),
+                           n_cand, stream);
+  const int wc2 = wc2_max >> pk.choice;
   const size_t smem = colSmem<Real>(d, wc2);
   auto k = colTransformKernel<Real, kColJB>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -370,6 +394,7 @@ void launchColTransform(const FrontendArgs& a, const cplx_t<Real>* Xp, cplx_t<Re
   k<<<grid, d.R * wc2, smem, stream>>>(d, a.sectors, a.col_start, a.Tc, a.Fb, a.G0, Xp, G,
                                        g_sector_stride, wc2);
   DCAACC_LAUNCH_CHECK();
+  tuneEnd(a.tuner, pk, stream);
 }
 
 size_t frontendSmemRequirement(const TpDims& d, int /*n_max*/, bool fp64) {

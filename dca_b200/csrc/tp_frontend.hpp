@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "launch_tuner.hpp"
 #include "tp_layout.hpp"
 
 namespace dcaacc {
@@ -23,6 +24,7 @@ struct FrontendArgs {
   double2* Tc;                // packed twiddles, column-sorted order (== Tr when rows == cols)
   const double2* Fb;          // (r, k, b): e^{i k (r + a_b)}, nb * Nc * Nc
   const double2* G0;          // (b1, b2, k, w, s) over the extended mesh
+  LaunchTuner* tuner;         // launch-shape tuner (null: the built-in shapes)
 };
 
 void launchTwiddles(const FrontendArgs& a, cudaStream_t stream);

@@ -445,21 +445,31 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
     ++launches;
   }
   const long mrows = std::min<long>((a.n_max + kBN - 1) / kBN * kBN, s.Kr);
-  // Up to 8 warps per block, as many as their Kr-double rows fit in 200 KB of shared memory.
-  const int mwarps = static_cast<int>(std::max<long>(1, std::min<long>(8, 200L * 1024 / (8L * s.Kr))));
+  // Up to 8 warps per block, as many as their Kr-double rows fit in 200 KB of shared memory; the
+  // tuner may halve it (each row is one warp's work whatever the block).
+  const int mwarps_max = static_cast<int>(std::max<long>(1, std::min<long>(8, 200L * 1024 / (8L * s.Kr))));
+  const auto pm = tunePick(a.tuner, tuneKey("tc_m", d.nb, d.nc, d.nw_ext, a.n_max, a.n_sectors, 2),
+                           mwarps_max >= 2 ? 2 : 1, stream);
+  const int mwarps = mwarps_max >> pm.choice;
   const size_t msmem = sizeof(double) * mwarps * size_t(s.Kr);
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(buildMOperandKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(msmem)));
   buildMOperandKernel<<<dim3(static_cast<unsigned>((mrows + mwarps - 1) / mwarps), a.n_sectors), 32 * mwarps, msmem,
                         stream>>>(a.sectors, a.perm_r, a.perm_c, s.Kr, static_cast<__half*>(w.mb), w.mInv);
   DCAACC_LAUNCH_CHECK();
+  tuneEnd(a.tuner, pm, stream);
   if (a.Tc == a.Tr && orb_c == orb_r) {  // density-density: one pass for P and Q
+    // 256 or 128 threads per block (grid-stride loop over independent elements).
     const long groups4 = (a.n_max + kBK - 1) / kBK * (kBK / 4);
+    const auto pp = tunePick(a.tuner, tuneKey("tc_pq", d.nb, d.nc, d.nw_ext, a.n_max, a.n_sectors, 2), 2, stream);
+    const int threads = pp.choice == 0 ? 256 : 128;
+    const unsigned gx = static_cast<unsigned>(std::max(1L, std::min(8192L, (groups4 * d.nw_ext + threads - 1) / threads)));
     auto k = d.nb == 1 ? buildPhasePairKernel<true> : buildPhasePairKernel<false>;
-    k<<<dim3(gridX(groups4 * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
+    k<<<dim3(gx, a.n_sectors), threads, 0, stream>>>(
         d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, w.eQ, s.Dp, s.Dq, s.Kr, static_cast<__half*>(w.pr),
         static_cast<__half*>(w.bq));
     DCAACC_LAUNCH_CHECK();
+    tuneEnd(a.tuner, pp, stream);
     return launches + 2;
   }
   const long groups = (a.n_max + kBK - 1) / kBK * (kBK / 8);

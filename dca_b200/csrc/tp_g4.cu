@@ -616,21 +616,40 @@ static bool singlebandPHApplies(const TpDims& d) {
   return (size_t(d.R) * d.R * sizeof(GT)) % 16 == 0;
 }
 
-template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH, int MAXT, int MINB>
-static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_stride, int target_threads,
-                               cudaStream_t stream) {
+// Momentum transfers per CTA of updateG4SinglebandPH for a thread target, and its shared memory;
+// 0 when one transfer does not fit the launch bound or the CTA's shared memory.
+template <typename GT, typename AT, int KT, int MAXT>
+static int singlebandPHChunk(const G4Args& a, int target_threads, size_t* smem_out) {
   const TpDims& d = a.dims;
-  const int n_kc = (d.nc + KT - 1) / KT;
-  const int per_q = d.nc * n_kc;
+  const int per_q = d.nc * ((d.nc + KT - 1) / KT);
   if (per_q > MAXT)  // one q per CTA must fit the kernel's launch bound
-    return false;
+    return 0;
   const int q_chunk = std::max(1, std::min(d.nq, std::min(target_threads, MAXT) / per_q));
-  const int threads = per_q * q_chunk;
   const int n_stages = a.n_slots > 1 ? 2 : 1;
   const size_t smem = 16 + sizeof(GT) * n_stages * 8 * size_t(d.R) * d.R +
                       sizeof(cplx_t<AT>) * 4 * q_chunk * d.nc + sizeof(int) * d.nc * d.nc;
   if (smem > 220 * 1024)
+    return 0;
+  if (smem_out)
+    *smem_out = smem;
+  return q_chunk;
+}
+
+// Every G4 entry is summed over the batch by one thread in slot order whatever the number of
+// transfers per CTA, so the tuner may choose it: the q chunk for 256 threads or for 128.
+template <typename GT, typename AT, int KT, bool QFAST, bool PREFETCH, int MAXT, int MINB>
+static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  size_t smem = 0;
+  const int chunk_a = singlebandPHChunk<GT, AT, KT, MAXT>(a, 256, nullptr);
+  if (chunk_a == 0)
     return false;
+  const int chunk_b = singlebandPHChunk<GT, AT, KT, MAXT>(a, 128, nullptr);
+  const auto pk = tunePick(a.tuner, tuneKey("g4ph", d.nb, d.nc, d.nw_ext, d.nq, a.n_slots, sizeof(GT)),
+                           chunk_b != chunk_a ? 2 : 1, stream);
+  const int q_chunk = singlebandPHChunk<GT, AT, KT, MAXT>(a, pk.choice == 0 ? 256 : 128, &smem);
+  const int n_kc = (d.nc + KT - 1) / KT;
+  const int threads = d.nc * n_kc * q_chunk;
   auto k = updateG4SinglebandPH<GT, AT, KT, QFAST, PREFETCH, MAXT, MINB>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int n_qchunks = (d.nq + q_chunk - 1) / q_chunk;
@@ -638,6 +657,7 @@ static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_strid
   k<<<grid, threads, smem, stream>>>(d, G, g_sector_stride, a.signs, a.n_slots, a.k_add, a.q_list,
                                      a.wex_list, a.G4, a.atomic, q_chunk, n_kc, a.err);
   DCAACC_LAUNCH_CHECK();
+  tuneEnd(a.tuner, pk, stream);
   return true;
 }
 
@@ -650,9 +670,9 @@ int launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStrea
   if (singlebandPHApplies<GT>(a.dims)) {
     bool done;
     if constexpr (std::is_same_v<GT, double2>)
-      done = launchSinglebandPH<double2, double, 2, false, true, 256, 4>(a, G, g_sector_stride, 256, stream);
+      done = launchSinglebandPH<double2, double, 2, false, true, 256, 4>(a, G, g_sector_stride, stream);
     else
-      done = launchSinglebandPH<float2, float, 16, true, false, 256, 2>(a, G, g_sector_stride, 256, stream);
+      done = launchSinglebandPH<float2, float, 16, true, false, 256, 2>(a, G, g_sector_stride, stream);
     if (done)
       return 1;
   }

@@ -7,6 +7,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "launch_tuner.hpp"
 #include "tp_layout.hpp"
 
 namespace dcaacc {
@@ -27,6 +28,7 @@ struct G4Args {
   const int* gmax = nullptr;  // [2 slot + spin] largest |G| of each sector as float bits (or null)
   int n_sm = 0;               // multiprocessors (persistent grids)
   const unsigned* tile_order = nullptr;  // half_g4: the (w1 | w2 << 16) tiles to update, mirror pairs adjacent
+  LaunchTuner* tuner = nullptr;          // launch-shape tuner (null: the built-in shapes)
 };
 
 // Workspace of the tensor-core disconnected-term GEMM (tp_g4_disc.cu): U / V operand planes, their

@@ -189,6 +189,17 @@ int dcaacc_tp_stage_times(dcaacc_tp* acc, double* ms, uint64_t* launches, int32_
 int dcaacc_tp_set_graphs(dcaacc_tp* acc, int32_t on);
 int dcaacc_tp_graph_stats(const dcaacc_tp* acc, uint64_t* captures, uint64_t* replays);
 
+/* Launch-shape tuner (no reference counterpart).  Kernels with several launch shapes that give
+ * bit-identical results (tile widths, threads or warps per block) run each shape a few times on the
+ * handle's first batches of a given problem shape, timed with CUDA events, and keep the fastest.
+ * On by default; environment DCAACC_TUNE=0 keeps the built-in shapes.  tuning_settled is 1 when
+ * no problem shape is still being explored (graphs are captured only then).  tuning_report writes
+ * one line per tuned launch ("key n=<candidates> choice=<c> ms=<median per candidate>") as a
+ * NUL-terminated string of at most cap bytes into buf (which may be null) and the full length
+ * (without the NUL) into *len. */
+int32_t dcaacc_tp_tuning_settled(const dcaacc_tp* acc);
+int dcaacc_tp_tuning_report(dcaacc_tp* acc, char* buf, size_t cap, size_t* len);
+
 /* Reads count complex entries of one channel's running G4 starting at offset, without finalizing
  * (processes queued measurements first, then a synchronous device-to-host copy).  For monitoring
  * an accumulation in progress. */

@@ -168,6 +168,7 @@ def test_graph_replay_matches_eager(monkeypatch):
     from dca_b200.accumulators import TpAccumulator
     w = _small("c3", n_range=(40, 120))
     case = case_from_workload(w, 24)  # 6 batches of 4, three per device input set
+    monkeypatch.setenv("DCAACC_TUNE", "0")  # built-in launch shapes: graphs from the second batch on
 
     def run(graphs, env="1"):
         monkeypatch.setenv("DCAACC_TP_GRAPHS", env)
@@ -186,6 +187,39 @@ def test_graph_replay_matches_eager(monkeypatch):
     assert graph.kernel_launches() == eager.kernel_launches()
     for g, e, o in zip(graph.get_G4(), eager.get_G4(), off.get_G4()):
         assert np.array_equal(g, e) and np.array_equal(g, o)
+
+
+@pytest.mark.parametrize("precision,max_batch,n_meas", [(0, 1, 16), (1, 4, 48)])
+def test_tuned_launch_shapes_match_builtin(monkeypatch, precision, max_batch, n_meas):
+    """The launch-shape tuner times each candidate shape (FP64: row-transform tiles, column-transform
+    widths, transfers per G4 CTA; mixed: operand-builder blocks) on the first batches of a problem
+    shape and keeps the fastest.  Every candidate gives the same bits, so G4 equals that of the
+    built-in shapes (DCAACC_TUNE=0), and every tuned launch has decided."""
+    from dca_b200.accumulators import TpAccumulator
+    w = _small("c3", n_range=(40, 60))
+    case = case_from_workload(w, n_meas)
+
+    def run(tune):
+        monkeypatch.setenv("DCAACC_TUNE", tune)
+        acc = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=max_batch))
+        acc.resetAccumulation(0)
+        for m in case.measurements:
+            acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+        acc.finalize()
+        return acc
+
+    tuned, builtin = run("1"), run("0")
+    report = [line for line in tuned.tuning_report().splitlines() if line]
+    print("\n".join(report))
+    assert report and tuned.tuning_settled()
+    for line in report:  # "key n=<candidates> choice=<c> ms=<median per candidate>"
+        fields = dict(f.split("=", 1) for f in line.split()[1:])
+        ms = [float(x) for x in fields["ms"].split(",")]
+        assert len(ms) == int(fields["n"]) and min(ms) > 0
+        assert ms[int(fields["choice"])] == min(ms)
+    assert builtin.tuning_report() == "" and builtin.tuning_settled()
+    for a, b in zip(tuned.get_G4(), builtin.get_G4()):
+        assert np.array_equal(a, b)
 
 
 def test_large_cluster_fp64_matches_oracle(oracle_lib):
