@@ -218,8 +218,9 @@ class TpAccumulator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            N.lib.dcaacc_tp_destroy(h)
+        lib = getattr(N, "lib", None)  # None while the interpreter shuts down
+        if h and lib is not None:
+            lib.dcaacc_tp_destroy(h)
             self._h = None
 
     # -- reference method set ----------------------------------------------------------------
@@ -381,8 +382,9 @@ class SpAccumulator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            N.lib.dcaacc_sp_destroy(h)
+        lib = getattr(N, "lib", None)  # None while the interpreter shuts down
+        if h and lib is not None:
+            lib.dcaacc_sp_destroy(h)
             self._h = None
 
     def resetAccumulation(self):

@@ -585,6 +585,253 @@ updateG4SinglebandOuter(const TpDims dims, const float2* __restrict__ G, long g_
   }
 }
 
+// Direct term for clusters whose NC^3 sums per (w1, w2, wq) tile do not fit one CTA's registers
+// (Nc = 36: 46,656 complex sums): the same outer products as updateG4SinglebandOuter, with
+// NC / KG CTAs per tile, CTA g owning the rows k1 in [g KG, (g + 1) KG).  Per measurement and spin
+// a CTA stages the KG rows of the A block it reads and the whole B block (bulk copies, DEPTH
+// measurements deep); thread (d, k1 block, l1 block) keeps a TA x TB tile of sums in registers.
+// The flush table T[k2][k1 - g KG][q] covers the CTA's entries, and lanes write runs of KG
+// consecutive k1 of G4 (and read the disconnected terms in the same order).
+template <int NC, int KG, int TA, int TB, int DEPTH>
+__global__ void __launch_bounds__(NC * (KG / TA) * (NC / TB), 1)
+updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
+                             const int* __restrict__ signs, int n_slots, const int* __restrict__ k_sub,
+                             const int* __restrict__ q_list, const int* __restrict__ wex_list,
+                             const float2* __restrict__ disc, double2* const* __restrict__ G4, bool atomic,
+                             int* __restrict__ err) {
+  constexpr int BLK = NC * NC;
+  constexpr int AR = KG * NC;         // staged rows of A
+  constexpr int SP = AR + BLK;        // one spin's staged A rows + B block
+  constexpr int NKB = KG / TA, NLB = NC / TB;
+  constexpr int NT = NC * NKB * NLB;  // threads
+  constexpr int KSPLIT = NC / KG;
+  constexpr int QP = NC + 1;          // padded row of the flush table
+  static_assert(NC % KG == 0 && KG % TA == 0 && NC % TB == 0 && NT % 32 == 0, "tile shape");
+  const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq;
+  const int grp = blockIdx.x % KSPLIT;
+  const int tile = blockIdx.x / KSPLIT;  // the KSPLIT CTAs of a tile run next to each other
+  int w1, w2;
+  tileOfIndex(tile % (nw * nw), nw, w1, w2);
+  const int iwq = tile / (nw * nw);
+  const int wex = wex_list[iwq];
+  const int ext = dims.ext;
+  const int t = threadIdx.x;
+  const int d = t / (NKB * NLB), sub = t % (NKB * NLB);
+  const int kg0 = grp * KG;
+  const int k1_0 = kg0 + (sub / NLB) * TA, l1_0 = (sub % NLB) * TB;
+
+  const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
+  const long b_A = (static_cast<long>(w1e) * nw_ext + w2e) * BLK + static_cast<long>(kg0) * NC;
+  const long b_B = (static_cast<long>(w2x) * nw_ext + w1x) * BLK;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);     // [DEPTH] copies landed
+  uint64_t* empty = full + DEPTH;                              // [DEPTH] all warps done reading
+  int* ksub = reinterpret_cast<int*>(smem_raw + 16 * DEPTH);  // [NC * NC]
+  int* qinv = ksub + BLK;                                     // [NC]
+  constexpr int kHead = (16 * DEPTH + 4 * (BLK + NC) + 15) / 16 * 16;
+  float2* stage = reinterpret_cast<float2*>(smem_raw + kHead);  // [DEPTH][A0 rows, B0, A1 rows, B1]
+  float2* T = stage;                                           // flush table, after the batch loop
+  const int lane = t % 32;
+
+  for (int e = t; e < BLK; e += NT)
+    ksub[e] = k_sub[e];
+  for (int e = t; e < NC; e += NT)
+    qinv[q_list[e]] = e;
+
+  constexpr uint32_t a_bytes = AR * sizeof(float2), b_bytes = BLK * sizeof(float2);
+  auto issue = [&](int slot) {
+    const int st = slot % DEPTH;
+    float2* dst = stage + st * 2 * SP;
+    mbarArriveExpectTx(&full[st], 2 * (a_bytes + b_bytes));
+    const float2* src0 = G + g_sector_stride * (2 * slot);
+    const float2* src1 = src0 + g_sector_stride;
+    bulkCopyG2S(dst, src0 + b_A, a_bytes, &full[st]);
+    bulkCopyG2S(dst + AR, src0 + b_B, b_bytes, &full[st]);
+    bulkCopyG2S(dst + SP, src1 + b_A, a_bytes, &full[st]);
+    bulkCopyG2S(dst + SP + AR, src1 + b_B, b_bytes, &full[st]);
+  };
+  if (t == 0) {
+    for (int s2 = 0; s2 < DEPTH; ++s2) {
+      mbarInit(&full[s2], 1);
+      mbarInit(&empty[s2], NT / 32);
+    }
+    fenceBarrierInit();
+  }
+  __syncthreads();
+  if (t == 0)
+    for (int m = 0; m < DEPTH && m < n_slots; ++m)
+      issue(m);
+
+  // Fixed gather offsets: alpha from the staged A rows (row k1 - kg0, column k1 - d), beta from B
+  // (row l1 - d, column l1); two 16-bit offsets per register (SP < 2^16), so that the TA x TB sums
+  // stay in registers.
+  static_assert(SP < 65536, "16-bit gather offsets");
+  uint32_t oab[(TA + TB + 1) / 2];
+#pragma unroll
+  for (int i = 0; i < (TA + TB + 1) / 2; ++i)
+    oab[i] = 0;
+#pragma unroll
+  for (int a = 0; a < TA; ++a)
+    oab[a / 2] |= static_cast<uint32_t>((k1_0 + a - kg0) * NC + ksub[d + NC * (k1_0 + a)]) << (16 * (a & 1));
+#pragma unroll
+  for (int b = 0; b < TB; ++b)
+    oab[(TA + b) / 2] |= static_cast<uint32_t>(AR + ksub[d + NC * (l1_0 + b)] * NC + l1_0 + b)
+                         << (16 * ((TA + b) & 1));
+  auto off = [&](int i) { return static_cast<int>((oab[i / 2] >> (16 * (i & 1))) & 0xffffu); };
+
+  float2 acc[TA][TB];
+#pragma unroll
+  for (int a = 0; a < TA; ++a)
+#pragma unroll
+    for (int b = 0; b < TB; ++b)
+      acc[a][b] = make_float2(0.f, 0.f);
+
+  bool ok = true;
+  int sg = n_slots > 0 ? signs[0] : 1;
+  for (int m = 0; m < n_slots; ++m) {
+    const int st = m % DEPTH;
+    const int sg_next = m + 1 < n_slots ? signs[m + 1] : 1;
+    ok = __all_sync(0xffffffffu, mbarWait(&full[st], (m / DEPTH) & 1, err));
+    if (!ok)
+      break;
+    const bool add = sg < 0;
+#pragma unroll
+    for (int spin = 0; spin < 2; ++spin) {
+      const float2* S = stage + (st * 2 + spin) * SP;
+      float2 av[TA];
+#pragma unroll
+      for (int a = 0; a < TA; ++a)
+        av[a] = S[off(a)];
+      // One beta at a time: TA complex FMAs per beta load.
+#pragma unroll
+      for (int b = 0; b < TB; ++b) {
+        const float2 bv = S[off(TA + b)];
+        if (add) {
+#pragma unroll
+          for (int a = 0; a < TA; ++a)
+            cfma(acc[a][b], av[a], bv);
+        }
+        else {
+#pragma unroll
+          for (int a = 0; a < TA; ++a) {
+            float2& c = acc[a][b];
+            c.x = fmaf(-av[a].x, bv.x, c.x);
+            c.x = fmaf(av[a].y, bv.y, c.x);
+            c.y = fmaf(-av[a].x, bv.y, c.y);
+            c.y = fmaf(-av[a].y, bv.x, c.y);
+          }
+        }
+      }
+    }
+    sg = sg_next;
+    __syncwarp();
+    if (lane == 0)
+      mbarArrive(&empty[st]);  // release: this warp's reads of the stage are done
+    if (t == 0 && m + DEPTH < n_slots) {
+      if (!mbarWait(&empty[st], (m / DEPTH) & 1, err)) {
+        ok = false;  // the other warps see the missing copy as a timeout of their own
+        break;
+      }
+      issue(m + DEPTH);
+    }
+  }
+  if (__syncthreads_or(!ok))
+    return;  // uniform bail-out; the host reports the error word
+
+#pragma unroll
+  for (int a = 0; a < TA; ++a)
+#pragma unroll
+    for (int b = 0; b < TB; ++b) {
+      const int k1 = k1_0 + a, l1 = l1_0 + b;
+      const int k2 = ksub[d + NC * k1];
+      const int qi = qinv[ksub[k1 + NC * l1]];
+      T[(k2 * KG + k1 - kg0) * QP + qi] = make_float2(0.5f * acc[a][b].x, 0.5f * acc[a][b].y);
+    }
+  __syncthreads();
+  const long M = static_cast<long>(NC) * nw;
+  const long s_w1 = NC, s_k2 = s_w1 * nw, s_w2 = s_k2 * NC, s_q = s_w2 * nw, s_wq = s_q * nq;
+  const int n_ch = dims.n_channels;
+  constexpr int U = 4;
+  const int total = KG * NC * nq;
+  for (int base = t; base < total; base += U * NT) {
+    float2 v[U];
+    long g4i[U], di[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = min(base + u * NT, total - 1);
+      const int fk1l = idx % KG, j = (idx / KG) % NC, fqi = idx / (KG * NC);
+      const int fk1 = kg0 + fk1l;
+      v[u] = T[(j * KG + fk1l) * QP + fqi];
+      g4i[u] = fk1 + w1 * s_w1 + j * s_k2 + w2 * s_w2 + fqi * s_q + iwq * s_wq;
+      di[u] = (static_cast<long>(iwq * nq + fqi) * n_ch * M + j + static_cast<long>(NC) * w2) * M + fk1 +
+              static_cast<long>(NC) * w1;
+    }
+    for (int c = 0; c < n_ch; ++c) {
+      float2 dv[U];
+      double2 o[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        dv[u] = __ldg(disc + di[u] + static_cast<long>(c) * M * M);
+        o[u] = atomic ? make_double2(0., 0.) : G4[c][g4i[u]];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (base + u * NT >= total)
+          continue;
+        double2* p = G4[c] + g4i[u];
+        const double re = static_cast<double>(v[u].x + dv[u].x), im = static_cast<double>(v[u].y + dv[u].y);
+        if (atomic) {
+          atomicAdd(&p->x, re);
+          atomicAdd(&p->y, im);
+        }
+        else {
+          o[u].x += re;
+          o[u].y += im;
+          *p = o[u];
+        }
+      }
+    }
+  }
+}
+
+// Nc = 36: 3 CTAs per tile (12 rows k1 each), 6 measurements staged (166 KB; the flush table,
+// 128 KB, reuses the staging); per thread 3 x 9 sums (576 threads) or 6 x 9 (288 threads), which
+// the launch-shape tuner chooses between (same sums in the same order either way).
+constexpr int kSplitNc = 36, kSplitKG = 12, kSplitTB = 9, kSplitDepth = 6;
+
+size_t outerSplitSmem() {
+  constexpr int BLK = kSplitNc * kSplitNc;
+  constexpr size_t head = (16 * kSplitDepth + 4 * (BLK + kSplitNc) + 15) / 16 * 16;
+  const size_t loop = sizeof(float2) * kSplitDepth * 2 * (kSplitKG * kSplitNc + BLK);
+  const size_t table = sizeof(float2) * size_t(kSplitNc) * kSplitKG * (kSplitNc + 1);
+  return head + std::max(loop, table);
+}
+
+template <int TA>
+void launchOuterSplitTA(const G4Args& a, const float2* G, long stride, const float2* disc, cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  const size_t smem = outerSplitSmem();
+  auto k = updateG4SinglebandOuterSplit<kSplitNc, kSplitKG, TA, kSplitTB, kSplitDepth>;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long blocks = long(d.nw) * d.nw * d.nwq * (kSplitNc / kSplitKG);
+  constexpr int threads = kSplitNc * (kSplitKG / TA) * (kSplitNc / kSplitTB);
+  k<<<static_cast<unsigned>(blocks), threads, smem, stream>>>(d, G, stride, a.signs, a.n_slots, a.k_sub,
+                                                              a.q_list, a.wex_list, disc, a.G4, a.atomic,
+                                                              a.err);
+  DCAACC_LAUNCH_CHECK();
+}
+
+void launchOuterSplit(const G4Args& a, const float2* G, long stride, const float2* disc, cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  const auto pk = tunePick(a.tuner, tuneKey("g4split", d.nb, d.nc, d.nw_ext, d.nq, a.n_slots, 8), 2, stream);
+  if (pk.choice == 1)
+    launchOuterSplitTA<6>(a, G, stride, disc, stream);
+  else
+    launchOuterSplitTA<3>(a, G, stride, disc, stream);
+  tuneEnd(a.tuner, pk, stream);
+}
+
 template <int NC>
 struct OuterTile;  // per-thread tile (k1 x l1) of the outer-product kernel
 // A beta gather B[l1 - d][l1] falls in the bank of column l1, so the threads of a warp that read
@@ -694,13 +941,23 @@ int launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sec
       return launchForNc<4>(a, G, g_sector_stride, mag, charge, stream);
     case 8:
       return launchForNc<8>(a, G, g_sector_stride, mag, charge, stream);
+    case kSplitNc:
+      // Disconnected terms on the tensor cores and the split direct term; without the workspace
+      // or with a subset of the transfers, the general one-band kernel (return 0).
+      if (!a.q_all || a.dims.half_g4)
+        return 0;
+      if (const float2* disc = launchDiscGemm(a, G, g_sector_stride, stream)) {
+        launchOuterSplit(a, G, g_sector_stride, disc, stream);
+        return 3;
+      }
+      return 0;
     default:
       return launchForNc<16>(a, G, g_sector_stride, mag, charge, stream);
   }
 }
 
 bool singlebandBatchedApplies(const TpDims& d) {
-  if (d.nb != 1 || (d.nc != 4 && d.nc != 8 && d.nc != 16))
+  if (d.nb != 1 || (d.nc != 4 && d.nc != 8 && d.nc != 16 && d.nc != kSplitNc))
     return false;
   for (int c = 0; c < d.n_channels; ++c)
     if (d.channels[c] != 2 && d.channels[c] != 3)

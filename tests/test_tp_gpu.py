@@ -233,6 +233,28 @@ def test_large_cluster_fp64_matches_oracle(oracle_lib):
         assert rel_err(got, want) <= FP64_TOL
 
 
+@pytest.mark.parametrize("channels", [(2,), (2, 3)])
+def test_large_cluster_mixed_split_direct_term(oracle_lib, channels):
+    """6x6 single band, all 36 momentum transfers, batches of 3: the mixed path takes the
+    disconnected terms on the tensor cores and the direct term on the split outer-product kernel
+    (three CTAs per frequency tile, 12 rows k1 each).  Against the oracle (FP64), and the G4
+    stage must be those three launches per batch."""
+    w = _small("c5", nw_half=2, n_sp=64, n_range=(20, 40), channels=channels)
+    case = case_from_workload(w, 7)
+    from dca_b200.accumulators import TpAccumulator
+    acc = TpAccumulator(case.G0, case.tp_params(precision=1, max_batch=3))
+    acc.enable_timing(True)
+    acc.resetAccumulation(0)
+    for m in case.measurements:
+        acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    acc.finalize()
+    assert acc.stage_times()["update_g4"][1] == 3 * 3  # 3 batches (3 + 3 + 1 measurements)
+    ora = run_oracle(oracle_lib, case)
+    for got, want in zip(acc.get_G4(), ora.get_G4()):
+        print("split direct term, relative error:", rel_err(got, want))
+        assert rel_err(got, want) <= MIXED_TOL
+
+
 @pytest.mark.parametrize("channels", [(4,), (2, 3)])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_multiband_batched_matches_oracle(oracle_lib, channels, precision):
