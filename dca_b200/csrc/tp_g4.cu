@@ -187,9 +187,11 @@ updateG4Kernel(const TpDims dims, const GT* __restrict__ G, long g_sector_stride
 // steps form one sequence, so the ring keeps running across chunks.
 //   A = G(w1; w2)  B = G(w2+x; w1+x)  C = G(w1; w1+x)  E = G(w2+x; w2)  P = G(m1; m2)
 constexpr int kStagedMaxCh = 2;
-constexpr int kStagedEpt = 4;
 
-template <typename GT, typename AT>
+// EPT entries per thread: every chunk of EPT x 256 entries re-stages the tile's blocks for each
+// measurement, so a larger EPT cuts that traffic; NCH = number of channels (registers for NCH only).
+// The sum of an entry is the same whatever EPT, so the launch-shape tuner chooses it.
+template <typename GT, typename AT, int EPT, int NCH>
 __global__ void __launch_bounds__(256)
 updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_stride,
                      const int* __restrict__ signs, int n_slots, const int* __restrict__ k_add,
@@ -197,7 +199,7 @@ updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_
                      const int* __restrict__ wex_list, double2* const* __restrict__ G4, bool atomic,
                      int* __restrict__ err) {
   using C = cplx_t<AT>;
-  constexpr int EPT = kStagedEpt;
+  static_assert(NCH >= 1 && NCH <= kStagedMaxCh, "channels");
   const int nb = dims.nb, nc = dims.nc, nw = dims.nw, nw_ext = dims.nw_ext, R = dims.R;
   const int w1 = blockIdx.x, w2 = blockIdx.y, iwq = blockIdx.z;
   const int wex = wex_list[iwq];
@@ -271,8 +273,8 @@ updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_
     // This chunk's entries: G4 index and, per channel, the shared-memory offsets of the two G
     // elements of the second-order term (id in A, ie in B or P) and, for PH magnetic / charge,
     // of the disconnected-term elements (iu in C, iv in E).
-    long g4i[EPT];
-    int id[EPT][kStagedMaxCh], ie[EPT][kStagedMaxCh], iu[EPT], iv[EPT];
+    int g4o[EPT];  // offset from the tile base (a tile holds fewer than 2^31 entries)
+    int id[EPT][NCH], ie[EPT][NCH], iu[EPT], iv[EPT];
     bool live[EPT];
 #pragma unroll
     for (int e = 0; e < EPT; ++e) {
@@ -287,12 +289,12 @@ updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_
       const int q = q_list[iq];
       const int k1q = k_add[k1 + nc * q], k2q = k_add[k2 + nc * q];
       auto rc = [&](int b, int k) { return b + nb * k; };
-      g4i[e] = tile_base + in + k2 * s_k2 + iq * s_q;
+      g4o[e] = static_cast<int>(in + k2 * s_k2 + iq * s_q);
       iu[e] = rc(b1, k1) * R + rc(b2, k1q);
       iv[e] = rc(b4, k2q) * R + rc(b3, k2);
 #pragma unroll
-      for (int c = 0; c < kStagedMaxCh; ++c) {
-        const int ch = c < n_ch ? dims.channels[c] : 0;
+      for (int c = 0; c < NCH; ++c) {
+        const int ch = dims.channels[c];
         if (ch == 2) {
           id[e][c] = rc(b1, k1) * R + rc(b3, k2);
           ie[e][c] = rc(b4, k2q) * R + rc(b2, k1q);
@@ -312,11 +314,11 @@ updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_
         }
       }
     }
-    C acc[EPT][kStagedMaxCh];
+    C acc[EPT][NCH];
 #pragma unroll
     for (int e = 0; e < EPT; ++e)
 #pragma unroll
-      for (int c = 0; c < kStagedMaxCh; ++c)
+      for (int c = 0; c < NCH; ++c)
         acc[e][c] = mk(AT(0), AT(0));
 
     for (int slot = 0; slot < n_slots; ++slot, ++step) {
@@ -333,9 +335,7 @@ updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_
         if (!live[e])
           continue;
 #pragma unroll
-        for (int c = 0; c < kStagedMaxCh; ++c) {
-          if (c >= n_ch)
-            break;
+        for (int c = 0; c < NCH; ++c) {
           const int ch = dims.channels[c];
           C v;
           if (ch == 2 || ch == 3) {
@@ -388,10 +388,8 @@ updateG4StagedKernel(const TpDims dims, const GT* __restrict__ G, long g_sector_
       if (!live[e])
         continue;
 #pragma unroll
-      for (int c = 0; c < kStagedMaxCh; ++c) {
-        if (c >= n_ch)
-          break;
-        double2* p = G4[c] + g4i[e];
+      for (int c = 0; c < NCH; ++c) {
+        double2* p = G4[c] + tile_base + g4o[e];
         if (atomic) {
           atomicAdd(&p->x, static_cast<double>(acc[e][c].x));
           atomicAdd(&p->y, static_cast<double>(acc[e][c].y));
@@ -692,11 +690,18 @@ int launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStrea
     const size_t smem = 16 + 2 * 2 * size_t(nblk) * a.dims.R * a.dims.R * sizeof(GT);
     if (smem <= 200 * 1024) {
       using AT = std::conditional_t<std::is_same_v<GT, double2>, double, float>;
-      auto k = updateG4StagedKernel<GT, AT>;
+      // Entries per thread: 4 (candidate 0), 8 or 16.
+      const auto pk = tunePick(a.tuner, tuneKey("g4staged", a.dims.nb, a.dims.nc, a.dims.nw_ext, a.dims.nq,
+                                                a.n_slots, sizeof(GT)), 3, stream);
+      const bool two = a.dims.n_channels == 2;
+      auto k = pk.choice == 2 ? (two ? updateG4StagedKernel<GT, AT, 16, 2> : updateG4StagedKernel<GT, AT, 16, 1>)
+               : pk.choice == 1 ? (two ? updateG4StagedKernel<GT, AT, 8, 2> : updateG4StagedKernel<GT, AT, 8, 1>)
+                                : (two ? updateG4StagedKernel<GT, AT, 4, 2> : updateG4StagedKernel<GT, AT, 4, 1>);
       DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
       k<<<grid, 256, smem, stream>>>(a.dims, G, g_sector_stride, a.signs, a.n_slots, a.k_add, a.k_sub, a.q_list,
                                      a.wex_list, a.G4, a.atomic, a.err);
       DCAACC_LAUNCH_CHECK();
+      tuneEnd(a.tuner, pk, stream);
       return 1;
     }
   }

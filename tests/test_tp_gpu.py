@@ -189,14 +189,19 @@ def test_graph_replay_matches_eager(monkeypatch):
         assert np.array_equal(g, e) and np.array_equal(g, o)
 
 
-@pytest.mark.parametrize("precision,max_batch,n_meas", [(0, 1, 16), (1, 4, 48)])
-def test_tuned_launch_shapes_match_builtin(monkeypatch, precision, max_batch, n_meas):
+@pytest.mark.parametrize("wname,precision,max_batch,n_meas", [("c3", 0, 1, 16), ("c3", 1, 4, 48),
+                                                              ("c4", 1, 2, 24)])
+def test_tuned_launch_shapes_match_builtin(monkeypatch, wname, precision, max_batch, n_meas):
     """The launch-shape tuner times each candidate shape (FP64: row-transform tiles, column-transform
-    widths, transfers per G4 CTA; mixed: operand-builder blocks) on the first batches of a problem
-    shape and keeps the fastest.  Every candidate gives the same bits, so G4 equals that of the
-    built-in shapes (DCAACC_TUNE=0), and every tuned launch has decided."""
+    widths, transfers per G4 CTA; mixed: operand-builder blocks, and for three bands the staged G4
+    kernel's entries per thread) on the first batches of a problem shape and keeps the fastest.
+    Every candidate gives the same bits, so G4 equals that of the built-in shapes (DCAACC_TUNE=0),
+    and every tuned launch has decided."""
     from dca_b200.accumulators import TpAccumulator
-    w = _small("c3", n_range=(40, 60))
+    if wname == "c3":
+        w = _small("c3", n_range=(40, 60))
+    else:
+        w = _small("c4", nw_half=4, n_sp=64, n_range=(20, 40), freq_transfer=1)
     case = case_from_workload(w, n_meas)
 
     def run(tune):
