@@ -63,6 +63,7 @@ class SpConfig(ctypes.Structure):
         ("r_sub", POINTER(c_int32)),
         ("accumulate_m_sqr", c_int32),
         ("max_order", c_int32),
+        ("stamping", c_int32),
     ]
 
 
@@ -134,6 +135,11 @@ def _load():
         "dcaacc_sp_synchronize": (i, [p]),
         "dcaacc_sp_device_fingerprint": (sz, [p]),
         "dcaacc_sp_kernel_launches": (c_uint64, [p]),
+        "dcaacc_sp_get_single_measurement_m_r_w": (i, [p, POINTER(c_double), sz]),
+        "dcaacc_sp_get_single_measurement_f_tau": (i, [p, POINTER(c_double), sz]),
+        "dcaacc_sp_clear_single_measurement": (i, [p]),
+        "dcaacc_sp_f_tau_size": (sz, [p]),
+        "dcaacc_tp_static_device_fingerprint": (sz, []),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -299,6 +299,11 @@ class TpAccumulator:
     def deviceFingerprint(self) -> int:
         return N.lib.dcaacc_tp_device_fingerprint(self._h)
 
+    @staticmethod
+    def staticDeviceFingerprint() -> int:
+        """Device bytes held process-wide (the allocation-free entry point's static scratch)."""
+        return N.lib.dcaacc_tp_static_device_fingerprint()
+
     def kernel_launches(self) -> int:
         return N.lib.dcaacc_tp_kernel_launches(self._h)
 
@@ -357,6 +362,7 @@ class SpParameters:
     beta: float
     r_sub: np.ndarray  # [i, j] = index of r_j - r_i
     max_order: int = 512
+    stamping: bool = False  # keep the last measurement's own f(tau) (stamping_period() > 0)
 
     @classmethod
     def from_workload(cls, w: W.Workload, cluster: Optional[W.Cluster] = None, **kw):
@@ -375,7 +381,7 @@ class SpAccumulator:
         self.parameters = p
         self._rsub = np.ascontiguousarray(np.asarray(p.r_sub, np.int32).T)
         cfg = N.SpConfig(p.n_bands, p.n_sites, p.n_sp_freq, p.beta, _iptr(self._rsub),
-                         int(accumulate_m_squared), p.max_order)
+                         int(accumulate_m_squared), p.max_order, int(p.stamping))
         self._sqr = bool(accumulate_m_squared)
         self._h = ctypes.c_void_p()
         _check(N.lib.dcaacc_sp_create(ctypes.byref(cfg), ctypes.byref(self._h)))
@@ -412,6 +418,27 @@ class SpAccumulator:
 
     def get_sign_times_M_r_w_sqr(self) -> np.ndarray:
         return self._get(True)
+
+    def get_single_measurement_sign_times_MFunction(self) -> np.ndarray:
+        """M(r, w) of the last measurement alone (stamping), computed on each call."""
+        p = self.parameters
+        size = (2 * p.n_bands) ** 2 * p.n_sites * 2 * p.n_sp_freq
+        out = np.empty(size, np.complex128)
+        _check(N.lib.dcaacc_sp_get_single_measurement_m_r_w(
+            self._h, out.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)), size))
+        return out
+
+    def get_single_measurement_sign_times_MFunction_time(self) -> np.ndarray:
+        """The last measurement's f(tau): [spin][label][padded time], FP64."""
+        size = N.lib.dcaacc_sp_f_tau_size(self._h)
+        out = np.empty(size, np.float64)
+        _check(N.lib.dcaacc_sp_get_single_measurement_f_tau(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), size))
+        p = self.parameters
+        return out.reshape(2, p.n_bands ** 2 * p.n_sites, -1)
+
+    def clearSingleMeasurement(self):
+        _check(N.lib.dcaacc_sp_clear_single_measurement(self._h))
 
     def sumTo(self, other: "SpAccumulator"):
         _check(N.lib.dcaacc_sp_sum_to(self._h, other._h))

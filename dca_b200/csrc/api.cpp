@@ -14,6 +14,7 @@
 namespace dcaacc {
 void computeGNoAlloc(const dcaacc_tp_config& c, const double* G0_dev, const dcaacc_sector* sec,
                      double* G_out, cudaStream_t stream);
+size_t staticScratchBytes();
 }
 
 struct dcaacc_tp {
@@ -164,6 +165,10 @@ uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc) {
   return acc ? acc->impl.kernelLaunches() : 0;
 }
 
+size_t dcaacc_tp_static_device_fingerprint(void) {
+  return dcaacc::staticScratchBytes();
+}
+
 int dcaacc_tp_enable_timing(dcaacc_tp* acc, int32_t on) {
   if (!acc)
     return null_handle();
@@ -259,6 +264,28 @@ int dcaacc_sp_get_m_r_w_sqr(const dcaacc_sp* acc, double* out, size_t count) {
   if (!acc || !out)
     return null_handle();
   return guard([&] { acc->impl.get(true, out, count); });
+}
+
+int dcaacc_sp_get_single_measurement_m_r_w(dcaacc_sp* acc, double* out, size_t count) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.singleMeasurementMrw(out, count); });
+}
+
+int dcaacc_sp_get_single_measurement_f_tau(dcaacc_sp* acc, double* out, size_t count) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.singleMeasurementFtau(out, count); });
+}
+
+int dcaacc_sp_clear_single_measurement(dcaacc_sp* acc) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.clearSingleMeasurement(); });
+}
+
+size_t dcaacc_sp_f_tau_size(const dcaacc_sp* acc) {
+  return acc ? acc->impl.fTauSize() : 0;
 }
 
 int dcaacc_sp_sum_to(const dcaacc_sp* acc, dcaacc_sp* other) {

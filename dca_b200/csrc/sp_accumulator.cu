@@ -45,7 +45,8 @@ __global__ void spAccumulateKernel(const NfftGrid g, const SpSector* __restrict_
                                    const int* __restrict__ row_start, const int* __restrict__ col_start,
                                    const double* __restrict__ tau, const int* __restrict__ r_of,
                                    const double* __restrict__ coeff, double factor,
-                                   double* __restrict__ f_tau, double* __restrict__ f_tau_sqr) {
+                                   double* __restrict__ f_tau, double* __restrict__ f_tau_sqr,
+                                   double* __restrict__ f_tau_single) {
   extern __shared__ __align__(16) double sp_smem[];
   double* row = sp_smem;
   double* row_sqr = sp_smem + g.n_padded;
@@ -103,6 +104,11 @@ __global__ void spAccumulateKernel(const NfftGrid g, const SpSector* __restrict_
   double* out = f_tau + (static_cast<long>(spin) * g.n_labels + label) * g.n_padded;
   for (int t = threadIdx.x; t < g.n_padded; t += blockDim.x)
     out[t] += row[t];
+  if (f_tau_single) {  // this measurement alone (replaces the previous one)
+    double* one = f_tau_single + (static_cast<long>(spin) * g.n_labels + label) * g.n_padded;
+    for (int t = threadIdx.x; t < g.n_padded; t += blockDim.x)
+      one[t] = row[t];
+  }
   if (sqr) {
     double* out2 = f_tau_sqr + (static_cast<long>(spin) * g.n_labels + label) * g.n_padded;
     for (int t = threadIdx.x; t < g.n_padded; t += blockDim.x)
@@ -226,12 +232,13 @@ struct SpAccumulator::Impl {
   int n_sp = 0, max_order = 0;
   double beta = 0;
   bool sqr = false;
+  bool stamping = false;
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   cudaEvent_t upload_done = nullptr;
   std::vector<int> r_of;
-  DevBuf<double> coeff, inv_phi, f_tau, f_tau_sqr, tau_d, M_d;
+  DevBuf<double> coeff, inv_phi, f_tau, f_tau_sqr, f_tau_single, tau_d, M_d;
   DevBuf<int> r_of_d, perm_r_d, perm_c_d, rs_d, cs_d;
   DevBuf<SpSector> sectors_d;
   DevBuf<double2> out_d;
@@ -253,6 +260,7 @@ SpAccumulator::SpAccumulator(const dcaacc_sp_config& c) : d_(new Impl) {
   d.n_sp = c.n_sp_freq;
   d.beta = c.beta;
   d.sqr = c.accumulate_m_sqr != 0;
+  d.stamping = c.stamping != 0;
   d.max_order = c.max_order;
   // r_of[r_j + nc dr] = r_i with r_sub(r_j, r_i) = dr, i.e. x_{r_i} - x_{r_j} = x_dr.
   d.r_of.assign(nc * nc, -1);
@@ -319,6 +327,8 @@ SpAccumulator::SpAccumulator(const dcaacc_sp_config& c) : d_(new Impl) {
   d.f_tau.alloc(ft);
   if (d.sqr)
     d.f_tau_sqr.alloc(ft);
+  if (d.stamping)
+    d.f_tau_single.alloc(ft);
   const size_t nv = 2 * size_t(d.max_order);
   d.tau_d.alloc(nv);
   d.M_d.alloc(2 * size_t(d.max_order) * d.max_order);
@@ -353,6 +363,8 @@ void SpAccumulator::reset() {
   DCAACC_CUDA_CHECK(cudaMemsetAsync(d.f_tau.get(), 0, d.f_tau.bytes(), d.stream));
   if (d.sqr)
     DCAACC_CUDA_CHECK(cudaMemsetAsync(d.f_tau_sqr.get(), 0, d.f_tau_sqr.bytes(), d.stream));
+  if (d.stamping)
+    DCAACC_CUDA_CHECK(cudaMemsetAsync(d.f_tau_single.get(), 0, d.f_tau_single.bytes(), d.stream));
   d.ready = true;
   d.finalized = false;
 }
@@ -412,8 +424,11 @@ void SpAccumulator::accumulate(const dcaacc_sector* sec, double factor) {
     d.sectors_h[s] = sd;
     vtx += x.n;
   }
-  if (vtx == 0)
+  if (vtx == 0) {
+    if (d.stamping)  // an empty measurement: its own f(tau) is zero
+      DCAACC_CUDA_CHECK(cudaMemsetAsync(d.f_tau_single.get(), 0, d.f_tau_single.bytes(), d.stream));
     return;
+  }
   auto h2d = [&](void* dst, const void* src, size_t bytes) {
     if (bytes)
       DCAACC_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, d.stream));
@@ -430,31 +445,68 @@ void SpAccumulator::accumulate(const dcaacc_sector* sec, double factor) {
   spAccumulateKernel<<<dim3(g.n_labels, 2), 256, smem, d.stream>>>(
       g, d.sectors_d.get(), d.perm_r_d.get(), d.perm_c_d.get(), d.rs_d.get(), d.cs_d.get(),
       d.tau_d.get(), d.r_of_d.get(), d.coeff.get(), factor, d.f_tau.get(),
-      d.sqr ? d.f_tau_sqr.get() : nullptr);
+      d.sqr ? d.f_tau_sqr.get() : nullptr, d.stamping ? d.f_tau_single.get() : nullptr);
   DCAACC_LAUNCH_CHECK();
   ++d.launches;
 }
 
 void SpAccumulator::finalize() {
   auto& d = *d_;
-  auto& g = d.g;
   if (d.finalized)
     return;
-  const size_t smem = sizeof(double) * 3 * g.n;
-  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(spFinalizeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  auto run = [&](const double* ft, std::vector<double2>& host) {
-    DCAACC_CUDA_CHECK(cudaMemsetAsync(d.out_d.get(), 0, d.out_d.bytes(), d.stream));
-    spFinalizeKernel<<<dim3(g.n_labels, 2), 256, smem, d.stream>>>(g, ft, d.inv_phi.get(), d.n_sp, d.out_d.get());
-    DCAACC_LAUNCH_CHECK();
-    ++d.launches;
-    host.resize(d.out_d.size());
-    DCAACC_CUDA_CHECK(cudaMemcpyAsync(host.data(), d.out_d.get(), d.out_d.bytes(), cudaMemcpyDeviceToHost, d.stream));
-  };
-  run(d.f_tau.get(), d.mrw);
+  finalizeInto(d.f_tau.get(), d.mrw);
   if (d.sqr)
-    run(d.f_tau_sqr.get(), d.mrw_sqr);
+    finalizeInto(d.f_tau_sqr.get(), d.mrw_sqr);
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(d.stream));
   d.finalized = true;
+}
+
+// Fold, DFT and window division of one f(tau) set into host memory (enqueued on the stream).
+void SpAccumulator::finalizeInto(const double* f_tau, std::vector<double2>& host) {
+  auto& d = *d_;
+  auto& g = d.g;
+  const size_t smem = sizeof(double) * 3 * g.n;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(spFinalizeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  DCAACC_CUDA_CHECK(cudaMemsetAsync(d.out_d.get(), 0, d.out_d.bytes(), d.stream));
+  spFinalizeKernel<<<dim3(g.n_labels, 2), 256, smem, d.stream>>>(g, f_tau, d.inv_phi.get(), d.n_sp, d.out_d.get());
+  DCAACC_LAUNCH_CHECK();
+  ++d.launches;
+  host.resize(d.out_d.size());
+  DCAACC_CUDA_CHECK(cudaMemcpyAsync(host.data(), d.out_d.get(), d.out_d.bytes(), cudaMemcpyDeviceToHost, d.stream));
+}
+
+void SpAccumulator::singleMeasurementMrw(double* out, size_t count) {
+  auto& d = *d_;
+  if (!d.stamping)
+    throw Error(DCAACC_NOT_READY, "single-measurement functions need stamping");
+  if (count != d.out_d.size())
+    throw Error(DCAACC_INVALID_ARG, "output size does not match");
+  std::vector<double2> host;
+  finalizeInto(d.f_tau_single.get(), host);
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(d.stream));
+  std::memcpy(out, host.data(), 16 * count);
+}
+
+void SpAccumulator::singleMeasurementFtau(double* out, size_t count) {
+  auto& d = *d_;
+  if (!d.stamping)
+    throw Error(DCAACC_NOT_READY, "single-measurement functions need stamping");
+  if (count != d.f_tau_single.size())
+    throw Error(DCAACC_INVALID_ARG, "output size does not match");
+  DCAACC_CUDA_CHECK(cudaMemcpyAsync(out, d.f_tau_single.get(), d.f_tau_single.bytes(), cudaMemcpyDeviceToHost,
+                                    d.stream));
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(d.stream));
+}
+
+void SpAccumulator::clearSingleMeasurement() {
+  auto& d = *d_;
+  if (!d.stamping)
+    throw Error(DCAACC_NOT_READY, "single-measurement functions need stamping");
+  DCAACC_CUDA_CHECK(cudaMemsetAsync(d.f_tau_single.get(), 0, d.f_tau_single.bytes(), d.stream));
+}
+
+size_t SpAccumulator::fTauSize() const {
+  return d_->f_tau.size();
 }
 
 void SpAccumulator::get(bool sqr, double* out, size_t count) const {
@@ -502,7 +554,8 @@ void SpAccumulator::synchronize() {
 
 size_t SpAccumulator::deviceFingerprint() const {
   auto& d = *d_;
-  return d.coeff.bytes() + d.inv_phi.bytes() + d.f_tau.bytes() + d.f_tau_sqr.bytes() + d.tau_d.bytes() +
+  return d.coeff.bytes() + d.inv_phi.bytes() + d.f_tau.bytes() + d.f_tau_sqr.bytes() + d.f_tau_single.bytes() +
+         d.tau_d.bytes() +
          d.M_d.bytes() + d.r_of_d.bytes() + d.perm_r_d.bytes() + d.perm_c_d.bytes() + d.rs_d.bytes() +
          d.cs_d.bytes() + d.sectors_d.bytes() + d.out_d.bytes();
 }

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <vector>
 
 #include "../../include/dcaacc.h"
 #include "tp_accumulator.hpp"
@@ -36,10 +37,15 @@ public:
   size_t deviceFingerprint() const;
   uint64_t kernelLaunches() const;
   size_t outputSize() const;
+  size_t fTauSize() const;
+  void singleMeasurementMrw(double* out, size_t count);
+  void singleMeasurementFtau(double* out, size_t count);
+  void clearSingleMeasurement();
 
 private:
   struct Impl;
   std::unique_ptr<Impl> d_;
+  void finalizeInto(const double* f_tau, std::vector<double2>& host);
 };
 
 }  // namespace dcaacc

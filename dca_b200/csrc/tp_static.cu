@@ -247,4 +247,8 @@ void computeGNoAlloc(const dcaacc_tp_config& c, const double* G0_dev, const dcaa
                              stream);
 }
 
+size_t staticScratchBytes() {
+  return kStaticScratchBytes;
+}
+
 }  // namespace dcaacc

@@ -164,6 +164,12 @@ size_t dcaacc_tp_device_fingerprint(const dcaacc_tp* acc);
 /* Number of this library's kernels launched by the handle since creation. */
 uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc);
 
+/* staticDeviceFingerprint() — tp_accumulator_gpu.hpp:158-167: device bytes held process-wide, not
+ * by a handle.  The reference counts its static shared G4 and G0 there; here G4 and G0 belong to
+ * their handle (dcaacc_tp_device_fingerprint), and the process-wide device state is the
+ * allocation-free entry point's static scratch array. */
+size_t dcaacc_tp_static_device_fingerprint(void);
+
 /* Which mirror symmetries the mixed path uses (no reference counterpart; monitoring): bit 0, only
  * the upper frequency half of G is computed (real M and G0(-k,-w) = conj G0(k,w)); bit 1, only
  * the G4 tiles with w1 >= Nw/2 are accumulated and the rest is their conjugated mirror. */
@@ -243,6 +249,8 @@ typedef struct dcaacc_sp_config {
   const int32_t* r_sub;       /* [n_sites * n_sites], (i,j) at i + Nc*j: index of r_j - r_i */
   int32_t accumulate_m_sqr;   /* also accumulate sign * M^2 (sp_accumulator.hpp:195-196) */
   int32_t max_order;
+  int32_t stamping;           /* keep the last measurement's own f(tau) as well, the reference's
+                                 stamping_period() > 0 (sp_accumulator_gpu.hpp:160-183) */
 } dcaacc_sp_config;
 
 typedef struct dcaacc_sp dcaacc_sp;
@@ -268,6 +276,18 @@ int dcaacc_sp_get_m_r_w_sqr(const dcaacc_sp* acc, double* out, size_t count);
 
 /* sumTo(other) — sp_accumulator_gpu.hpp:231-236: other.f_tau += this.f_tau (time domain). */
 int dcaacc_sp_sum_to(const dcaacc_sp* acc, dcaacc_sp* other);
+
+/* Single measurement (config.stamping != 0): each accumulate replaces it with that measurement's
+ * own f(tau).  get_single_measurement_sign_times_MFunction() — sp_accumulator_gpu.hpp:251-259: the
+ * finalize (fold, DFT, window division) of that f(tau), same layout and count as get_m_r_w, computed
+ * on each call.  get_single_measurement_sign_times_MFunction_time() — :264-271: the f(tau) itself,
+ * FP64 [spin][label = b_i + nb (b_j + nb dr)][8 n_sp_freq + 16 padded times], count =
+ * dcaacc_sp_f_tau_size(acc).  clearSingleMeasurement() — sp_accumulator.hpp:286-288: zeroes it.
+ * Without stamping these return DCAACC_NOT_READY. */
+int dcaacc_sp_get_single_measurement_m_r_w(dcaacc_sp* acc, double* out, size_t count);
+int dcaacc_sp_get_single_measurement_f_tau(dcaacc_sp* acc, double* out, size_t count);
+int dcaacc_sp_clear_single_measurement(dcaacc_sp* acc);
+size_t dcaacc_sp_f_tau_size(const dcaacc_sp* acc);
 
 int dcaacc_sp_set_stream(dcaacc_sp* acc, void* stream);
 int dcaacc_sp_synchronize(dcaacc_sp* acc);

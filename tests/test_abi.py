@@ -24,6 +24,13 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(_native.lib, s), s
 
 
+def test_static_device_fingerprint_is_the_static_scratch():
+    """staticDeviceFingerprint: the process-wide device state is the allocation-free entry point's
+    48 MiB static scratch array (no device call is needed to report it)."""
+    from dca_b200.accumulators import TpAccumulator
+    assert TpAccumulator.staticDeviceFingerprint() == 48 << 20
+
+
 def test_invalid_configuration_rejected_before_any_device_work():
     from dca_b200 import _native as N
     from dca_b200 import workloads as W

@@ -58,6 +58,34 @@ def test_sp_sum_to_linearity():
     assert rel_err(b.get_sign_times_M_r_w(), both.get_sign_times_M_r_w()) <= 1e-13
 
 
+def test_sp_single_measurement_matches_oracle(oracle_lib):
+    """Stamping (the reference's stamping_period() > 0): after each accumulate the handle also holds
+    that measurement's own f(tau); its M(r, w) equals the oracle's for an accumulator fed only that
+    measurement, clearSingleMeasurement zeroes it, and the running sum is unchanged."""
+    from dca_b200.accumulators import LogicError, SpAccumulator
+    case, _ = golden("c1_mag")
+    p = case.sp_params(stamping=True)
+    acc = SpAccumulator(p)
+    acc.resetAccumulation()
+    ms = case.measurements[:3]
+    for m in ms:
+        acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+        ora = oracle_lib.OracleSp(case.sp_params())
+        ora.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+        ora.finalize()
+        assert rel_err(acc.get_single_measurement_sign_times_MFunction(), ora.get()) <= SP_TOL
+    ft = acc.get_single_measurement_sign_times_MFunction_time()
+    assert ft.shape == (2, p.n_bands ** 2 * p.n_sites, 8 * p.n_sp_freq + 16) and np.any(ft != 0)
+    acc.clearSingleMeasurement()
+    assert not np.any(acc.get_single_measurement_sign_times_MFunction_time())
+    acc.finalize()
+    ref = run_sp(case, ms, sqr=False)
+    assert np.array_equal(acc.get_sign_times_M_r_w(), ref.get_sign_times_M_r_w())
+    plain = SpAccumulator(case.sp_params())
+    with pytest.raises(LogicError):  # no stamping
+        plain.clearSingleMeasurement()
+
+
 def test_sp_errors():
     from dca_b200.accumulators import LogicError, SpAccumulator
     case, _ = golden("c1_mag")
