@@ -79,8 +79,8 @@ def test_sp_single_measurement_matches_oracle(oracle_lib):
     acc.clearSingleMeasurement()
     assert not np.any(acc.get_single_measurement_sign_times_MFunction_time())
     acc.finalize()
-    ref = run_sp(case, ms, sqr=False)
-    assert np.array_equal(acc.get_sign_times_M_r_w(), ref.get_sign_times_M_r_w())
+    ref = run_sp(case, ms, sqr=False)  # shared-memory atomics: equal up to summation order
+    assert rel_err(acc.get_sign_times_M_r_w(), ref.get_sign_times_M_r_w()) <= 1e-13
     plain = SpAccumulator(case.sp_params())
     with pytest.raises(LogicError):  # no stamping
         plain.clearSingleMeasurement()
