@@ -198,9 +198,8 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStages * kStageStride);
   uint64_t* full = bars;                     // [kStages] TMA -> MMA
-  uint64_t* empty = bars + kStages;          // [kStages] MMA -> TMA
-  uint64_t* acc_full = bars + 2 * kStages;   // [2] MMA -> epilogue
-  uint64_t* acc_empty = acc_full + 2;        // [2] epilogue -> MMA
+  uint64_t* empty = bars + kStages;          // [kStages] MMA -> TMA, and MMA -> epilogue
+  uint64_t* acc_empty = bars + 2 * kStages;  // [2] epilogue -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
   uint64_t* red_bar = bars + 12;                     // epilogue warps exchanged their chunk maxima
   float* red = reinterpret_cast<float*>(bars + 16);  // [2][4 quarters][4 column groups] chunk maxima
@@ -216,10 +215,8 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
       mbarInit(&full[s], 1);
       mbarInit(&empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbarInit(&acc_full[b], 1);
+    for (int b = 0; b < 2; ++b)
       mbarInit(&acc_empty[b], kEpiWarps);  // one arrival per epilogue warp
-    }
     mbarInit(red_bar, kEpiWarps);
     fenceBarrierInit();
     tc::prefetchTensorMap(&tmA);
@@ -314,8 +311,9 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
               }
             }
           }
+          // One commit per chunk: its arrival on the stage's empty barrier both frees the stage for
+          // the producer and tells the epilogue that the chunk's sums are in tensor memory.
           tc::commitTo(&empty[s]);
-          tc::commitTo(&acc_full[buf]);
         }
       }
     }
@@ -383,7 +381,11 @@ frontGemmKernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         const int buf = g & 1;
         // Column step: the A rows of chunk c carry the scale 2^e of that X' row chunk; undo it.
         const float f = MODE == 1 ? xinv[c] : 1.f;
-        ok = __all_sync(0xffffffffu, mbarWait(&acc_full[buf], (g >> 1) & 1, err));
+        // Chunk g's MMAs are complete when their commit arrives on empty[g % kStages] (its
+        // (g / kStages)-th phase).  That barrier cannot run a phase further ahead meanwhile: chunk
+        // g + kStages reuses the tensor-memory buffer of chunk g + 1, which this warp releases
+        // only after this wait.
+        ok = __all_sync(0xffffffffu, mbarWait(&empty[g % kStages], (g / kStages) & 1, err));
         if (!ok)
           break;
         tc::fenceAfterThreadSync();
