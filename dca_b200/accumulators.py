@@ -101,6 +101,19 @@ class TpParameters:
         return (nb, nb, nb, nb, nc, nw, nc, nw, len(self.k_ex), len(self.w_ex))
 
 
+def write_G4(path: str, acc: "TpAccumulator", normalized: bool = True) -> None:
+    """Writes each channel's G4 as the dataset "G4_<channel name>" (the names DcaData gives them,
+    dca_data.hpp:329-336), shaped (b1, b2, b3, b4, k1, w1, k2, w2, q, wq) in Fortran order like the
+    reference's function, into an .npz file (no HDF5 library in this environment).  normalized:
+    divided by accumulated sign * beta^2 as the solver does before writing
+    (ctaux_cluster_solver.hpp:521-525)."""
+    shape = acc.parameters.g4_shape()
+    g4 = acc.get_G4_normalized() if normalized else acc.get_G4()
+    arrays = {"G4_" + W.CHANNEL_NAMES[ch]: g.reshape(shape, order="F")
+              for ch, g in zip(acc.parameters.channels, g4)}
+    np.savez(path, **arrays)
+
+
 # dcaacc_sector as a numpy record (same layout as the C struct and _native.Sector), so that the
 # descriptors of a whole batch are filled with a few vectorised assignments.
 _SECTOR_FIELDS = ("n", "tau", "left_band", "right_band", "left_site", "right_site", "M", "ldm", "m_on_device")
@@ -268,6 +281,23 @@ class TpAccumulator:
         if self._g4 is None:
             raise LogicError("There is no G4 stored in this class.")
         return self._g4
+
+    def sign_sum(self):
+        """(sum of the measurement signs since resetAccumulation, number of measurements)."""
+        s, n = ctypes.c_double(), ctypes.c_uint64()
+        _check(N.lib.dcaacc_tp_sign_sum(self._h, ctypes.byref(s), ctypes.byref(n)))
+        return s.value, n.value
+
+    def get_G4_normalized(self) -> List[np.ndarray]:
+        """G4 / (accumulated sign * beta^2), the solver's normalisation (after finalize)."""
+        size = N.lib.dcaacc_tp_g4_size(self._h)
+        out = []
+        for c in range(len(self.parameters.channels)):
+            g = np.empty(size, np.complex128)
+            _check(N.lib.dcaacc_tp_get_g4_normalized(self._h, c, g.view(np.float64).ctypes.data_as(
+                ctypes.POINTER(ctypes.c_double)), size))
+            out.append(g)
+        return out
 
     def sumTo(self, other: "TpAccumulator"):
         _check(N.lib.dcaacc_tp_sum_to(self._h, other._h))

@@ -165,6 +165,18 @@ uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc) {
   return acc ? acc->impl.kernelLaunches() : 0;
 }
 
+int dcaacc_tp_sign_sum(const dcaacc_tp* acc, double* sum, uint64_t* count) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.signSum(sum, count); });
+}
+
+int dcaacc_tp_get_g4_normalized(const dcaacc_tp* acc, int32_t channel, double* out, size_t count) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.getG4Normalized(channel, out, count); });
+}
+
 size_t dcaacc_tp_static_device_fingerprint(void) {
   return dcaacc::staticScratchBytes();
 }

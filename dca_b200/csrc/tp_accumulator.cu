@@ -352,6 +352,8 @@ void TpAccumulator::reset() {
   n_max_batch_ = 0;
   for (auto& g : G4_)
     DCAACC_CUDA_CHECK(cudaMemsetAsync(g.get(), 0, g.bytes(), stream_));
+  sign_sum_ = 0;
+  n_meas_ = 0;
   ready_ = true;
   finalized_ = false;
   have_g_ = false;
@@ -717,6 +719,8 @@ double TpAccumulator::accumulate(const dcaacc_sector* sectors, int sign) {
     invalid("sign must be +1 or -1");
   validateSector(sectors[0]);
   validateSector(sectors[1]);
+  sign_sum_ += sign;  // the solver's accumulated sign counts every measurement
+  ++n_meas_;
   if (sectors[0].n + sectors[1].n == 0)  // empty configuration (tp_accumulator_cpu.hpp:238-239)
     return 0.;
   if (slots_ == max_batch_)
@@ -787,6 +791,28 @@ void TpAccumulator::sumTo(TpAccumulator& other) {
   DCAACC_CUDA_CHECK(cudaStreamWaitEvent(other.stream_, ev, 0));
   DCAACC_CUDA_CHECK(cudaEventDestroy(ev));
   other.finalized_ = false;
+  other.sign_sum_ += sign_sum_;
+  other.n_meas_ += n_meas_;
+  sign_sum_ = 0;
+  n_meas_ = 0;
+}
+
+// The solver's normalisation of the accumulated G4 (ctaux_cluster_solver.hpp:521-525):
+// G4 / (accumulated sign * beta^2).
+void TpAccumulator::getG4Normalized(int channel, double* out, size_t count) const {
+  if (sign_sum_ == 0)
+    throw Error(DCAACC_NOT_READY, "the accumulated sign is zero");
+  getG4(channel, out, count);
+  const double f = 1.0 / (sign_sum_ * dims_.beta * dims_.beta);
+  for (size_t i = 0; i < 2 * count; ++i)
+    out[i] *= f;
+}
+
+void TpAccumulator::signSum(double* sum, uint64_t* count) const {
+  if (sum)
+    *sum = sign_sum_;
+  if (count)
+    *count = n_meas_;
 }
 
 void TpAccumulator::getG(int spin, double* out, size_t count) const {

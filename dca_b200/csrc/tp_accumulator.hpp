@@ -101,6 +101,8 @@ public:
   void flush();
   void finalize();
   void getG4(int channel, double* out, size_t count) const;
+  void getG4Normalized(int channel, double* out, size_t count) const;
+  void signSum(double* sum, uint64_t* count) const;
   void sumTo(TpAccumulator& other);
   void getG(int spin, double* out, size_t count) const;
   void setStream(cudaStream_t s);
@@ -225,6 +227,8 @@ private:
   size_t mcopy_bytes_ = 0;
   void flushMCopy();
   int n_max_batch_ = 0;   // largest order staged
+  double sign_sum_ = 0;   // signs of the measurements accumulated since reset (sumTo moves them)
+  uint64_t n_meas_ = 0;
   bool ready_ = false;    // reset() called since the last finalize
   bool finalized_ = false;
   bool have_g_ = false;   // FP64 mode: G of the last measurement is in G64_

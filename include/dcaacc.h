@@ -164,6 +164,14 @@ size_t dcaacc_tp_device_fingerprint(const dcaacc_tp* acc);
 /* Number of this library's kernels launched by the handle since creation. */
 uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc);
 
+/* The solver's normalisation of G4 (ctaux_cluster_solver.hpp:521-525): G4 / (accumulated sign *
+ * beta^2).  The handle sums the signs passed to accumulate since resetAccumulation (every
+ * measurement counts, empty configurations included; sum_to moves the sum with G4).  sign_sum
+ * returns that sum and the number of measurements; get_g4_normalized is get_g4 divided by
+ * sum * beta^2 (DCAACC_NOT_READY while the sum is zero). */
+int dcaacc_tp_sign_sum(const dcaacc_tp* acc, double* sum, uint64_t* count);
+int dcaacc_tp_get_g4_normalized(const dcaacc_tp* acc, int32_t channel, double* out, size_t count);
+
 /* staticDeviceFingerprint() — tp_accumulator_gpu.hpp:158-167: device bytes held process-wide, not
  * by a handle.  The reference counts its static shared G4 and G0 there; here G4 and G0 belong to
  * their handle (dcaacc_tp_device_fingerprint), and the process-wide device state is the

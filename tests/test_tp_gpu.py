@@ -227,6 +227,40 @@ def test_tuned_launch_shapes_match_builtin(monkeypatch, wname, precision, max_ba
         assert np.array_equal(a, b)
 
 
+def test_sign_sum_and_normalized_g4(tmp_path):
+    """The handle sums the measurement signs (sumTo moves them with G4); the normalised G4 is
+    G4 / (sign sum * beta^2), as the solver divides it, and write_G4 stores it under the
+    reference's dataset names in the reference's index order."""
+    from dca_b200.accumulators import LogicError, TpAccumulator, write_G4
+    case, _ = golden("c1_mag")
+    ms = case.measurements
+    a = TpAccumulator(case.G0, case.tp_params())
+    b = TpAccumulator(case.G0, case.tp_params())
+    a.resetAccumulation(0)
+    b.resetAccumulation(0)
+    for m in ms[:2]:
+        a.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    for m in ms[2:]:
+        b.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    a.sumTo(b)
+    assert a.sign_sum() == (0.0, 0)
+    assert b.sign_sum() == (float(sum(m.sign for m in ms)), len(ms))
+    b.finalize()
+    total = sum(m.sign for m in ms)
+    for g, n in zip(b.get_G4(), b.get_G4_normalized()):
+        np.testing.assert_allclose(n, g / (total * case.beta ** 2), rtol=1e-15, atol=0)
+    path = tmp_path / "g4.npz"
+    write_G4(str(path), b)
+    with np.load(path) as f:
+        assert list(f.keys()) == ["G4_PARTICLE_HOLE_MAGNETIC"]
+        stored = f["G4_PARTICLE_HOLE_MAGNETIC"]
+    assert stored.shape == b.parameters.g4_shape()
+    assert np.array_equal(stored.reshape(-1, order="F"), b.get_G4_normalized()[0])
+    a.finalize()
+    with pytest.raises(LogicError):  # nothing accumulated: the sign sum is zero
+        a.get_G4_normalized()
+
+
 def test_large_cluster_fp64_matches_oracle(oracle_lib):
     """6x6 single band (Nc = 36): one momentum transfer's k1 x k2 block does not fit the tuned
     single-band kernel's thread block, so the FP64 update takes the general kernel."""
