@@ -397,13 +397,10 @@ def run_ours(args, world, rank, local):
     D = nb * nc * nwe
     n_g4 = nb ** 4 * nc ** 2 * nw ** 2 * len(w.exchange_momenta(nc)) * len(w.exchange_frequencies())
     simt = os.environ.get("DCAACC_TP_SIMT_ONLY") == "1"
-    # The G4 update stage against HBM (the north star's "updateG4 HBM %"), whether or not it is the
+    # The G4 update stage against HBM (the metric's "updateG4 HBM %"), whether or not it is the
     # dominant stage.  Algorithmic bytes of one batch: the FP64 read-modify-write of every G4 entry
-    # of every channel, one read of the batch's G (FP32 complex, both spins), and the disconnected
-    # terms (FP32, one write by their GEMM and one read by the direct-term kernel per channel).
-    # Algorithmic bytes as the survey of the reference defines them: the FP64 read-modify-write of
-    # every G4 entry of every channel and one read of the batch's G (FP32 complex, both spins).  With
-    # the mirror symmetries (mirror_mode) the kernels move about half of that.
+    # of every channel and one read of the batch's G (FP32 complex, both spins).  With the mirror
+    # symmetries (mirror_mode) the kernels move about half of that.
     g4_alg_bytes = len(w.channels) * n_g4 * 32 + B * 2 * D * D * 8
     g4_sec = stages["update_g4"][0] / args.steps / 1e3  # the stage's time per batch
     g4_roof = {"kernels": "discPlanesKernel + frontGemmKernel<2> (disconnected terms) + updateG4DirectMma "

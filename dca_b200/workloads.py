@@ -288,7 +288,7 @@ class Workload:
                 self.mu = find_mu(self.model, self.beta)
         return self.mu
 
-    # Derived sizes (SURVEY-style notation: NwExt = Nw + 2 ext, D = nb Nc NwExt).
+    # Derived sizes (NwExt = Nw + 2 ext, D = nb Nc NwExt).
     def exchange_frequencies(self) -> List[int]:
         if self.all_transfers:
             return list(range(self.freq_transfer + 1))
