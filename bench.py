@@ -474,10 +474,10 @@ def run_ours(args, world, rank, local):
         "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (G, G4 partials) + fp64 (running G4)",
         "data": "synthetic (seeded; dca_b200.workloads)",
-        "config": {"workload": f"{w.name}: single-band Hubbard 4x4 (Nc=16), Nw=64, 16 q x 1 wq, "
-                               f"PH-magnetic + PH-charge, n~U[{w.n_range[0]},{w.n_range[1]}], batch {B}",
+        "config": {"workload": w.describe(),
                    "measurements_per_step": B, "precision": "mixed", "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (G4 537 MB, G 1 GB per batch)"},
+                   "l2": f"inputs larger than L2 (G4 {len(w.channels) * n_g4 * 16 / 1e6:.0f} MB, "
+                         f"G {B * 2 * D * D * 8 / 1e9:.1f} GB per batch)"},
         "e2e": e2e,
         "gpu_launches": int(launches),
         "cuda_graphs": graph_info,
@@ -495,7 +495,7 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         val, P, kind, t, timed = run_cpu_reference(w, 2, 1)
         result["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": P, "kind": kind,
-                                  "sample": f"{P} single-threaded processes x {timed} timed c3 measurement "
+                                  "sample": f"{P} single-threaded processes x {timed} timed {w.name} measurement "
                                             f"(after 1 warm-up), FP64 TpAccumulator<CPU>, {t:.1f} s"}
     return result
 
@@ -512,8 +512,7 @@ def run_reference_arm(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / max(timed, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
             "data": "synthetic (seeded; dca_b200.workloads)",
-            "config": {"workload": f"{w.name}: single-band Hubbard 4x4 (Nc=16), Nw=64, 16 q x 1 wq, "
-                                   f"PH-magnetic + PH-charge, n~U[{w.n_range[0]},{w.n_range[1]}]",
+            "config": {"workload": w.describe(with_batch=False),
                        "parallelism": f"{P} CPU processes"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": P, "kind": kind,
                              "sample": f"{P} processes x {timed} measurements (after {warm} warm-up), "

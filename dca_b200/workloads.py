@@ -302,6 +302,22 @@ class Workload:
     def ext(self) -> int:
         return max(abs(w) for w in self.exchange_frequencies())
 
+    def describe(self, with_batch: bool = True) -> str:
+        """One line naming the workload by what it is: model, cluster, frequencies, transfers,
+        channels, expansion orders and batch."""
+        cl = self.cluster()
+        if self.model.kind == "single":
+            model = f"single-band Hubbard (t={self.model.t:g}, t'={self.model.tp:g}, U={self.model.U:g})"
+        else:
+            model = f"three-band Emery (U_dd={self.model.U:g})"
+        kind = self.cluster_kind[0]
+        cluster = f"{self.cluster_kind[1]}x{self.cluster_kind[1]}" if kind == "square" else kind
+        chans = " + ".join(CHANNEL_NAMES[c] for c in self.channels)
+        s = (f"{self.name}: {model}, {cluster} cluster (Nc={cl.nc}), beta={self.beta:g}, "
+             f"Nw={2 * self.nw_half}, {len(self.exchange_momenta(cl.nc))} q x "
+             f"{len(self.exchange_frequencies())} wq, {chans}, n~U[{self.n_range[0]},{self.n_range[1]}]")
+        return s + (f", batch {self.batch}" if with_batch else "")
+
 
 WORKLOADS = {
     # 2x2 single-band Hubbard, the reference CPU path's own scale.
