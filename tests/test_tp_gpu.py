@@ -189,8 +189,8 @@ def test_graph_replay_matches_eager(monkeypatch):
         assert np.array_equal(g, e) and np.array_equal(g, o)
 
 
-@pytest.mark.parametrize("wname,precision,max_batch,n_meas", [("c3", 0, 1, 16), ("c3", 1, 4, 48),
-                                                              ("c4", 1, 2, 24)])
+@pytest.mark.parametrize("wname,precision,max_batch,n_meas", [("c3", 0, 1, 16), ("c3", 1, 4, 64),
+                                                              ("c4", 1, 2, 30)])
 def test_tuned_launch_shapes_match_builtin(monkeypatch, wname, precision, max_batch, n_meas):
     """The launch-shape tuner times each candidate shape (FP64: row-transform tiles, column-transform
     widths, transfers per G4 CTA; mixed: operand-builder blocks, and for three bands the staged G4
