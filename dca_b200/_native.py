@@ -122,6 +122,7 @@ def _load():
         "dcaacc_tp_tuning_settled": (i, [p]),
         "dcaacc_tp_tuning_report": (i, [p, ctypes.c_char_p, sz, POINTER(sz)]),
         "dcaacc_tp_peek_g4": (i, [p, i, sz, sz, POINTER(c_double)]),
+        "dcaacc_tp_peek_g4_async": (i, [p, i, sz, sz, POINTER(c_double)]),
         "dcaacc_tp_compute_g_noalloc": (i, [POINTER(TpConfig), p, POINTER(Sector), p, p]),
         "dcaacc_sp_create": (i, [POINTER(SpConfig), POINTER(p)]),
         "dcaacc_sp_destroy": (None, [p]),

@@ -380,6 +380,13 @@ class TpAccumulator:
         _check(N.lib.dcaacc_tp_peek_g4(self._h, channel, offset, count, _dptr(out.view(np.float64))))
         return out
 
+    def peek_G4_async(self, channel: int, offset: int, out: np.ndarray):
+        """Enqueues the read of len(out) entries into out (complex128, ideally pinned); they are
+        there after synchronizeCopy().  The caller keeps out alive until then."""
+        if out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous complex128 array")
+        _check(N.lib.dcaacc_tp_peek_g4_async(self._h, channel, offset, out.size, _dptr(out.view(np.float64))))
+
     def num_channels(self) -> int:
         return len(self.parameters.channels)
 

@@ -230,6 +230,12 @@ int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t cou
   return guard([&] { acc->impl.peekG4(channel, offset, count, out); });
 }
 
+int dcaacc_tp_peek_g4_async(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out) {
+  if (!acc || !out)
+    return null_handle();
+  return guard([&] { acc->impl.peekG4(channel, offset, count, out, false); });
+}
+
 int dcaacc_tp_compute_g_noalloc(const dcaacc_tp_config* cfg, const double* G0,
                                 const dcaacc_sector* sectors, double* G_out, void* stream) {
   if (!cfg)

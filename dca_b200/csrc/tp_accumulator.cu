@@ -894,7 +894,7 @@ void TpAccumulator::stageTimes(double* ms, uint64_t* launches, int n) {
   }
 }
 
-void TpAccumulator::peekG4(int channel, size_t offset, size_t count, double* out) {
+void TpAccumulator::peekG4(int channel, size_t offset, size_t count, double* out, bool wait) {
   if (channel < 0 || channel >= static_cast<int>(G4_.size()))
     invalid("channel index out of range");
   if (offset > g4_size_ || count > g4_size_ - offset)
@@ -902,14 +902,17 @@ void TpAccumulator::peekG4(int channel, size_t offset, size_t count, double* out
   process();
   const double2* src = G4_[channel].get() + offset;
   if (dims_.half_g4) {  // entries with w1 < Nw / 2 come from their mirrors
-    if (peek_d_.size() < count)
+    if (peek_d_.size() < count) {
+      DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));  // earlier reads may still use the window
       peek_d_.alloc(count);
+    }
     launchG4Window(G4_[channel].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), offset, count, peek_d_.get(),
                    stream_);
     src = peek_d_.get();
   }
   DCAACC_CUDA_CHECK(cudaMemcpyAsync(out, src, 16 * count, cudaMemcpyDeviceToHost, stream_));
-  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  if (wait)
+    DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 
 void TpAccumulator::setStream(cudaStream_t s) {

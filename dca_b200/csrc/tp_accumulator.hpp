@@ -130,7 +130,7 @@ public:
   std::string tuningReport() {
     return tuner_.report();
   }
-  void peekG4(int channel, size_t offset, size_t count, double* out);
+  void peekG4(int channel, size_t offset, size_t count, double* out, bool wait = true);
 
 private:
   void validateSector(const dcaacc_sector& s) const;

@@ -219,6 +219,12 @@ int dcaacc_tp_tuning_report(dcaacc_tp* acc, char* buf, size_t cap, size_t* len);
  * an accumulation in progress. */
 int dcaacc_tp_peek_g4(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out);
 
+/* The same read enqueued on the handle's stream without waiting: out (pinned host memory for an
+ * asynchronous copy) holds the entries once the stream has reached this point, e.g. after
+ * dcaacc_tp_synchronize; it must stay valid until then.  Lets a caller read every batch's result
+ * while the next batch is being staged and copied. */
+int dcaacc_tp_peek_g4_async(dcaacc_tp* acc, int32_t channel, size_t offset, size_t count, double* out);
+
 /* Allocation-free G of one measurement.  No counterpart in the reference: it exists for callers
  * that cannot allocate device memory while they run -- applications whose device memory is fully
  * reserved by their own pool allocator, and per-measurement loops that must not pay the

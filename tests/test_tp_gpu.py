@@ -227,6 +227,25 @@ def test_tuned_launch_shapes_match_builtin(monkeypatch, wname, precision, max_ba
         assert np.array_equal(a, b)
 
 
+def test_peek_async_matches_peek():
+    """peek_G4_async enqueues the read of the running G4 (after the queued measurements) into
+    caller memory; after synchronizeCopy it equals the synchronous peek, also with the mirror
+    window of the half-G4 path (c3-like)."""
+    import torch
+    from dca_b200.accumulators import TpAccumulator
+    case = case_from_workload(_small("c3", n_range=(40, 80)), 6)
+    acc = TpAccumulator(case.G0, case.tp_params(precision=1, max_batch=4))
+    acc.resetAccumulation(0)
+    outs = []
+    for m in case.measurements:
+        acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+        buf = torch.empty(300, dtype=torch.complex128, pin_memory=True).numpy()
+        acc.peek_G4_async(1, 1000, buf)
+        outs.append(buf)
+    acc.synchronizeCopy()
+    assert np.array_equal(outs[-1], acc.peek_G4(1, 1000, 300)) and np.any(outs[-1] != 0)
+
+
 def test_sign_sum_and_normalized_g4(tmp_path):
     """The handle sums the measurement signs (sumTo moves them with G4); the normalised G4 is
     G4 / (sign sum * beta^2), as the solver divides it, and write_G4 stores it under the
