@@ -68,3 +68,46 @@ def test_case_file_round_trip():
     assert np.array_equal(c.k_add, cl.k_add) and np.array_equal(c.r_sub, cl.r_sub)
     assert np.array_equal(c.G0, g0.reshape(-1))
     assert np.array_equal(c.measurements[1].sectors[1].M, ms[1].sectors[1].M)
+
+
+def test_workload_descriptions_name_what_they_are():
+    c3 = W.WORKLOADS["c3"].describe()
+    assert c3.startswith("c3: single-band Hubbard") and "4x4 cluster (Nc=16)" in c3
+    assert "Nw=64" in c3 and "16 q x 1 wq" in c3 and "batch 64" in c3
+    c4 = W.WORKLOADS["c4"].describe(with_batch=False)
+    assert "three-band Emery" in c4 and "8 q x 4 wq" in c4 and "PARTICLE_PARTICLE_UP_DOWN" in c4
+    assert "batch" not in c4
+
+
+def test_write_g4_uses_reference_names_and_order(tmp_path):
+    """write_G4 on a stand-in accumulator (no GPU): one dataset per channel named as DcaData names
+    them, shaped (b1, b2, b3, b4, k1, w1, k2, w2, q, wq) in Fortran order."""
+    from dca_b200.accumulators import TpParameters, write_G4
+    w = W.WORKLOADS["c1"]
+    cl = w.cluster()
+    p = TpParameters.from_workload(w, cl, channels=(W.PH_MAGNETIC, W.PH_CHARGE))
+    shape = p.g4_shape()
+    size = int(np.prod(shape))
+    rng = np.random.default_rng(3)
+    g4 = [rng.standard_normal(size) + 1j * rng.standard_normal(size) for _ in range(2)]
+
+    class StandIn:
+        parameters = p
+
+        def get_G4(self):
+            return g4
+
+        def get_G4_normalized(self):
+            return [g / 2.0 for g in g4]
+
+    path = tmp_path / "g4.npz"
+    write_G4(str(path), StandIn())
+    with np.load(path) as f:
+        assert sorted(f.keys()) == ["G4_PARTICLE_HOLE_CHARGE", "G4_PARTICLE_HOLE_MAGNETIC"]
+        mag = f["G4_PARTICLE_HOLE_MAGNETIC"]
+    assert mag.shape == shape
+    # first index fastest: element (b1..wq) = flat index b1 + nb (b2 + ...)
+    assert mag[0, 0, 0, 0, 1, 0, 0, 0, 0, 0] == g4[0][1 * p.n_bands ** 4] / 2.0
+    write_G4(str(path), StandIn(), normalized=False)
+    with np.load(path) as f:
+        assert np.array_equal(f["G4_PARTICLE_HOLE_CHARGE"].reshape(-1, order="F"), g4[1])
