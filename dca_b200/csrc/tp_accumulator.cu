@@ -648,8 +648,10 @@ int TpAccumulator::launchBatchGraph(int set, const FrontendArgs& fa, const G4Arg
     if (graphs_.size() >= kMaxGraphs) {
       auto lru = std::min_element(graphs_.begin(), graphs_.end(),
                                   [](const BatchGraph& a, const BatchGraph& b) { return a.last < b.last; });
-      if (lru->exec)
+      if (lru->exec) {
+        DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));  // no launch of it may be pending
         cudaGraphExecDestroy(lru->exec);
+      }
       graphs_.erase(lru);
     }
     graphs_.push_back(BatchGraph{set, ga.n_slots, fa.n_max, false, nullptr, 0, 0});
@@ -698,8 +700,10 @@ void TpAccumulator::releaseGraphs() {
 }
 
 void TpAccumulator::setGraphs(bool on) {
-  if (!on)
+  if (!on) {
+    DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));  // no launch of them may be pending
     releaseGraphs();
+  }
   graphs_on_ = on;
 }
 
