@@ -111,3 +111,26 @@ def test_oracle_sp_sum_linearity(oracle_lib):
         both.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
     both.finalize()
     assert rel_err(both.get(), parts[0] + parts[1]) <= 1e-13
+
+
+@pytest.mark.parametrize("wname", ["c3", "c5"])
+def test_oracle_g_mirror_symmetry(oracle_lib, wname):
+    """The identity the mixed path's half-G mode rests on: with real M and G0(-k, -w) =
+    conj G0(k, w) (real hopping, t' included), G(-k1 w1', -k2 w2') = conj G(k1 w1; k2 w2) with
+    w' = NwExt - 1 - w, on one seeded measurement of the 4x4 and of the 6x6 configuration."""
+    import dataclasses
+    w = dataclasses.replace(W.WORKLOADS[wname], nw_half=4, n_sp=64, n_range=(20, 40))
+    case = case_from_workload(w, 1)
+    acc = oracle_lib.OracleTp(case.G0, case.tp_params())
+    m = case.measurements[0]
+    acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    cl = w.cluster()
+    nc = cl.nc
+    zero = next(i for i in range(nc) if all(cl.k_add[i, j] == j for j in range(nc)))
+    neg = np.array([next(j for j in range(nc) if cl.k_add[k, j] == zero) for k in range(nc)])
+    for spin in range(2):
+        g = acc.get_G(spin)
+        nwe = int(round(np.sqrt(g.size // (nc * nc))))
+        g = g.reshape(nwe, nwe, nc, nc)  # [w2][w1][k2][k1] (k1 fastest, one band)
+        mirrored = g[::-1, ::-1][:, :, neg][:, :, :, neg]
+        assert np.max(np.abs(mirrored - g.conj())) <= 1e-12 * np.max(np.abs(g))
