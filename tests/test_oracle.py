@@ -134,3 +134,24 @@ def test_oracle_g_mirror_symmetry(oracle_lib, wname):
         g = g.reshape(nwe, nwe, nc, nc)  # [w2][w1][k2][k1] (k1 fastest, one band)
         mirrored = g[::-1, ::-1][:, :, neg][:, :, :, neg]
         assert np.max(np.abs(mirrored - g.conj())) <= 1e-12 * np.max(np.abs(g))
+
+
+def test_oracle_g4_mirror_symmetry(oracle_lib):
+    """The identity behind the half-G4 mode: G4(-k1 w1', -k2 w2', -q, wq = 0) = conj G4(k1 w1, k2 w2,
+    q, 0) with w' = Nw - 1 - w, for both particle-hole channels over all momentum transfers of the
+    4x4 configuration (three seeded measurements)."""
+    import dataclasses
+    w = dataclasses.replace(W.WORKLOADS["c3"], nw_half=4, n_sp=64, n_range=(20, 40))
+    case = case_from_workload(w, 3)
+    acc = oracle_lib.OracleTp(case.G0, case.tp_params())
+    for m in case.measurements:
+        acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    cl = w.cluster()
+    nc, nw = cl.nc, 2 * w.nw_half
+    assert list(w.exchange_momenta(nc)) == list(range(nc)) and w.exchange_frequencies() == [0]
+    zero = next(i for i in range(nc) if all(cl.k_add[i, j] == j for j in range(nc)))
+    neg = np.array([next(j for j in range(nc) if cl.k_add[k, j] == zero) for k in range(nc)])
+    for g4 in acc.get_G4():
+        g = g4.reshape(nc, nw, nc, nw, nc)  # [q][w2][k2][w1][k1] (k1 fastest, one band, one wq)
+        mirrored = g[neg][:, ::-1][:, :, neg][:, :, :, ::-1][:, :, :, :, neg]
+        assert np.max(np.abs(mirrored - g.conj())) <= 1e-12 * np.max(np.abs(g))
