@@ -60,3 +60,20 @@ def test_invalid_configuration_rejected_before_any_device_work():
     assert N.lib.dcaacc_tp_create(ctypes.byref(cfg), dp(g0), ctypes.byref(h)) == 1
     assert b"too small" in N.lib.dcaacc_last_error()
     assert N.lib.dcaacc_tp_reset(None) == 1
+
+
+def test_bench_reference_arm_prints_one_contract_line():
+    """bench.py --impl reference (the reference's own CPU accumulator on the host cores, or the
+    restatement where it was not built) prints one JSON line with the contract's keys."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "meas/s"
+    assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": "meas/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
