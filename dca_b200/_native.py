@@ -142,6 +142,8 @@ def _load():
         "dcaacc_sp_f_tau_size": (sz, [p]),
         "dcaacc_tp_static_device_fingerprint": (sz, []),
         "dcaacc_tp_sign_sum": (i, [p, POINTER(c_double), POINTER(c_uint64)]),
+        "dcaacc_tp_share_g4": (i, [p, p]),
+        "dcaacc_tp_reset_loop": (i, [p, i]),
         "dcaacc_tp_get_g4_normalized": (i, [p, i, POINTER(c_double), sz]),
     }
     for name, (res, args) in sigs.items():

@@ -238,8 +238,13 @@ class TpAccumulator:
 
     # -- reference method set ----------------------------------------------------------------
     def resetAccumulation(self, dca_loop: int = 0):
-        _check(N.lib.dcaacc_tp_reset(self._h))
+        """Zeroes G4 (a G4 shared with share_G4_with: once per dca_loop) and arms accumulate."""
+        _check(N.lib.dcaacc_tp_reset_loop(self._h, int(dca_loop)))
         self._g4 = None
+
+    def share_G4_with(self, owner: "TpAccumulator"):
+        """Accumulate into owner's G4 (the reference's accumulator threads share one device G4)."""
+        _check(N.lib.dcaacc_tp_share_g4(self._h, owner._h))
 
     def accumulate(self, M_pair, configs, sign: int) -> float:
         keep: list = []

@@ -165,6 +165,20 @@ uint64_t dcaacc_tp_kernel_launches(const dcaacc_tp* acc) {
   return acc ? acc->impl.kernelLaunches() : 0;
 }
 
+int dcaacc_tp_share_g4(dcaacc_tp* acc, dcaacc_tp* owner) {
+  if (!acc || !owner)
+    return null_handle();
+  return guard([&] { acc->impl.shareG4(owner->impl); });
+}
+
+int dcaacc_tp_reset_loop(dcaacc_tp* acc, int32_t dca_loop) {
+  if (!acc)
+    return null_handle();
+  if (dca_loop < 0)
+    return guard([&] { throw dcaacc::Error(DCAACC_INVALID_ARG, "dca_loop must be non-negative"); });
+  return guard([&] { acc->impl.reset(dca_loop); });
+}
+
 int dcaacc_tp_sign_sum(const dcaacc_tp* acc, double* sum, uint64_t* count) {
   if (!acc)
     return null_handle();

@@ -174,17 +174,16 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   upload_ints(wex_d_, wex_list_);
 
   // ---- G4 per channel ----
-  G4_ = std::vector<DevBuf<double2>>(c.n_channels);
-  std::vector<double2*> ptrs;
-  for (auto& g : G4_) {
+  g4s_ = std::make_shared<SharedG4>();
+  g4() = std::vector<DevBuf<double2>>(c.n_channels);
+  for (auto& g : g4()) {
     g.alloc(g4_size_);
     DCAACC_CUDA_CHECK(cudaMemset(g.get(), 0, g.bytes()));
-    ptrs.push_back(g.get());
   }
   err_d_.alloc(1);
   DCAACC_CUDA_CHECK(cudaMemset(err_d_.get(), 0, sizeof(int)));
-  G4_ptrs_.alloc(ptrs.size());
-  DCAACC_CUDA_CHECK(cudaMemcpy(G4_ptrs_.get(), ptrs.data(), G4_ptrs_.bytes(), cudaMemcpyHostToDevice));
+  G4_ptrs_.alloc(c.n_channels);
+  uploadG4Ptrs();
 
   // ---- batch workspace ----
   const size_t n_sec = 2 * size_t(max_batch_);
@@ -340,7 +339,36 @@ TpAccumulator::~TpAccumulator() {
     cudaStreamDestroy(stream_);
 }
 
-void TpAccumulator::reset() {
+void TpAccumulator::uploadG4Ptrs() {
+  std::vector<double2*> ptrs;
+  for (auto& g : g4())
+    ptrs.push_back(g.get());
+  DCAACC_CUDA_CHECK(cudaMemcpy(G4_ptrs_.get(), ptrs.data(), G4_ptrs_.bytes(), cudaMemcpyHostToDevice));
+}
+
+// This handle accumulates into owner's G4 from now on (its own is released when no handle uses it
+// any more); both switch to atomic read-modify-writes, since their streams run concurrently.
+void TpAccumulator::shareG4(TpAccumulator& owner) {
+  if (&owner == this || owner.g4s_ == g4s_)
+    return;
+  if (owner.g4_size_ != g4_size_ || owner.g4().size() != g4().size() || owner.dims_.half_g4 != dims_.half_g4)
+    invalid("accumulators with different G4 shapes cannot share G4");
+  if (owner.device_ != device_)
+    invalid("sharing G4 requires both accumulators on the same device");
+  process();
+  owner.process();
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));  // this handle's kernels are done with its own G4
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(owner.stream_));
+  g4s_ = owner.g4s_;
+  uploadG4Ptrs();
+  // The update mode is a kernel argument: graphs captured before are dropped on both sides.
+  releaseGraphs();
+  owner.releaseGraphs();
+  atomic_ = true;
+  owner.atomic_ = true;
+}
+
+void TpAccumulator::reset(long dca_loop) {
   // resetAccumulation: zero G4 and arm accumulate (tp_accumulator_gpu.hpp:285-296).
   for (auto& h : hstage_)
     DCAACC_CUDA_CHECK(cudaEventSynchronize(h.uploaded));
@@ -350,8 +378,22 @@ void TpAccumulator::reset() {
   m_used_ = 0;
   mcopy_bytes_ = 0;  // a copy of a discarded batch is not issued
   n_max_batch_ = 0;
-  for (auto& g : G4_)
-    DCAACC_CUDA_CHECK(cudaMemsetAsync(g.get(), 0, g.bytes(), stream_));
+  if (g4Shared()) {
+    // Shared G4: zeroed once per DCA loop, by the first handle that resets for it
+    // (callOncePerLoop in tp_accumulator_gpu.hpp:285-296); synchronously, so that no handle's
+    // accumulation of this loop can run before the zeroing.
+    std::lock_guard<std::mutex> lock(g4s_->m);
+    if (dca_loop < 0 || dca_loop != g4s_->last_loop) {
+      for (auto& g : g4())
+        DCAACC_CUDA_CHECK(cudaMemsetAsync(g.get(), 0, g.bytes(), stream_));
+      DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+      g4s_->last_loop = dca_loop;
+    }
+  }
+  else {
+    for (auto& g : g4())
+      DCAACC_CUDA_CHECK(cudaMemsetAsync(g.get(), 0, g.bytes(), stream_));
+  }
   sign_sum_ = 0;
   n_meas_ = 0;
   ready_ = true;
@@ -743,11 +785,11 @@ void TpAccumulator::finalize() {
   if (finalized_)
     return;
   process();
-  for (size_t c = 0; c < G4_.size(); ++c) {
+  for (size_t c = 0; c < g4().size(); ++c) {
     if (dims_.half_g4)  // the entries with w1 < Nw / 2 from their mirrors
-      launchG4Mirror(G4_[c].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), stream_);
+      launchG4Mirror(g4()[c].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), stream_);
     G4_host_[c].resize(g4_size_);
-    DCAACC_CUDA_CHECK(cudaMemcpyAsync(G4_host_[c].data(), G4_[c].get(), G4_[c].bytes(),
+    DCAACC_CUDA_CHECK(cudaMemcpyAsync(G4_host_[c].data(), g4()[c].get(), g4()[c].bytes(),
                                       cudaMemcpyDeviceToHost, stream_));
   }
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
@@ -777,18 +819,32 @@ void TpAccumulator::getG4(int channel, double* out, size_t count) const {
 }
 
 void TpAccumulator::sumTo(TpAccumulator& other) {
-  if (other.G4_.size() != G4_.size() || other.g4_size_ != g4_size_)
+  if (other.g4().size() != g4().size() || other.g4_size_ != g4_size_)
     invalid("Objects accumulate different number of channels.");
   if (other.device_ != device_)
     invalid("sumTo requires both accumulators on the same device");
   process();
   other.process();
+  if (other.g4s_ == g4s_) {  // one shared G4: nothing to add (tp_accumulator_gpu.hpp:487-491)
+    // but what other reads of it afterwards (finalize, peek) comes after this handle's updates.
+    cudaEvent_t done;
+    DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    DCAACC_CUDA_CHECK(cudaEventRecord(done, stream_));
+    DCAACC_CUDA_CHECK(cudaStreamWaitEvent(other.stream_, done, 0));
+    DCAACC_CUDA_CHECK(cudaEventDestroy(done));
+    other.sign_sum_ += sign_sum_;
+    other.n_meas_ += n_meas_;
+    sign_sum_ = 0;
+    n_meas_ = 0;
+    other.finalized_ = false;
+    return;
+  }
   cudaEvent_t ev;
   DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   DCAACC_CUDA_CHECK(cudaEventRecord(ev, other.stream_));
   DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, ev, 0));
-  for (size_t c = 0; c < G4_.size(); ++c) {
-    launchAddAndClear(other.G4_[c].get(), G4_[c].get(), g4_size_, stream_);
+  for (size_t c = 0; c < g4().size(); ++c) {
+    launchAddAndClear(other.g4()[c].get(), g4()[c].get(), g4_size_, stream_);
     ++launches_;
   }
   DCAACC_CUDA_CHECK(cudaEventRecord(ev, stream_));
@@ -899,18 +955,18 @@ void TpAccumulator::stageTimes(double* ms, uint64_t* launches, int n) {
 }
 
 void TpAccumulator::peekG4(int channel, size_t offset, size_t count, double* out, bool wait) {
-  if (channel < 0 || channel >= static_cast<int>(G4_.size()))
+  if (channel < 0 || channel >= static_cast<int>(g4().size()))
     invalid("channel index out of range");
   if (offset > g4_size_ || count > g4_size_ - offset)
     invalid("window outside G4");
   process();
-  const double2* src = G4_[channel].get() + offset;
+  const double2* src = g4()[channel].get() + offset;
   if (dims_.half_g4) {  // entries with w1 < Nw / 2 come from their mirrors
     if (peek_d_.size() < count) {
       DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));  // earlier reads may still use the window
       peek_d_.alloc(count);
     }
-    launchG4Window(G4_[channel].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), offset, count, peek_d_.get(),
+    launchG4Window(g4()[channel].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), offset, count, peek_d_.get(),
                    stream_);
     src = peek_d_.get();
   }
@@ -938,7 +994,7 @@ size_t TpAccumulator::deviceFingerprint() const {
   size_t b = G0_.bytes() + Fb_.bytes() + k_add_d_.bytes() + k_sub_d_.bytes() + q_d_.bytes() +
              wex_d_.bytes() + G4_ptrs_.bytes() + Tr_d_.bytes() + Tc_d_.bytes() + X64_.bytes() +
              G64_.bytes() + X32_.bytes() + G32_.bytes() + err_d_.bytes();
-  for (const auto& g : G4_)
+  for (const auto& g : g4())  // a shared G4 is counted by every handle that shares it
     b += g.bytes();
   for (const auto& d : dstage_)
     b += d.sectors.bytes() + d.tau.bytes() + d.M.bytes() + d.perm_r.bytes() + d.perm_c.bytes() +

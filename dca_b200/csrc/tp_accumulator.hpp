@@ -12,6 +12,8 @@
 
 #include <complex>
 #include <cstdint>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -96,7 +98,8 @@ public:
   TpAccumulator(const dcaacc_tp_config& cfg, const double* G0);
   ~TpAccumulator();
 
-  void reset();
+  void reset(long dca_loop = -1);
+  void shareG4(TpAccumulator& owner);
   double accumulate(const dcaacc_sector* sectors, int sign);
   void flush();
   void finalize();
@@ -155,7 +158,24 @@ private:
   bool own_stream_ = false;
   DevBuf<double2> G0_, Fb_;
   DevBuf<int> k_add_d_, k_sub_d_, q_d_, wex_d_;
-  std::vector<DevBuf<double2>> G4_;
+  // The running G4 per channel.  Usually this handle's own; several handles may share one
+  // (shareG4), as the reference's accumulator threads share their static device G4.
+  struct SharedG4 {
+    std::vector<DevBuf<double2>> bufs;
+    std::mutex m;
+    long last_loop = -1;  // dca_loop of the last once-per-loop reset
+  };
+  std::shared_ptr<SharedG4> g4s_;
+  std::vector<DevBuf<double2>>& g4() {
+    return g4s_->bufs;
+  }
+  const std::vector<DevBuf<double2>>& g4() const {
+    return g4s_->bufs;
+  }
+  bool g4Shared() const {
+    return g4s_.use_count() > 1;
+  }
+  void uploadG4Ptrs();
   DevBuf<double2*> G4_ptrs_;
   DevBuf<int> err_d_;  // kernels' error word (async_copy.cuh kErr* bits)
   // Batch workspace.

@@ -117,6 +117,19 @@ void dcaacc_tp_destroy(dcaacc_tp* acc);
 /* resetAccumulation(dca_loop) — tp_accumulator_gpu.hpp:285-296: zeroes G4, re-slices G0, arms accumulate. */
 int dcaacc_tp_reset(dcaacc_tp* acc);
 
+/* The reference's accumulator threads share one static device G4 (get_G4Dev,
+ * tp_accumulator_gpu.hpp:493-497), updated atomically when there are several
+ * (tp_accumulator_kernels.cu:677-680), zeroed once per DCA loop (callOncePerLoop,
+ * tp_accumulator_gpu.hpp:271-296), and sumTo has nothing to add for it (:487-491).  Here each handle
+ * owns its G4 unless share_g4 makes acc accumulate into owner's (same G4 shape and device; acc's
+ * own is released; both switch to atomic updates).  reset_loop is resetAccumulation(dca_loop): a
+ * shared G4 is zeroed only by the first handle that resets for a given dca_loop (synchronously),
+ * a private one on every call.  sum_to between handles sharing G4 moves only the sign sums and
+ * orders the target's later reads (finalize, peek) after the source's updates; without it, a
+ * handle's reads of a shared G4 see another handle's updates once that handle has synchronized. */
+int dcaacc_tp_share_g4(dcaacc_tp* acc, dcaacc_tp* owner);
+int dcaacc_tp_reset_loop(dcaacc_tp* acc, int32_t dca_loop);
+
 /* accumulate(M, configs, sign) — tp_accumulator_gpu.hpp:322-367.
  * sectors: [2] (spin 0, spin 1).  sign: +1 / -1.  flops_out (may be null) receives the
  * reference's flop estimate for the call.  In FP64 mode the measurement is processed

@@ -227,6 +227,40 @@ def test_tuned_launch_shapes_match_builtin(monkeypatch, wname, precision, max_ba
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_shared_g4_matches_single_handle(precision):
+    """Two handles accumulating into one shared G4 (atomic updates, two streams), reset once per
+    DCA loop, give the G4 of one handle fed every measurement; a second reset for the same loop
+    keeps the sums, a reset for the next loop clears them; sumTo between them moves only signs."""
+    from dca_b200.accumulators import TpAccumulator
+    case = case_from_workload(_small("c3", n_range=(30, 60)), 6)
+    kw = dict(precision=precision, max_batch=2)
+    single = run_gpu(case, **kw)
+    a = TpAccumulator(case.G0, case.tp_params(**kw))
+    b = TpAccumulator(case.G0, case.tp_params(**kw))
+    b.share_G4_with(a)
+    a.resetAccumulation(7)
+    b.resetAccumulation(7)
+    for i, m in enumerate(case.measurements):
+        (a if i % 2 == 0 else b).accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    a.flush()
+    b.flush()
+    b.sumTo(a)  # shared G4: only the signs move
+    assert a.sign_sum() == (float(sum(m.sign for m in case.measurements)), 6) and b.sign_sum() == (0.0, 0)
+    a.finalize()
+    # FP64: atomics change only the summation order.  Mixed: the two handles form other batches
+    # than the single one, so the FP32 partial sums round differently (about 3e-8 measured).
+    tol = 1e-12 if precision == 0 else 1e-7
+    for got, want in zip(a.get_G4(), single.get_G4()):
+        assert rel_err(got, want) <= tol
+    window = a.peek_G4(0, 0, 4096)
+    assert np.any(window)
+    b.resetAccumulation(7)  # same loop: the shared sums stay
+    assert np.array_equal(a.peek_G4(0, 0, 4096), window)
+    b.resetAccumulation(8)  # next loop: cleared for both
+    assert not np.any(a.peek_G4(0, 0, 4096))
+
+
 def test_peek_async_matches_peek():
     """peek_G4_async enqueues the read of the running G4 (after the queued measurements) into
     caller memory; after synchronizeCopy it equals the synchronous peek, also with the mirror
