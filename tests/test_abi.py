@@ -77,3 +77,12 @@ def test_bench_reference_arm_prints_one_contract_line():
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": "meas/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_integration_notes_cover_every_entry_point():
+    """Every entry point the header declares has its row (reference counterpart or none) in the
+    integration notes."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    doc = open(os.path.join(root, "INTEGRATION.md")).read()
+    missing = [s for s in declared_symbols() if s not in doc]
+    assert not missing, missing
