@@ -16,9 +16,14 @@ per-spin expansion orders n ~ U[50, 400], batches of 64 measurements, synthetic 
              enqueued without blocking (all landed before the clock stops), wall-clock timed;
              value_blocking_readback: the same loop with a blocking read per step
   roofline   the dominant stage, timed with CUDA events on the accumulator's stream around each
-             stage's launches, in a second pass over the same steps (eager launches)
-  cpu_baseline  the reference's own CPU TpAccumulator (oracle/_ref/tp_ref, FP64) on a bounded
-             sample, one single-threaded process per core
+             stage's launches, in a second pass over the same steps (eager launches): the
+             survey's algorithmic flops (front-end stages) or bytes (G4 update) per launch over
+             that time, against the measured dense BF16 peak or HBM copy bandwidth
+             (MEASURED_PEAKS.json); update_g4_roofline gives the G4 stage in every run, with the
+             DRAM bytes its kernels actually move (committed ncu capture) beside the effective rate
+  cpu_baseline  the reference's own CPU TpAccumulator (oracle/_ref/tp_ref_openblas, FP64) on a
+             bounded sample: one single-threaded process per core, 1 warm-up and 5 timed
+             measurements each, throughput over the wall-clock window of all timed measurements
 
 --impl reference times the reference's CPU accumulator alone (the same workload and unit).
 Multi-GPU (torchrun): independent replicas, one per GPU; value = all ranks' measurements / the
@@ -211,9 +216,28 @@ def _cpu_workers(per_worker_bytes):
     return max(1, min(cores, 64))
 
 
-def run_cpu_reference(w, n_meas_per_worker, warmup, workers=None, tag="sample"):
-    """Runs oracle/_ref/tp_ref (or the restatement oracle if it is absent) in parallel workers.
-    Returns (meas_per_s, workers, kind, seconds)."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+CPU_WARMUP = 1  # untimed measurements per process (first-touch of the process's G4)
+CPU_TIMED = 5   # timed measurements per process
+
+
+def run_cpu_reference(w, timed, warmup, workers=None):
+    """The reference's own TpAccumulator<CPU> (oracle/_ref/tp_ref_openblas, else tp_ref with its
+    naive zgemm_, else the restatement oracle) in P single-threaded processes, one per core, each
+    accumulating warmup + timed measurements of the workload.  Throughput = all processes' timed
+    measurements / the wall-clock window from the first timed measurement's start to the last
+    one's end (every process's timed loop lies inside it).  Returns a dict."""
     from dca_b200 import workloads as W
     from oracle import casefile as CF
     from oracle import pyoracle
@@ -222,35 +246,55 @@ def run_cpu_reference(w, n_meas_per_worker, warmup, workers=None, tag="sample"):
     g4_bytes = 16 * (w.nb ** 4) * cl.nc ** 2 * (2 * w.nw_half) ** 2 * len(w.exchange_momenta(cl.nc)) * len(
         w.exchange_frequencies()) * len(w.channels)
     P = workers or _cpu_workers(g4_bytes * 1.5 + 256e6)
-    kind = "reference" if os.path.exists(pyoracle.REF_BIN) else "port"
+    ref_blas = os.path.join(os.path.dirname(pyoracle.REF_BIN), "tp_ref_openblas")
+    binary = ref_blas if os.path.exists(ref_blas) else pyoracle.REF_BIN
+    kind = "reference" if os.path.exists(binary) else "port"
+    n_per = warmup + timed
     with tempfile.TemporaryDirectory() as d:
+        # Every worker's input is written first, then all workers start together, so that their
+        # timed loops overlap (the throughput is taken over the union of their windows).
+        for i in range(P):
+            ms = W.make_measurements(w, n_per, start=10_000 + i * n_per)
+            CF.write_case(os.path.join(d, f"w{i}.case"), w, cl, g0, ms)
         procs = []
         for i in range(P):
-            ms = W.make_measurements(w, n_meas_per_worker, start=10_000 + i * n_meas_per_worker)
             case = os.path.join(d, f"w{i}.case")
-            CF.write_case(case, w, cl, g0, ms)
             out = os.path.join(d, f"w{i}.out")
             if kind == "reference":
-                cmd = [pyoracle.REF_BIN, case, out, "--no-sp", "--time", "--warmup", str(warmup)]
+                cmd = [binary, case, out, "--no-sp", "--time", "--warmup", str(warmup)]
             else:
                 cmd = [sys.executable, "-c",
-                       "import sys,time;sys.path.insert(0,%r);from oracle import pyoracle;t=time.time();"
-                       "pyoracle.run_case(%r,%r,True,False);print('tp_seconds=%%f'%%(time.time()-t),file=sys.stderr)"
-                       % (ROOT, case, out)]
+                       "import sys,time;sys.path.insert(0,%r);from oracle import pyoracle;"
+                       "pyoracle.run_case(%r,%r,True,False,warmup=%d,report=True)" % (ROOT, case, out, warmup)]
             env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
             procs.append(subprocess.Popen(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
                                           env=env))
-        secs = []
+        starts, ends, blas = [], [], "naive-zgemm"
         for pr in procs:
             _, err = pr.communicate()
             if pr.returncode != 0:
                 raise RuntimeError(f"CPU baseline worker failed: {err}")
             for tok in err.split():
-                if tok.startswith("tp_seconds="):
-                    secs.append(float(tok.split("=")[1]))
-    timed = n_meas_per_worker - (warmup if kind == "reference" else 0)
-    t = max(secs)
-    return P * timed / t, P, kind, t, timed
+                k, _, v = tok.partition("=")
+                if k == "tp_epoch_start":
+                    starts.append(float(v))
+                elif k == "tp_epoch_end":
+                    ends.append(float(v))
+                elif k == "blas":
+                    blas = v
+    window = max(ends) - min(starts)
+    value = P * timed / window
+    if kind == "reference":
+        blas = ("OpenBLAS (" + blas + ", opencv-python-headless wheel, 1 thread)" if blas != "naive-zgemm"
+                else "naive triple-loop zgemm_ (oracle/refbuild/blas_naive.cpp)")
+    else:
+        blas = "none (restatement, own loops)"
+    return {"value": value, "unit": UNIT, "cores": P, "kind": kind,
+            "per_core": value / P, "cpu_model": cpu_model(), "blas": blas,
+            "sample": f"{P} single-threaded processes (one per core) x {timed} timed {w.name} measurements "
+                      f"after {warmup} warm-up, FP64 TpAccumulator<CPU>; window {window:.1f} s from the first "
+                      "timed start to the last timed end",
+            "window_s": window, "timed_per_process": timed, "warmup_per_process": warmup}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -387,82 +431,135 @@ def run_ours(args, world, rank, local):
             j += 1
         torch.cuda.synchronize()
         ref_acc.resetAccumulation(0)
-        ref_acc.enable_timing(True)
         rs = torch.cuda.ExternalStream(ref_acc.get_stream())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # One call for all measurements (each is still processed on its own, max_batch = 1), so
+        # that the host keeps ahead of the GPU.
         e0.record(rs)
-        for j in range(n_cmp):
-            ref_acc.accumulate(dev_M[j], configs[j], signs[j])
+        ref_acc.accumulate_batch(dev_M[:n_cmp], configs[:n_cmp], signs[:n_cmp])
         e1.record(rs)
         torch.cuda.synchronize()
         fp64_ms = max_over_ranks(e0.elapsed_time(e1), world)
         fp64 = world * n_cmp / (fp64_ms / 1e3)
+        # Stage breakdown in a second pass (events between the kernels).
+        ref_acc.resetAccumulation(0)
+        ref_acc.enable_timing(True)
+        ref_acc.accumulate_batch(dev_M[:n_cmp], configs[:n_cmp], signs[:n_cmp])
+        torch.cuda.synchronize()
         fp64_stages = {k: v[0] / n_cmp for k, v in ref_acc.stage_times().items()}
+        ref_acc.enable_timing(False)
         ref_acc.finalize()
-        mixed_acc = TpAccumulator(g0, params)
-        mixed_acc.resetAccumulation(0)
-        for j in range(n_cmp):
-            mixed_acc.accumulate(dev_M[j], configs[j], signs[j])
-        mixed_acc.finalize()
-        err = [float(np.linalg.norm(a - b) / np.linalg.norm(b))
-               for a, b in zip(mixed_acc.get_G4(), ref_acc.get_G4())]
-        del mixed_acc, ref_acc
+        # The mixed handle of the timed region, reset, on the same measurements.
+        acc.resetAccumulation(1)
+        acc.accumulate_batch(dev_M[:n_cmp], configs[:n_cmp], signs[:n_cmp])
+        acc.finalize()
+        err = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(acc.get_G4(), ref_acc.get_G4())]
+        del ref_acc
 
-    # Roofline of the dominant stage.
     hbm_gbs, bf16_tf, peak_src = peaks()
-    dom = max(stages, key=lambda k: stages[k][0])
-    dom_ms, dom_launches = stages[dom]
-    per_launch_ms = dom_ms / max(dom_launches, 1)
+    simt = os.environ.get("DCAACC_TP_SIMT_ONLY") == "1"
     nc, nb, nw = cl.nc, w.nb, 2 * w.nw_half
     nwe = nw + 2 * w.ext()
     D = nb * nc * nwe
+    n_orb = nb * nc
     n_g4 = nb ** 4 * nc ** 2 * nw ** 2 * len(w.exchange_momenta(nc)) * len(w.exchange_frequencies())
-    simt = os.environ.get("DCAACC_TP_SIMT_ONLY") == "1"
-    # The G4 update stage against HBM (the metric's "updateG4 HBM %"), whether or not it is the
-    # dominant stage.  Algorithmic bytes of one batch: the FP64 read-modify-write of every G4 entry
-    # of every channel and one read of the batch's G (FP32 complex, both spins).  With the mirror
-    # symmetries (mirror_mode) the kernels move about half of that.
+    ns = np.array([s.n for m in pool for s in m.sectors], dtype=np.float64)  # both batches of the pool
+    per_step = B / len(pool)  # sectors of one step = per_step * (all sectors of the pool)
+
+    # Algorithmic work of each stage, per step (one batch), from the survey's per-spin counts:
+    # row step 8 NwExt n^2 (row NDFT) + 8 Nc D^2 (row half of the cluster transform); column step
+    # 8 NwExt^2 n_orb n (column NDFT) + 8 Nc D^2 (column half) + 12 D^2 (G0 epilogue, one band) or
+    # 16 nb D^2; G4 update: the FP64 read-modify-write of every running-G4 entry of every channel
+    # and one read of the batch's G (FP32 complex, both spins).
+    epi = 12.0 if nb == 1 else 16.0 * nb
+    alg_flops = {
+        "row_transform": per_step * float(np.sum(8.0 * nwe * ns * ns + 8.0 * nc * D * D)),
+        "col_transform": per_step * float(np.sum(8.0 * nwe * nwe * n_orb * ns + 8.0 * nc * D * D + epi * D * D)),
+    }
     g4_alg_bytes = len(w.channels) * n_g4 * 32 + B * 2 * D * D * 8
     g4_sec = stages["update_g4"][0] / args.steps / 1e3  # the stage's time per batch
-    g4_roof = {"kernels": "discPlanesKernel + frontGemmKernel<2> (disconnected terms) + updateG4DirectMma "
-                          "(direct term, G4 flush)" if not simt else "updateG4SinglebandBatched",
-               "bound": "hbm", "achieved": g4_alg_bytes / g4_sec / 1e9, "peak": hbm_gbs, "unit": "GB/s",
+    g4_paths = {"direct_tc": "discPlanesKernel + frontGemmKernel<2> (disconnected terms) + updateG4DirectMma "
+                             "(direct term, G4 flush)",
+                "split36": "discPlanesKernel + frontGemmKernel<2> (disconnected terms) + "
+                           "updateG4SinglebandOuterSplit (direct term, G4 flush)",
+                "staged": "updateG4StagedKernel (all terms, G blocks staged in shared memory)",
+                "simt": "updateG4SinglebandBatched"}
+    if simt:
+        g4_path = "simt"
+    elif nb > 1:
+        g4_path = "staged"
+    elif nc == 36:
+        g4_path = "split36"
+    else:
+        g4_path = "direct_tc"
+    stage_kernels = {"update_g4": {"direct_tc": ["discPlanesKernel", "frontGemmKernel<2>", "updateG4DirectMma"],
+                                   "split36": ["discPlanesKernel", "frontGemmKernel<2>",
+                                               "updateG4SinglebandOuterSplit"],
+                                   "staged": ["updateG4StagedKernel"]}.get(g4_path, []),
+                     "col_transform": ["frontGemmKernel<1>"], "row_transform": ["frontGemmKernel<0>"],
+                     "twiddle": ["twiddleWiKernel", "buildMOperandKernel", "buildPhasePairKernel"]}
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of each stage's kernels per launch of
+    # the stage, from the committed ncu capture of this workload (cold caches).
+    traffic = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            tk = json.load(f)["workloads"].get(w.name, {})
+        for st, ks in stage_kernels.items():
+            if ks and not simt and all(k in tk for k in ks):
+                traffic[st] = sum(tk[k]["dram_read_bytes"] + tk[k]["dram_write_bytes"] for k in ks)
+    except (OSError, ValueError, KeyError):
+        pass
+
+    g4_roof = {"kernels": g4_paths[g4_path], "bound": "hbm",
+               "achieved": g4_alg_bytes / g4_sec / 1e9, "peak": hbm_gbs, "unit": "GB/s",
                "frac": g4_alg_bytes / g4_sec / 1e9 / hbm_gbs, "algorithmic_bytes": g4_alg_bytes,
-               "ms_per_batch": g4_sec * 1e3, "peak_source": peak_src, "mirror_mode": mirror}
+               "ms_per_batch": g4_sec * 1e3, "peak_source": peak_src, "mirror_mode": mirror,
+               "frac_of_nominal_8tbs": g4_alg_bytes / g4_sec / 8e12}
+    if "update_g4" in traffic:
+        # What the kernels actually move (ncu) over the same time: with the mirror symmetry about
+        # half of the algorithmic bytes, so this rate is below the effective one above.
+        g4_roof["dram_bytes_per_batch"] = traffic["update_g4"]
+        g4_roof["dram_gbs"] = traffic["update_g4"] / g4_sec / 1e9
+        g4_roof["dram_frac"] = g4_roof["dram_gbs"] / hbm_gbs
+
+    # Roofline of the dominant stage (its kernels' CUDA-event time per launch of the stage).
+    dom = max(stages, key=lambda k: stages[k][0])
+    dom_ms, dom_launches = stages[dom]
+    per_launch_ms = dom_ms / max(dom_launches, 1)
+    sec = per_launch_ms / 1e3
     if dom == "update_g4":
         roof = {"kernel": "update_g4 stage: " + g4_roof["kernels"], "bound": "hbm",
-                "achieved": g4_roof["achieved"], "peak": hbm_gbs, "unit": "GB/s",
-                "traffic": None, "peak_source": peak_src, "algorithmic_bytes": g4_alg_bytes}
-    elif dom in ("col_transform", "row_transform") and os.environ.get("DCAACC_TP_SIMT_ONLY") != "1":
-        # Tensor-core front-end.  Algorithmic flops: the complex contractions themselves,
-        # G = X' Q^H (8 D^2 n per sector) or X' = P M (4 D n^2, M real).  The split-FP16 products
-        # cost three FP16 MMAs per such flop (two planes, three plane products), so the roofline
-        # is the measured dense BF16/FP16 peak / 3; the issued MMA rate (tiles of 128 x 128,
-        # K padded to 32) is reported beside it against the plain peak.
-        ns = np.array([s.n for m in pool for s in m.sectors], dtype=np.float64)  # both halves
+                "achieved": g4_alg_bytes / sec / 1e9, "peak": hbm_gbs, "unit": "GB/s",
+                "algorithmic_bytes": g4_alg_bytes}
+        for k in ("dram_gbs", "dram_frac"):
+            if k in g4_roof:
+                roof[k] = g4_roof[k]
+    elif dom in ("col_transform", "row_transform") and not simt:
+        # Tensor-core front-end: the survey's algorithmic flops against the measured dense BF16 peak.
+        # Beside it, the work the kernel is built to do (the dense complex product over all vertices,
+        # split FP16: three MMAs per complex multiply-add pair) and its issued MMA rate (128 x 128
+        # tiles, K padded to 32) against the same peak.
         chunks = np.ceil(ns / 32)
         Dp = -(-D // 128) * 128
-        per_step = B / len(pool)  # pool holds two batches' measurements
         mma_flop = 2.0 * 128 * 128 * 16
-        rows_done = 0.5 if mirror & 1 else 1.0  # half G: the upper frequency half of the rows of G / X'
+        rows_done = 0.5 if mirror & 1 else 1.0  # half G: the upper frequency half of the rows
         if dom == "col_transform":
-            alg = per_step * float(np.sum(8.0 * D * D * ns))
+            dense = per_step * float(np.sum(8.0 * D * D * ns)) * rows_done
             mma = per_step * float(np.sum((Dp // 128) ** 2 * rows_done * chunks * 24 * mma_flop))
             kern = "frontGemmKernel<1> (column step, G = X' Q^H + beta G0 delta)"
         else:
-            alg = per_step * float(np.sum(4.0 * D * ns * ns))
+            dense = per_step * float(np.sum(4.0 * D * ns * ns)) * rows_done
             mma = per_step * float(np.sum((Dp // 128) * rows_done * np.ceil(ns / 128) * chunks * 12 * mma_flop))
             kern = "frontGemmKernel<0> (row step, X' = P M)"
-        sec = per_launch_ms / 1e3
-        roof = {"kernel": kern, "bound": "tensor", "achieved": alg / sec / 1e12, "peak": bf16_tf / 3,
-                "unit": "TFLOP/s", "traffic": None, "peak_source": peak_src,
-                "peak_note": "measured dense BF16 TFLOP/s / 3 (three FP16 MMAs per split-FP16 flop); "
-                             "algorithmic flops count all of G, of which the kernel computes "
-                             f"{int(rows_done * 100)} % (mirror symmetry)",
+        roof = {"kernel": kern, "bound": "tensor", "achieved": alg_flops[dom] / sec / 1e12, "peak": bf16_tf,
+                "unit": "TFLOP/s", "algorithmic_flops": alg_flops[dom],
+                "peak_note": "measured dense BF16 burst peak; algorithmic flops per the survey's per-spin "
+                             "count, so the dense reformulation's extra work is not credited",
+                "dense_form_flops": dense, "dense_form_tflops": dense / sec / 1e12,
                 "mma_issued_tflops": mma / sec / 1e12, "mma_frac_of_bf16_peak": mma / sec / 1e12 / bf16_tf}
     else:
-        # Front-end stages are dominated by their global traffic (M / X' / G, FP32 complex).
-        mean_n = float(np.mean([s.n for m in pool[:B] for s in m.sectors]))
+        # SIMT front-end stages are dominated by their global traffic (M / X' / G, FP32 complex).
+        mean_n = float(np.mean(ns))
         if dom == "col_transform":
             alg_bytes = 2 * B * (D * mean_n * 8 + D * D * 8)
             kern = "colTransformKernel<float>"
@@ -472,23 +569,21 @@ def run_ours(args, world, rank, local):
         else:
             alg_bytes = 2 * B * mean_n * nwe * 16
             kern = "twiddleKernel"
-        roof = {"kernel": kern, "bound": "hbm", "achieved": alg_bytes / (per_launch_ms / 1e3) / 1e9,
-                "peak": hbm_gbs, "unit": "GB/s", "traffic": None, "peak_source": peak_src}
+        roof = {"kernel": kern, "bound": "hbm", "achieved": alg_bytes / sec / 1e9,
+                "peak": hbm_gbs, "unit": "GB/s"}
     roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["peak_source"] = peak_src + " (MEASURED_PEAKS.json)" if peak_src == "measured" else peak_src
     roof["ms_per_launch"] = per_launch_ms
-    # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the stage's kernels from the
-    # committed ncu capture of this workload (one batch, cold caches), per launch of the stage.
-    stage_kernels = {"update_g4": ["discPlanesKernel", "frontGemmKernel<2>", "updateG4DirectMma"],
-                     "col_transform": ["frontGemmKernel<1>"], "row_transform": ["frontGemmKernel<0>"],
-                     "twiddle": ["twiddleWiKernel", "buildMOperandKernel", "buildPhasePairKernel"]}.get(dom, [])
-    try:
-        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
-            tk = json.load(f)["kernels"]
-        if w.name == "c3" and not simt and stage_kernels and all(k in tk for k in stage_kernels):
-            roof["traffic"] = sum(tk[k]["dram_read_bytes"] + tk[k]["dram_write_bytes"] for k in stage_kernels)
-            roof["traffic_unit"] = "bytes per launch of the stage (ncu, profiles/dram_traffic.json)"
-    except (OSError, ValueError, KeyError):
-        pass
+    roof["traffic"] = traffic.get(dom)
+    if roof["traffic"] is not None:
+        roof["traffic_unit"] = "DRAM bytes per launch of the stage (ncu, profiles/dram_traffic.json)"
+    stage_frac = {}
+    for st, (ms_st, _n) in stages.items():
+        t_st = ms_st / args.steps / 1e3
+        if st in alg_flops:
+            stage_frac[st] = {"tflops": alg_flops[st] / t_st / 1e12, "frac_of_bf16": alg_flops[st] / t_st / 1e12 / bf16_tf}
+        elif st == "update_g4":
+            stage_frac[st] = {"gbs": g4_alg_bytes / t_st / 1e9, "frac_of_hbm": g4_alg_bytes / t_st / 1e9 / hbm_gbs}
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -507,6 +602,7 @@ def run_ours(args, world, rank, local):
         "roofline": roof,
         "update_g4_roofline": g4_roof,
         "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
+        "stages_roofline": stage_frac,
         "fp64_unbatched_meas_per_s": fp64,
         "fp64_stages_ms_per_meas": fp64_stages,
         "speedup_vs_fp64": (value / fp64) if fp64 else None,
@@ -514,30 +610,37 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        val, P, kind, t, timed = run_cpu_reference(w, 2, 1)
-        result["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": P, "kind": kind,
-                                  "sample": f"{P} single-threaded processes x {timed} timed {w.name} measurement "
-                                            f"(after 1 warm-up), FP64 TpAccumulator<CPU>, {t:.1f} s"}
+        result["cpu_baseline"] = run_cpu_reference(w, CPU_TIMED, CPU_WARMUP)
+        # The reference's own scale (2x2 cluster, c1) at one core and at all cores.
+        c1 = W.WORKLOADS["c1"]
+        one = run_cpu_reference(c1, 200, 5, workers=1)
+        allc = run_cpu_reference(c1, 200, 5)
+        result["cpu_baseline"]["c1"] = {"workload": c1.describe(with_batch=False),
+                                        "one_core": one["value"], "all_cores": allc["value"],
+                                        "cores": allc["cores"], "unit": UNIT}
     return result
 
 
 def run_reference_arm(args, world, rank):
+    """The reference's CPU accumulator on the host cores: one step = one measurement in each of the
+    P processes.  The run is bounded to a few minutes: at most 2 warm-up and 6 timed steps, and
+    the line reports the steps actually timed."""
     from dca_b200 import workloads as W
     w = W.WORKLOADS[args.workload]
     if rank != 0:
         return None
-    per_worker = min(args.warmup + args.steps, 12)
-    warm = min(args.warmup, max(per_worker - 1, 0))
-    val, P, kind, t, timed = run_cpu_reference(w, per_worker, warm)
+    timed = max(1, min(args.steps, 6))
+    warm = min(args.warmup, 2)
+    cb = run_cpu_reference(w, timed, warm)
+    val = cb["value"]
     return {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / max(timed, 1),
+            "steps": timed, "warmup": warm, "steps_requested": args.steps,
+            "ms_per_step": 1e3 * cb["window_s"] / timed,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
             "data": "synthetic (seeded; dca_b200.workloads)",
             "config": {"workload": w.describe(with_batch=False),
-                       "parallelism": f"{P} CPU processes"},
-            "cpu_baseline": {"value": val, "unit": UNIT, "cores": P, "kind": kind,
-                             "sample": f"{P} processes x {timed} measurements (after {warm} warm-up), "
-                                       f"one step = one measurement per process"},
+                       "parallelism": f"{cb['cores']} CPU processes, one per core"},
+            "cpu_baseline": cb,
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

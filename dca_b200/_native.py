@@ -102,6 +102,7 @@ def _load():
         "dcaacc_tp_destroy": (None, [p]),
         "dcaacc_tp_reset": (i, [p]),
         "dcaacc_tp_accumulate": (i, [p, POINTER(Sector), i, POINTER(c_double)]),
+        "dcaacc_tp_accumulate_typed": (i, [p, POINTER(Sector), i, c_double, c_double, POINTER(c_double)]),
         "dcaacc_tp_accumulate_batch": (i, [p, i, POINTER(Sector), POINTER(c_int32), POINTER(c_double)]),
         "dcaacc_tp_flush": (i, [p]),
         "dcaacc_tp_finalize": (i, [p]),
@@ -145,6 +146,8 @@ def _load():
         "dcaacc_tp_share_g4": (i, [p, p]),
         "dcaacc_tp_reset_loop": (i, [p, i]),
         "dcaacc_tp_get_g4_normalized": (i, [p, i, POINTER(c_double), sz]),
+        "dcaacc_tp_set_fault_injection": (i, [p, i, ctypes.c_uint32]),
+        "dcaacc_set_allocation_failure": (i, [ctypes.c_int64]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -126,19 +126,21 @@ _SECTOR_DTYPE = np.dtype({
 _VERTEX_INTS = ("left_band", "right_band", "left_site", "right_site")
 
 
-def _device_matrix(M, n: int, keep: list):
-    """(pointer, ldm) of a device float64 matrix, made column major if needed."""
+def _device_matrix(M, n: int, keep: list, m_dtype=np.float64):
+    """(pointer, ldm) of a device matrix of element type m_dtype, made column major if needed."""
     import torch
 
-    if M.dtype != torch.float64:
-        raise LogicError("device M must be float64")
+    want = {np.dtype(np.float64): torch.float64, np.dtype(np.float32): torch.float32,
+            np.dtype(np.complex128): torch.complex128, np.dtype(np.complex64): torch.complex64}[np.dtype(m_dtype)]
+    if M.dtype != want:
+        raise LogicError(f"device M must be {want}")
     if n and not (M.stride(0) == 1 and M.stride(1) >= max(n, 1)):
         M = M.t().contiguous().t()  # column major
         keep.append(M)
     return M.data_ptr(), (max(M.stride(1), 1) if n else 1)
 
 
-def _make_sectors(M_pair, configs, keep: list, count: int = 1):
+def _make_sectors(M_pair, configs, keep: list, count: int = 1, m_dtype=np.float64):
     """Sector descriptors for `count` measurements (M_pair / configs hold 2 * count entries), as a
     pointer to dcaacc_sector records.  The vertex arrays of all sectors are packed into one
     float64 and one int32 buffer; everything the pointers refer to is appended to `keep`."""
@@ -164,7 +166,7 @@ def _make_sectors(M_pair, configs, keep: list, count: int = 1):
     if torch is not None and all(type(M) is torch.Tensor and M.is_cuda for M in M_pair):
         # Device matrices (the walkers' M): one pass of attribute reads; a matrix that is not
         # column major float64 goes through _device_matrix.
-        f64 = torch.float64
+        f64 = torch.float64 if np.dtype(m_dtype) == np.float64 else None
         ptrs, lds = [], []
         for M, n in zip(M_pair, lens.tolist()):
             st = M.stride()
@@ -172,7 +174,7 @@ def _make_sectors(M_pair, configs, keep: list, count: int = 1):
                 ptrs.append(M.data_ptr())
                 lds.append(max(st[1], 1) if n else 1)
             else:
-                p_, l_ = _device_matrix(M, n, keep)
+                p_, l_ = _device_matrix(M, n, keep, m_dtype)
                 ptrs.append(p_)
                 lds.append(l_)
         rec["M"] = ptrs
@@ -185,10 +187,10 @@ def _make_sectors(M_pair, configs, keep: list, count: int = 1):
         for s in range(ns):
             M, n = M_pair[s], int(lens[s])
             if hasattr(M, "is_cuda") and M.is_cuda:
-                ptr[s], ldm[s] = _device_matrix(M, n, keep)
+                ptr[s], ldm[s] = _device_matrix(M, n, keep, m_dtype)
                 dev[s] = 1
             else:
-                Mh = np.asfortranarray(np.asarray(M, np.float64)) if n else np.zeros((1, 1), order="F")
+                Mh = np.asfortranarray(np.asarray(M, m_dtype)) if n else np.zeros((1, 1), m_dtype, order="F")
                 keep.append(Mh)
                 ptr[s] = Mh.ctypes.data
                 ldm[s] = max(n, 1)
@@ -252,6 +254,27 @@ class TpAccumulator:
         flops = ctypes.c_double(0)
         _check(N.lib.dcaacc_tp_accumulate(self._h, secs, int(sign), ctypes.byref(flops)))
         self._last_inputs = keep  # device M must outlive the queued work
+        return flops.value
+
+    _SCALARS = {np.dtype(np.float64): 0, np.dtype(np.float32): 1, np.dtype(np.complex128): 2,
+                np.dtype(np.complex64): 3}
+
+    def accumulate_typed(self, M_pair, configs, sign, m_dtype=None) -> float:
+        """accumulate for the reference's other SpScalar / SignType instantiations
+        (dcaacc_tp_accumulate_typed): M of element type m_dtype (by default that of M_pair[0]:
+        float64, float32, complex128 or complex64) and a sign that may be complex.  Complex M or a
+        sign with an imaginary part raise LogicError (DCAACC_UNSUPPORTED)."""
+        if m_dtype is None:
+            M0 = M_pair[0]
+            m_dtype = np.dtype(str(M0.dtype).replace("torch.", "")) if hasattr(M0, "is_cuda") else np.asarray(M0).dtype
+        m_dtype = np.dtype(m_dtype)
+        keep: list = []
+        secs = _make_sectors(M_pair, configs, keep, m_dtype=m_dtype)
+        flops = ctypes.c_double(0)
+        sg = complex(sign)
+        _check(N.lib.dcaacc_tp_accumulate_typed(self._h, secs, self._SCALARS[m_dtype], sg.real, sg.imag,
+                                                ctypes.byref(flops)))
+        self._last_inputs = keep
         return flops.value
 
     def accumulate_batch(self, Ms, configs, signs) -> float:
@@ -391,6 +414,12 @@ class TpAccumulator:
         if out.dtype != np.complex128 or not out.flags.c_contiguous:
             raise ValueError("out must be a contiguous complex128 array")
         _check(N.lib.dcaacc_tp_peek_g4_async(self._h, channel, offset, out.size, _dptr(out.view(np.float64))))
+
+    def set_fault_injection(self, stop_step: int = -1, wait_polls: int = 0):
+        """Error-path tests: the tensor-core direct G4 term's first block stops feeding its
+        consumers before pipeline step stop_step (-1: never), and bounded device waits give up after
+        wait_polls polls (0: built-in limit); the next synchronizeCopy / finalize raises."""
+        _check(N.lib.dcaacc_tp_set_fault_injection(self._h, stop_step, wait_polls))
 
     def num_channels(self) -> int:
         return len(self.parameters.channels)

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
@@ -12,6 +13,23 @@
 #include "tp_accumulator.hpp"
 
 namespace dcaacc {
+
+namespace {
+std::atomic<long> g_alloc_countdown{0};  // > 0: allocations left before the one that fails
+}
+
+void setAllocationFailure(long nth) {
+  g_alloc_countdown.store(nth > 0 ? nth : 0);
+}
+
+void allocationHook() {
+  long c = g_alloc_countdown.load();
+  while (c > 0 && !g_alloc_countdown.compare_exchange_weak(c, c - 1)) {
+  }
+  if (c == 1)
+    throw Error(DCAACC_OOM, "injected allocation failure (dcaacc_set_allocation_failure)");
+}
+
 void computeGNoAlloc(const dcaacc_tp_config& c, const double* G0_dev, const dcaacc_sector* sec,
                      double* G_out, cudaStream_t stream);
 size_t staticScratchBytes();
@@ -83,6 +101,25 @@ int dcaacc_tp_accumulate(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t s
     return null_handle();
   return guard([&] {
     const double f = acc->impl.accumulate(sectors, sign);
+    if (flops_out)
+      *flops_out = f;
+  });
+}
+
+int dcaacc_tp_accumulate_typed(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t m_scalar, double sign_re,
+                               double sign_im, double* flops_out) {
+  if (!acc)
+    return null_handle();
+  return guard([&] {
+    if (m_scalar == DCAACC_SCALAR_C64 || m_scalar == DCAACC_SCALAR_C128)
+      throw dcaacc::Error(DCAACC_UNSUPPORTED, "complex M (complex-valued models) is not implemented");
+    if (m_scalar != DCAACC_SCALAR_F64 && m_scalar != DCAACC_SCALAR_F32)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "unknown M scalar type");
+    if (sign_im != 0.)
+      throw dcaacc::Error(DCAACC_UNSUPPORTED, "complex measurement signs are not implemented");
+    if (sign_re != 1. && sign_re != -1.)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "sign must be +1 or -1");
+    const double f = acc->impl.accumulate(sectors, sign_re > 0 ? 1 : -1, m_scalar == DCAACC_SCALAR_F32);
     if (flops_out)
       *flops_out = f;
   });
@@ -255,6 +292,17 @@ int dcaacc_tp_compute_g_noalloc(const dcaacc_tp_config* cfg, const double* G0,
   if (!cfg)
     return null_handle();
   return guard([&] { dcaacc::computeGNoAlloc(*cfg, G0, sectors, G_out, static_cast<cudaStream_t>(stream)); });
+}
+
+int dcaacc_tp_set_fault_injection(dcaacc_tp* acc, int32_t stop_step, uint32_t wait_polls) {
+  if (!acc)
+    return null_handle();
+  return guard([&] { acc->impl.setFaultInjection(stop_step, wait_polls); });
+}
+
+int dcaacc_set_allocation_failure(int64_t nth) {
+  dcaacc::setAllocationFailure(static_cast<long>(nth));
+  return DCAACC_OK;
 }
 
 int dcaacc_sp_create(const dcaacc_sp_config* cfg, dcaacc_sp** out) {

@@ -71,9 +71,10 @@ __device__ inline bool mbarTryWait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait for the barrier phase with the given parity.  Returns false on timeout after
-// recording it in *err.
-__device__ inline bool mbarWait(uint64_t* bar, uint32_t parity, int* err) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i)
+// recording it in *err.  limit: polls before giving up (kernels that take a runtime limit pass it;
+// 0 is not a valid limit).
+__device__ inline bool mbarWait(uint64_t* bar, uint32_t parity, int* err, uint32_t limit = kWaitLimit) {
+  for (uint32_t i = 0; i < limit; ++i)
     if (mbarTryWait(bar, parity))
       return true;
   atomicOr(err, kErrBarrierTimeout);

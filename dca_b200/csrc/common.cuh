@@ -15,6 +15,12 @@ struct Error : std::runtime_error {
   Error(int s, const std::string& msg) : std::runtime_error(msg), status(s) {}
 };
 
+// Error-path tests: makes the nth device or pinned-host buffer allocation from now on fail as if
+// memory were exhausted (0 turns it off).  Process-wide; defined in api.cpp.
+void setAllocationFailure(long nth);
+// Called before each buffer allocation: throws Error(DCAACC_OOM) on the chosen one.
+void allocationHook();
+
 #define DCAACC_CUDA_CHECK(expr)                                                               \
   do {                                                                                        \
     cudaError_t _e = (expr);                                                                  \

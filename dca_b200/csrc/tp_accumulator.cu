@@ -9,6 +9,7 @@
 
 #include "tp_frontend.hpp"
 #include "tp_g4.hpp"
+#include "tp_sort.hpp"
 
 namespace dcaacc {
 
@@ -19,6 +20,18 @@ namespace {
 }  // namespace
 
 TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
+  // A failure part way (an invalid argument, or an allocation that fails) releases the streams
+  // and events created so far; the device and pinned buffers release themselves.
+  try {
+    init(c, G0);
+  }
+  catch (...) {
+    releaseStreamsAndEvents();
+    throw;
+  }
+}
+
+void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
   // ---- validation (the reference's logic_error cases, tp_accumulator_base.hpp:197-198,
   // tp_accumulator_gpu.hpp:456-468, plus the index tables G4Helper::set trusts) ----
   if (c.n_bands < 1 || c.n_sites < 1 || c.n_w_half < 1 || c.n_sp_freq < 1)
@@ -97,6 +110,7 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   g_sector_stride_ = long(nw_ext) * nw_ext * R * R;
 
   DCAACC_CUDA_CHECK(cudaGetDevice(&device_));
+  DCAACC_CUDA_CHECK(cudaDeviceGetAttribute(&n_sm_, cudaDevAttrMultiProcessorCount, device_));
   DCAACC_CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   own_stream_ = true;
   DCAACC_CUDA_CHECK(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
@@ -175,6 +189,7 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
 
   // ---- G4 per channel ----
   g4s_ = std::make_shared<SharedG4>();
+  g4s_->users.push_back(this);
   g4() = std::vector<DevBuf<double2>>(c.n_channels);
   for (auto& g : g4()) {
     g.alloc(g4_size_);
@@ -192,10 +207,18 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   for (auto& d : dstage_) {
     d.sectors.alloc(n_sec);
     d.tau.alloc(n_vtx);
+    d.vb_r.alloc(n_vtx);
+    d.vs_r.alloc(n_vtx);
+    if (non_density_) {
+      d.vb_c.alloc(n_vtx);
+      d.vs_c.alloc(n_vtx);
+    }
     d.perm_r.alloc(n_vtx);
-    d.perm_c.alloc(n_vtx);
     d.rstart.alloc(n_sec * n_orb1);
-    d.cstart.alloc(n_sec * n_orb1);
+    if (non_density_) {
+      d.perm_c.alloc(n_vtx);
+      d.cstart.alloc(n_sec * n_orb1);
+    }
     d.signs.alloc(max_batch_);
     d.M.alloc(n_sec * size_t(max_order_) * max_order_);
   }
@@ -228,7 +251,8 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
       for (auto& d : dstage_) {
         d.orb_r.alloc(n_vtx);
-        d.orb_c.alloc(n_vtx);
+        if (non_density_)
+          d.orb_c.alloc(n_vtx);
       }
       gmax_d_.alloc(2 * size_t(max_batch_));
       if (discGemmApplies(dims_, max_batch_)) {
@@ -300,13 +324,13 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
   for (auto& h : hstage_) {
     h.sectors.alloc(n_sec);
     h.tau.alloc(n_vtx);
-    h.perm_r.alloc(n_vtx);
-    h.perm_c.alloc(n_vtx);
-    h.rstart.alloc(n_sec * n_orb1);
-    h.cstart.alloc(n_sec * n_orb1);
+    h.vb_r.alloc(n_vtx);
+    h.vs_r.alloc(n_vtx);
+    if (non_density_) {
+      h.vb_c.alloc(n_vtx);
+      h.vs_c.alloc(n_vtx);
+    }
     h.signs.alloc(max_batch_);
-    h.orb_r.alloc(n_vtx);
-    h.orb_c.alloc(n_vtx);
     DCAACC_CUDA_CHECK(cudaEventRecord(h.uploaded, copy_stream_));
   }
   for (auto& d : dstage_)
@@ -318,6 +342,15 @@ TpAccumulator::TpAccumulator(const dcaacc_tp_config& c, const double* G0) {
 }
 
 TpAccumulator::~TpAccumulator() {
+  if (g4s_) {
+    std::lock_guard<std::mutex> lock(g4s_->m);
+    auto& u = g4s_->users;
+    u.erase(std::remove(u.begin(), u.end(), this), u.end());
+  }
+  releaseStreamsAndEvents();
+}
+
+void TpAccumulator::releaseStreamsAndEvents() {
   if (stream_)
     cudaStreamSynchronize(stream_);
   if (copy_stream_)
@@ -326,17 +359,33 @@ TpAccumulator::~TpAccumulator() {
     cudaEventDestroy(t.begin);
     cudaEventDestroy(t.end);
   }
+  timed_.clear();
   releaseGraphs();
   for (auto& h : hstage_)
-    if (h.uploaded)
+    if (h.uploaded) {
       cudaEventDestroy(h.uploaded);
+      h.uploaded = nullptr;
+    }
   for (auto& d : dstage_)
-    if (d.consumed)
+    if (d.consumed) {
       cudaEventDestroy(d.consumed);
+      d.consumed = nullptr;
+    }
   if (copy_stream_)
     cudaStreamDestroy(copy_stream_);
+  copy_stream_ = nullptr;
   if (own_stream_ && stream_)
     cudaStreamDestroy(stream_);
+  stream_ = nullptr;
+}
+
+// Error-path tests: see G4Args::wait_limit / fault_stop_step.  Launch arguments recorded in the
+// CUDA graphs change, so the graphs are dropped.
+void TpAccumulator::setFaultInjection(int stop_step, uint32_t wait_polls) {
+  DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
+  releaseGraphs();
+  fault_stop_step_ = stop_step;
+  wait_limit_ = wait_polls;
 }
 
 void TpAccumulator::uploadG4Ptrs() {
@@ -348,18 +397,56 @@ void TpAccumulator::uploadG4Ptrs() {
 
 // This handle accumulates into owner's G4 from now on (its own is released when no handle uses it
 // any more); both switch to atomic read-modify-writes, since their streams run concurrently.
+// True when other accumulates the same G4 entries as this handle: same sizes, transfer lists,
+// channels (in the same order) and beta.
+bool TpAccumulator::sameG4(const TpAccumulator& o) const {
+  if (o.g4_size_ != g4_size_ || o.g4().size() != g4().size() || o.dims_.nb != dims_.nb || o.dims_.nc != dims_.nc ||
+      o.dims_.nw != dims_.nw || o.q_list_ != q_list_ || o.wex_list_ != wex_list_ || o.dims_.beta != dims_.beta)
+    return false;
+  for (int c = 0; c < dims_.n_channels; ++c)
+    if (o.dims_.channels[c] != dims_.channels[c])
+      return false;
+  return true;
+}
+
 void TpAccumulator::shareG4(TpAccumulator& owner) {
   if (&owner == this || owner.g4s_ == g4s_)
     return;
-  if (owner.g4_size_ != g4_size_ || owner.g4().size() != g4().size() || owner.dims_.half_g4 != dims_.half_g4)
-    invalid("accumulators with different G4 shapes cannot share G4");
+  if (!sameG4(owner) || owner.dims_.half_g4 != dims_.half_g4)
+    invalid("accumulators with different G4 shapes, transfers, channels, beta or mirror modes cannot share G4");
   if (owner.device_ != device_)
     invalid("sharing G4 requires both accumulators on the same device");
   process();
   owner.process();
+  // What this handle has accumulated so far moves into the shared G4 (with its sign sum, which
+  // stays with this handle), so no measurement is dropped with the released buffers.
+  if (n_meas_ > 0) {
+    // After every update already enqueued on the streams of the handles that use owner's G4.
+    std::lock_guard<std::mutex> lock(owner.g4s_->m);
+    for (TpAccumulator* u : owner.g4s_->users) {
+      cudaEvent_t ev;
+      DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      DCAACC_CUDA_CHECK(cudaEventRecord(ev, u->stream_));
+      DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, ev, 0));
+      DCAACC_CUDA_CHECK(cudaEventDestroy(ev));
+    }
+    for (size_t c = 0; c < g4().size(); ++c) {
+      launchAddAndClear(owner.g4()[c].get(), g4()[c].get(), g4_size_, stream_);
+      ++launches_;
+    }
+  }
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));  // this handle's kernels are done with its own G4
   DCAACC_CUDA_CHECK(cudaStreamSynchronize(owner.stream_));
+  {
+    std::lock_guard<std::mutex> lock(g4s_->m);
+    auto& u = g4s_->users;
+    u.erase(std::remove(u.begin(), u.end(), this), u.end());
+  }
   g4s_ = owner.g4s_;
+  {
+    std::lock_guard<std::mutex> lock(g4s_->m);
+    g4s_->users.push_back(this);
+  }
   uploadG4Ptrs();
   // The update mode is a kernel argument: graphs captured before are dropped on both sides.
   releaseGraphs();
@@ -384,6 +471,17 @@ void TpAccumulator::reset(long dca_loop) {
     // accumulation of this loop can run before the zeroing.
     std::lock_guard<std::mutex> lock(g4s_->m);
     if (dca_loop < 0 || dca_loop != g4s_->last_loop) {
+      // Updates still in flight on the other sharing handles' streams (from the loop that ends
+      // here) land before the zeroing; measurements they have queued but not yet launched count
+      // toward the new loop.
+      for (TpAccumulator* u : g4s_->users)
+        if (u != this && u->stream_ != stream_) {
+          cudaEvent_t ev;
+          DCAACC_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+          DCAACC_CUDA_CHECK(cudaEventRecord(ev, u->stream_));
+          DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, ev, 0));
+          DCAACC_CUDA_CHECK(cudaEventDestroy(ev));
+        }
       for (auto& g : g4())
         DCAACC_CUDA_CHECK(cudaMemsetAsync(g.get(), 0, g.bytes(), stream_));
       DCAACC_CUDA_CHECK(cudaStreamSynchronize(stream_));
@@ -443,7 +541,7 @@ double TpAccumulator::flopEstimate(const dcaacc_sector* sec) const {
   return f;
 }
 
-void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
+void TpAccumulator::stage(const dcaacc_sector* sec, int sign, bool m_f32) {
   if (slots_ == 0) {
     DCAACC_CUDA_CHECK(cudaEventSynchronize(hs().uploaded));  // this staging set is free again
     // Copies into this device set wait for the kernels of the batch that last used it.
@@ -457,48 +555,24 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
     const int vtx_off = vtx_used_;
     const int sidx = 2 * slot + s;
     const int orb_off = sidx * (n_orb + 1);
-    // Orbital of each vertex on the row side (right band / site) and the column side
-    // (left band / site for non-density-density models), cached_ndft_base.hpp:97-103.
-    // A counting sort keeps vertex order inside an orbital, i.e. the reference's
-    // (orbital, idx) ordering.
-    auto sort_side = [&](bool left, int* perm, int* start) {
-      std::fill(start, start + n_orb + 1, 0);
-      for (int v = 0; v < n; ++v) {
-        const int o = left ? x.left_band[v] + dims_.nb * x.left_site[v]
-                           : x.right_band[v] + dims_.nb * x.right_site[v];
-        start[o + 1]++;
-      }
-      for (int o = 0; o < n_orb; ++o)
-        start[o + 1] += start[o];
-      std::vector<int> fill(start, start + n_orb);
-      for (int v = 0; v < n; ++v) {
-        const int o = left ? x.left_band[v] + dims_.nb * x.left_site[v]
-                           : x.right_band[v] + dims_.nb * x.right_site[v];
-        perm[fill[o]++] = v;
-      }
-    };
-    sort_side(false, hs().perm_r.get() + vtx_off, hs().rstart.get() + orb_off);
-    if (non_density_)
-      sort_side(true, hs().perm_c.get() + vtx_off, hs().cstart.get() + orb_off);
-    else {
-      std::copy_n(hs().perm_r.get() + vtx_off, n, hs().perm_c.get() + vtx_off);
-      std::copy_n(hs().rstart.get() + orb_off, n_orb + 1, hs().cstart.get() + orb_off);
-    }
-    // Orbital of each sorted position (the tensor-core front-end's per-vertex phases).
-    for (int o = 0; o < n_orb; ++o) {
-      const int* rs = hs().rstart.get() + orb_off;
-      const int* cs = hs().cstart.get() + orb_off;
-      std::fill(hs().orb_r.get() + vtx_off + rs[o], hs().orb_r.get() + vtx_off + rs[o + 1], o);
-      std::fill(hs().orb_c.get() + vtx_off + cs[o], hs().orb_c.get() + vtx_off + cs[o + 1], o);
+    // The vertices as given; the device sorts them by orbital (tp_sort.cu): the row side by the
+    // right band / site, the column side of non-density-density models by the left ones
+    // (cached_ndft_base.hpp:97-103).
+    std::copy_n(x.right_band, n, hs().vb_r.get() + vtx_off);
+    std::copy_n(x.right_site, n, hs().vs_r.get() + vtx_off);
+    if (non_density_) {
+      std::copy_n(x.left_band, n, hs().vb_c.get() + vtx_off);
+      std::copy_n(x.left_site, n, hs().vs_c.get() + vtx_off);
     }
     std::copy_n(x.tau, n, hs().tau.get() + vtx_off);
 
     const double* Mptr = x.M;
     int ldm = std::max(x.ldm, 1);
+    const size_t esize = m_f32 ? sizeof(float) : sizeof(double);
     if (n && !x.m_on_device) {
       double* dst = dstage_[hset_].M.get() + m_used_;
-      m_used_ += size_t(n) * n;
-      const size_t bytes = sizeof(double) * n * n;
+      m_used_ += (esize * n * n + sizeof(double) - 1) / sizeof(double);
+      const size_t bytes = esize * n * n;
       if (x.ldm == n) {
         if (mcopy_bytes_ && reinterpret_cast<const char*>(mcopy_src_) + mcopy_bytes_ == reinterpret_cast<const char*>(x.M) &&
             reinterpret_cast<char*>(mcopy_dst_) + mcopy_bytes_ == reinterpret_cast<char*>(dst)) {
@@ -515,8 +589,8 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
       }
       else {
         flushMCopy();
-        DCAACC_CUDA_CHECK(cudaMemcpy2DAsync(dst, sizeof(double) * n, x.M, sizeof(double) * x.ldm,
-                                            sizeof(double) * n, n, cudaMemcpyHostToDevice, copy_stream_));
+        DCAACC_CUDA_CHECK(cudaMemcpy2DAsync(dst, esize * n, x.M, esize * x.ldm, esize * n, n, cudaMemcpyHostToDevice,
+                                            copy_stream_));
       }
       Mptr = dst;
       ldm = n;
@@ -529,6 +603,7 @@ void TpAccumulator::stage(const dcaacc_sector* sec, int sign) {
     d.orb_off = orb_off;
     d.spin = s;
     d.slot = slot;
+    d.m_f32 = m_f32 ? 1 : 0;
     d.x_off = x_used_;
     hs().sectors[sidx] = d;
     x_used_ += long(dims_.R) * n * dims_.nw_ext;
@@ -550,7 +625,6 @@ void TpAccumulator::process() {
     return;
   flushMCopy();
   const int n_sec = 2 * slots_;
-  const int n_orb1 = dims_.n_orb + 1;
   // Uploads on the copy stream (after the kernels that last read this device set, see stage());
   // the kernels below wait for them.
   DevStage& ds = dstage_[hset_];
@@ -560,15 +634,13 @@ void TpAccumulator::process() {
   };
   h2d(ds.sectors.get(), hs().sectors.get(), sizeof(SectorDesc) * n_sec);
   h2d(ds.tau.get(), hs().tau.get(), sizeof(double) * vtx_used_);
-  h2d(ds.perm_r.get(), hs().perm_r.get(), sizeof(int) * vtx_used_);
-  h2d(ds.perm_c.get(), hs().perm_c.get(), sizeof(int) * vtx_used_);
-  h2d(ds.rstart.get(), hs().rstart.get(), sizeof(int) * n_sec * n_orb1);
-  h2d(ds.cstart.get(), hs().cstart.get(), sizeof(int) * n_sec * n_orb1);
-  h2d(ds.signs.get(), hs().signs.get(), sizeof(int) * slots_);
-  if (tc_front_) {
-    h2d(ds.orb_r.get(), hs().orb_r.get(), sizeof(int) * vtx_used_);
-    h2d(ds.orb_c.get(), (non_density_ ? hs().orb_c : hs().orb_r).get(), sizeof(int) * vtx_used_);
+  h2d(ds.vb_r.get(), hs().vb_r.get(), sizeof(int) * vtx_used_);
+  h2d(ds.vs_r.get(), hs().vs_r.get(), sizeof(int) * vtx_used_);
+  if (non_density_) {
+    h2d(ds.vb_c.get(), hs().vb_c.get(), sizeof(int) * vtx_used_);
+    h2d(ds.vs_c.get(), hs().vs_c.get(), sizeof(int) * vtx_used_);
   }
+  h2d(ds.signs.get(), hs().signs.get(), sizeof(int) * slots_);
   DCAACC_CUDA_CHECK(cudaEventRecord(hs().uploaded, copy_stream_));
   DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, hs().uploaded, 0));
   const int set = hset_;
@@ -615,8 +687,10 @@ void TpAccumulator::process() {
   ga.disc = have_disc_ ? &disc_ws_ : nullptr;
   ga.gmax = tc_front_ ? gmax_d_.get() : nullptr;
   ga.tile_order = dims_.half_g4 ? tile_order_d_.get() : nullptr;
-  ga.n_sm = ftc_.n_sm;
+  ga.n_sm = n_sm_;
   ga.tuner = &tuner_;
+  ga.wait_limit = wait_limit_;
+  ga.fault_stop_step = fault_stop_step_;
 
   const bool graphable = graphs_on_ && tc_front_ && !timing_ && n_max_batch_ > 0 && stream_ != nullptr &&
                          stream_ != cudaStreamLegacy && stream_ != cudaStreamPerThread;
@@ -639,6 +713,16 @@ int TpAccumulator::launchBatch(const FrontendArgs& fa, const G4Args& ga, DevStag
   cudaEvent_t b = nullptr;
   if (fa.n_max > 0) {
     timeBegin(DCAACC_STAGE_TWIDDLE, &b);
+    // Vertex order and orbital runs of every sector (sortConfiguration), row side and, for
+    // non-density-density models, column side.
+    launchSortVertices(fa.sectors, fa.n_sectors, ds.vb_r.get(), ds.vs_r.get(), dims_.nb, dims_.n_orb,
+                       ds.perm_r.get(), ds.rstart.get(), ds.orb_r.get(), stream_);
+    launched += 1;
+    if (non_density_) {
+      launchSortVertices(fa.sectors, fa.n_sectors, ds.vb_c.get(), ds.vs_c.get(), dims_.nb, dims_.n_orb,
+                         ds.perm_c.get(), ds.cstart.get(), ds.orb_c.get(), stream_);
+      launched += 1;
+    }
     int n_prep;
     if (tc_front_) {
       n_prep = launchFrontendTcPrep(fa, ftc_, ds.orb_r.get(), non_density_ ? ds.orb_c.get() : ds.orb_r.get(),
@@ -649,7 +733,7 @@ int TpAccumulator::launchBatch(const FrontendArgs& fa, const G4Args& ga, DevStag
       n_prep = non_density_ ? 2 : 1;
     }
     launched += n_prep;
-    timeEnd(DCAACC_STAGE_TWIDDLE, b, n_prep);
+    timeEnd(DCAACC_STAGE_TWIDDLE, b, n_prep + (non_density_ ? 2 : 1));
   }
   timeBegin(DCAACC_STAGE_ROW, &b);
   if (tc_front_)
@@ -756,7 +840,7 @@ void TpAccumulator::graphStats(uint64_t* captures, uint64_t* replays) const {
     *replays = graph_replays_;
 }
 
-double TpAccumulator::accumulate(const dcaacc_sector* sectors, int sign) {
+double TpAccumulator::accumulate(const dcaacc_sector* sectors, int sign, bool m_f32) {
   if (!ready_)
     throw Error(DCAACC_NOT_READY, "The accumulator is not ready to measure.");
   if (!sectors)
@@ -771,7 +855,7 @@ double TpAccumulator::accumulate(const dcaacc_sector* sectors, int sign) {
     return 0.;
   if (slots_ == max_batch_)
     process();
-  stage(sectors, sign);
+  stage(sectors, sign, m_f32);
   if (slots_ == max_batch_)
     process();
   return flopEstimate(sectors);
@@ -819,8 +903,10 @@ void TpAccumulator::getG4(int channel, double* out, size_t count) const {
 }
 
 void TpAccumulator::sumTo(TpAccumulator& other) {
-  if (other.g4().size() != g4().size() || other.g4_size_ != g4_size_)
+  if (other.g4().size() != g4().size())
     invalid("Objects accumulate different number of channels.");
+  if (!sameG4(other))
+    invalid("sumTo between accumulators of different G4 shapes, transfers, channels or beta");
   if (other.device_ != device_)
     invalid("sumTo requires both accumulators on the same device");
   process();
@@ -844,6 +930,13 @@ void TpAccumulator::sumTo(TpAccumulator& other) {
   DCAACC_CUDA_CHECK(cudaEventRecord(ev, other.stream_));
   DCAACC_CUDA_CHECK(cudaStreamWaitEvent(stream_, ev, 0));
   for (size_t c = 0; c < g4().size(); ++c) {
+    // A half-G4 source holds only the tiles with w1 >= Nw / 2; a full-G4 target needs the rest
+    // too, so the source's lower half is filled from its mirror first.  (A full source adding into
+    // a half target is complete already: the target refills its lower half from its upper half.)
+    if (dims_.half_g4 && !other.dims_.half_g4) {
+      launchG4Mirror(g4()[c].get(), dims_, q_mirror_d_.get(), wq_mirror_d_.get(), stream_);
+      ++launches_;
+    }
     launchAddAndClear(other.g4()[c].get(), g4()[c].get(), g4_size_, stream_);
     ++launches_;
   }
@@ -997,7 +1090,8 @@ size_t TpAccumulator::deviceFingerprint() const {
   for (const auto& g : g4())  // a shared G4 is counted by every handle that shares it
     b += g.bytes();
   for (const auto& d : dstage_)
-    b += d.sectors.bytes() + d.tau.bytes() + d.M.bytes() + d.perm_r.bytes() + d.perm_c.bytes() +
+    b += d.vb_r.bytes() + d.vs_r.bytes() + d.vb_c.bytes() + d.vs_c.bytes() +
+         d.sectors.bytes() + d.tau.bytes() + d.M.bytes() + d.perm_r.bytes() + d.perm_c.bytes() +
          d.rstart.bytes() + d.cstart.bytes() + d.signs.bytes() + d.orb_r.bytes() + d.orb_c.bytes();
   return b;
 }

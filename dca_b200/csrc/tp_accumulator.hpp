@@ -40,9 +40,12 @@ public:
     if (p_)
       cudaFree(p_);
     p_ = nullptr;
-    n_ = n;
-    if (n)
+    n_ = 0;
+    if (n) {
+      allocationHook();
       DCAACC_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+    }
+    n_ = n;
   }
   T* get() const {
     return p_;
@@ -74,9 +77,12 @@ public:
     if (p_)
       cudaFreeHost(p_);
     p_ = nullptr;
-    n_ = n;
-    if (n)
+    n_ = 0;
+    if (n) {
+      allocationHook();
       DCAACC_CUDA_CHECK(cudaMallocHost(&p_, n * sizeof(T)));
+    }
+    n_ = n;
   }
   T* get() const {
     return p_;
@@ -100,7 +106,8 @@ public:
 
   void reset(long dca_loop = -1);
   void shareG4(TpAccumulator& owner);
-  double accumulate(const dcaacc_sector* sectors, int sign);
+  // m_f32: the sectors' M hold float elements (else double).
+  double accumulate(const dcaacc_sector* sectors, int sign, bool m_f32 = false);
   void flush();
   void finalize();
   void getG4(int channel, double* out, size_t count) const;
@@ -134,10 +141,16 @@ public:
     return tuner_.report();
   }
   void peekG4(int channel, size_t offset, size_t count, double* out, bool wait = true);
+  void setFaultInjection(int stop_step, uint32_t wait_polls);
 
 private:
+  void init(const dcaacc_tp_config& cfg, const double* G0);
+  void releaseStreamsAndEvents();
+  int fault_stop_step_ = -1;  // error-path tests (G4Args::fault_stop_step)
+  uint32_t wait_limit_ = 0;   // error-path tests (G4Args::wait_limit)
   void validateSector(const dcaacc_sector& s) const;
-  void stage(const dcaacc_sector* sectors, int sign);
+  bool sameG4(const TpAccumulator& o) const;
+  void stage(const dcaacc_sector* sectors, int sign, bool m_f32);
   void process();
   double flopEstimate(const dcaacc_sector* sectors) const;
 
@@ -154,6 +167,7 @@ private:
 
   // Device state.
   int device_ = 0;
+  int n_sm_ = 0;  // multiprocessors of the device (persistent grids)
   cudaStream_t stream_ = nullptr;
   bool own_stream_ = false;
   DevBuf<double2> G0_, Fb_;
@@ -164,6 +178,7 @@ private:
     std::vector<DevBuf<double2>> bufs;
     std::mutex m;
     long last_loop = -1;  // dca_loop of the last once-per-loop reset
+    std::vector<TpAccumulator*> users;  // handles accumulating into it (guarded by m)
   };
   std::shared_ptr<SharedG4> g4s_;
   std::vector<DevBuf<double2>>& g4() {
@@ -184,7 +199,8 @@ private:
   struct DevStage {
     DevBuf<SectorDesc> sectors;
     DevBuf<double> tau, M;  // M: host-resident sectors' matrices, copied in
-    DevBuf<int> perm_r, perm_c, rstart, cstart, signs, orb_r, orb_c;
+    DevBuf<int> vb_r, vs_r, vb_c, vs_c;  // per-vertex band and site of the row / column side (uploaded)
+    DevBuf<int> perm_r, perm_c, rstart, cstart, signs, orb_r, orb_c;  // sorted on the device
     cudaEvent_t consumed = nullptr;  // the kernels that read this set have completed
   };
   DevStage dstage_[2];
@@ -226,7 +242,7 @@ private:
   struct HostStage {
     PinBuf<SectorDesc> sectors;
     PinBuf<double> tau;
-    PinBuf<int> perm_r, perm_c, rstart, cstart, signs, orb_r, orb_c;
+    PinBuf<int> vb_r, vs_r, vb_c, vs_c, signs;
     cudaEvent_t uploaded = nullptr;  // the uploads from this set have completed
   };
   HostStage hstage_[2];

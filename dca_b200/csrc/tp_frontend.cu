@@ -126,7 +126,7 @@ rowTransformKernel(const TpDims dims, const SectorDesc* __restrict__ sectors,
     for (int idx = t; idx < JC * ib_count; idx += blockDim.x) {
       const int c = idx / ib_count, ib = idx % ib_count;
       Ms[c * MS + ib] = c < jc_count
-                            ? static_cast<Real>(sd.M[static_cast<long>(sd.ldm) * pc[jj0 + c] + pr[i0 + ib]])
+                            ? static_cast<Real>(loadM(sd, static_cast<long>(sd.ldm) * pc[jj0 + c] + pr[i0 + ib]))
                             : Real(0);
     }
     __syncthreads();

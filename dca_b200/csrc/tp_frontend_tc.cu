@@ -307,7 +307,7 @@ buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restric
   const int* pr = perm_r + sd.vtx_off;
   const int warps = gridDim.x * (blockDim.x / 32);
   for (int j = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; j < rows; j += warps) {
-    const double* col = j < n ? sd.M + static_cast<long>(sd.ldm) * perm_c[sd.vtx_off + j] : nullptr;
+    const long col0 = j < n ? static_cast<long>(sd.ldm) * perm_c[sd.vtx_off + j] : -1;
     double mx = 0;
     __syncwarp();  // the previous row's reads of mrow are done
     for (int i0 = 0; i0 < n; i0 += 128) {  // four loads in flight per lane
@@ -315,7 +315,7 @@ buildMOperandKernel(const SectorDesc* __restrict__ sectors, const int* __restric
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const int i = i0 + 32 * u + lane;
-        m[u] = (col && i < n) ? col[i] : 0.;
+        m[u] = (col0 >= 0 && i < n) ? loadM(sd, col0 + i) : 0.;
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {

@@ -602,6 +602,157 @@ updateG4SinglebandPH(const TpDims dims, const GT* __restrict__ G, long g_sector_
   }
 }
 
+// Single-band PH-magnetic / PH-charge update of ONE measurement, streaming: the bandwidth-bound
+// case (the plain FP64 path feeds measurements one at a time).  Persistent CTAs walk the (w1, w2,
+// wq) tiles; per tile the eight R x R blocks (A, B, C, E of both spins, see updateG4SinglebandPH)
+// are bulk-copied into one of two shared-memory stages while the previous tile is processed, and
+// the tile's G4 entries are streamed in memory order (k1 contiguous, then k2, then q): a thread
+// takes 8 entries of one channel at a time, issues their 8 loads, then adds and stores them.  A's
+// rows are staged with a one-element pad (row stride R + 1) so that lanes of consecutive k1 read
+// distinct banks.  Each G4 entry is read and written once; G is read from L2 once per tile.
+template <typename GT, typename AT>
+__global__ void __launch_bounds__(256, 3)
+updateG4SinglebandStream(const TpDims dims, const GT* __restrict__ G, long g_sector_stride,
+                         const int* __restrict__ signs, const int* __restrict__ k_add,
+                         const int* __restrict__ q_list, const int* __restrict__ wex_list,
+                         double2* const* __restrict__ G4, bool atomic, int* __restrict__ err) {
+  using C = cplx_t<AT>;
+  constexpr int kRound = 8;  // entries in flight per thread
+  const int nc = dims.nc, nw = dims.nw, nw_ext = dims.nw_ext, R = dims.R, nq = dims.nq, ext = dims.ext;
+  const int n_tiles = nw * nw * dims.nwq;
+  const int t = threadIdx.x;
+  const int RP = R + 1;                        // padded row stride of A
+  const int blk = R * R, blkA = R * RP;
+  const int stage_elems = 2 * (blkA + 3 * blk);  // per spin: A (padded), B, C, E
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);  // [2]
+  int* kadd = reinterpret_cast<int*>(smem_raw + 16);      // [nc][nc]
+  int* qtab = kadd + nc * nc;                             // [nq]
+  GT* stage = reinterpret_cast<GT*>(smem_raw + 16 + ((sizeof(int) * (nc * nc + nq) + 15) / 16) * 16);
+
+  for (int i = t; i < nc * nc; i += blockDim.x)
+    kadd[i] = k_add[i];
+  for (int i = t; i < nq; i += blockDim.x)
+    qtab[i] = q_list[i];
+  if (t == 0) {
+    mbarInit(&bar[0], 1);
+    mbarInit(&bar[1], 1);
+    fenceBarrierInit();
+  }
+  __syncthreads();
+
+  auto tileOf = [&](int tile, int& w1, int& w2, int& iwq) {
+    w1 = tile % nw;
+    w2 = (tile / nw) % nw;
+    iwq = tile / (nw * nw);
+  };
+  // Warp 0 issues a tile's copies: per spin, A row by row (padded), then B, C, E whole.
+  const uint32_t row_bytes = static_cast<uint32_t>(R * sizeof(GT)), blk_bytes = row_bytes * R;
+  auto issue = [&](int tile, int st) {
+    int w1, w2, iwq;
+    tileOf(tile, w1, w2, iwq);
+    const int wex = wex_list[iwq];
+    const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
+    const long bA = (static_cast<long>(w1e) * nw_ext + w2e) * blk, bB = (static_cast<long>(w2x) * nw_ext + w1x) * blk,
+               bC = (static_cast<long>(w1e) * nw_ext + w1x) * blk, bE = (static_cast<long>(w2x) * nw_ext + w2e) * blk;
+    GT* dst = stage + static_cast<long>(st) * stage_elems;
+    const int lane = t & 31;
+    if (lane == 0)
+      mbarArriveExpectTx(&bar[st], 2 * (blk_bytes * 4));
+    __syncwarp();
+    for (int c = lane; c < 2 * (R + 3); c += 32) {  // per spin: R row copies of A, 3 block copies
+      const int s = c / (R + 3), j = c % (R + 3);
+      const GT* src = G + g_sector_stride * s;
+      GT* d = dst + s * (blkA + 3 * blk);
+      if (j < R)
+        bulkCopyG2S(d + j * RP, src + bA + j * R, row_bytes, &bar[st]);
+      else {
+        const int b = j - R;  // 0: B, 1: C, 2: E
+        bulkCopyG2S(d + blkA + b * blk, src + (b == 0 ? bB : b == 1 ? bC : bE), blk_bytes, &bar[st]);
+      }
+    }
+  };
+
+  // Bit c: channel c is PH-magnetic (else PH-charge); static indices keep dims in registers.
+  int mag_bits = 0;
+#pragma unroll
+  for (int c = 0; c < kMaxChannels; ++c)
+    mag_bits |= (c < dims.n_channels && dims.channels[c] == 2) << c;
+  const int n_ch = dims.n_channels;
+  const AT hs = AT(0.5) * static_cast<AT>(signs[0]);
+  const long s_w2 = long(nc) * nw * nc, s_wq = s_w2 * nw * nq;
+  const int s_w1 = nc, s_k2 = nc * nw, s_q = nc * nw * nc * nw;  // < 2^31 for R <= 16, Nw <= 2048
+  const int per_tile = nc * nc * nq;
+
+  int it = 0;
+  if (t < 32 && blockIdx.x < n_tiles)
+    issue(blockIdx.x, 0);
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++it) {
+    const int st = it & 1;
+    // The next tile's copies into the other stage (released by the __syncthreads that ended the
+    // previous iteration).
+    if (t < 32 && tile + gridDim.x < n_tiles) {
+      if (t == 0)
+        fenceProxyAsync();
+      __syncwarp();
+      issue(tile + gridDim.x, st ^ 1);
+    }
+    int w1, w2, iwq;
+    tileOf(tile, w1, w2, iwq);
+    const long base = long(w1) * s_w1 + w2 * s_w2 + iwq * s_wq;
+    const bool ok = mbarWait(&bar[st], (it >> 1) & 1, err);
+    if (!__syncthreads_and(ok)) {
+      // Give up; the copies of the other stage (if issued) land before the CTA exits.
+      if (t == 0 && tile + gridDim.x < n_tiles)
+        mbarWait(&bar[st ^ 1], ((it + 1) >> 1) & 1, err);
+      __syncthreads();
+      return;
+    }
+    const GT* S = stage + static_cast<long>(st) * stage_elems;
+    const GT *A0 = S, *B0 = S + blkA, *C0 = B0 + blk, *E0 = C0 + blk;
+    const GT *A1 = S + blkA + 3 * blk, *B1 = A1 + blkA, *C1 = B1 + blk, *E1 = C1 + blk;
+    auto ld = [](const GT* p) { return mk(static_cast<AT>(p->x), static_cast<AT>(p->y)); };
+    for (int c = 0; c < n_ch; ++c) {
+      const bool mag = (mag_bits >> c) & 1;
+      double2* g4 = G4[c] + base;
+      for (int e0 = t; e0 < per_tile; e0 += kRound * blockDim.x) {
+        double2 old[kRound];
+#pragma unroll
+        for (int r = 0; r < kRound; ++r) {
+          const int e = e0 + r * blockDim.x;
+          if (!atomic && e < per_tile) {
+            const int k1 = e % nc, k2 = (e / nc) % nc, iq = e / (nc * nc);
+            old[r] = g4[k1 + k2 * s_k2 + iq * s_q];
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < kRound; ++r) {
+          const int e = e0 + r * blockDim.x;
+          if (e >= per_tile)
+            break;
+          const int k1 = e % nc, k2 = (e / nc) % nc, iq = e / (nc * nc), q = qtab[iq];
+          const int kq1 = kadd[k1 + nc * q], kq2 = kadd[k2 + nc * q];
+          C d = cmul(ld(A0 + k1 * RP + k2), ld(B0 + kq2 * R + kq1));
+          cfma(d, ld(A1 + k1 * RP + k2), ld(B1 + kq2 * R + kq1));
+          const C u0 = ld(C0 + k1 * R + kq1), u1 = ld(C1 + k1 * R + kq1);
+          const C v0 = ld(E0 + kq2 * R + k2), v1 = ld(E1 + kq2 * R + k2);
+          const C u = mag ? csub(u0, u1) : cadd(u0, u1), v = mag ? csub(v0, v1) : cadd(v0, v1);
+          const C val = cscale(csub(cmul(u, v), d), hs);
+          double2* p = g4 + (k1 + k2 * s_k2 + iq * s_q);
+          if (atomic) {
+            atomicAdd(&p->x, static_cast<double>(val.x));
+            atomicAdd(&p->y, static_cast<double>(val.y));
+          }
+          else {
+            *p = make_double2(old[r].x + static_cast<double>(val.x), old[r].y + static_cast<double>(val.y));
+          }
+        }
+      }
+    }
+    __syncthreads();  // stage st is free for the tile after next
+  }
+}
+
 }  // namespace
 
 template <typename GT>
@@ -659,12 +810,34 @@ static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_strid
   return true;
 }
 
+// The streaming single-measurement kernel: one band, PH channels, R <= 16 (two stages of eight
+// blocks in shared memory).
+template <typename GT>
+static bool launchSinglebandStream(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
+  const TpDims& d = a.dims;
+  if (a.n_slots != 1 || !singlebandPHApplies<GT>(d) || d.R > 16 || a.n_sm <= 0)
+    return false;
+  using AT = std::conditional_t<std::is_same_v<GT, double2>, double, float>;
+  const size_t tables = ((sizeof(int) * (d.nc * d.nc + d.nq) + 15) / 16) * 16;
+  const size_t smem = 16 + tables + 2 * sizeof(GT) * 2 * (size_t(d.R) * (d.R + 1) + 3 * size_t(d.R) * d.R);
+  auto k = updateG4SinglebandStream<GT, AT>;
+  DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const long tiles = long(d.nw) * d.nw * d.nwq;
+  const int grid = int(std::max(1L, std::min<long>(tiles, 3L * a.n_sm)));
+  k<<<grid, 256, smem, stream>>>(d, G, g_sector_stride, a.signs, a.k_add, a.q_list, a.wex_list, a.G4, a.atomic,
+                                 a.err);
+  DCAACC_LAUNCH_CHECK();
+  return true;
+}
+
 template <typename GT>
 int launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
   if constexpr (std::is_same_v<GT, float2>) {
     if (const int n = launchUpdateG4SinglebandBatched(a, G, g_sector_stride, stream))
       return n;
   }
+  if (launchSinglebandStream<GT>(a, G, g_sector_stride, stream))
+    return 1;
   if (singlebandPHApplies<GT>(a.dims)) {
     bool done;
     if constexpr (std::is_same_v<GT, double2>)

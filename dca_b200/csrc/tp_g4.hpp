@@ -29,6 +29,11 @@ struct G4Args {
   int n_sm = 0;               // multiprocessors (persistent grids)
   const unsigned* tile_order = nullptr;  // half_g4: the (w1 | w2 << 16) tiles to update, mirror pairs adjacent
   LaunchTuner* tuner = nullptr;          // launch-shape tuner (null: the built-in shapes)
+  // Error-path tests: polls of a bounded device wait before it gives up (0: the built-in limit),
+  // and the pipeline step before which the tensor-core direct term's first CTA stops feeding its
+  // consumers (-1: never).
+  uint32_t wait_limit = 0;
+  int fault_stop_step = -1;
 };
 
 // Workspace of the tensor-core disconnected-term GEMM (tp_g4_disc.cu): U / V operand planes, their

@@ -169,7 +169,7 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
                   const int* __restrict__ q_list, const int* __restrict__ wex_list,
                   const int* __restrict__ gmax, const unsigned* __restrict__ tile_order,
                   const float2* __restrict__ disc, double2* const* __restrict__ G4, bool atomic,
-                  int* __restrict__ err) {
+                  int* __restrict__ err, uint32_t wait_limit, int fault_stop_step) {
   extern __shared__ __align__(16) unsigned char smem[];
   float2* table = reinterpret_cast<float2*>(smem + kOffTable);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOffBars);
@@ -244,7 +244,13 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
                              : (static_cast<long>(w2x) * nw_ext + w1x) * kBlk;
       for (int step = 0; step < n_steps; ++step, ++gs) {
         const int st = gs % kStages, use = gs / kStages;
-        if (use > 0 && !__all_sync(0xffffffffu, mbarWait(&empty[st], (use - 1) & 1, err))) {
+        // Injected failure (tests of the error path): CTA 0's producer stops before step gs, as if
+        // its copies never came, so the consumers' bounded wait for that stage runs out.
+        if (blockIdx.x == 0 && gs == fault_stop_step) {
+          ok = false;
+          break;
+        }
+        if (use > 0 && !__all_sync(0xffffffffu, mbarWait(&empty[st], (use - 1) & 1, err, wait_limit))) {
           ok = false;
           break;
         }
@@ -354,7 +360,7 @@ updateG4DirectMma(const TpDims dims, const float2* __restrict__ G, long g_sector
         }
       }
       if (ok)
-        ok = __all_sync(0xffffffffu, mbarWait(&full[st], (gs / kStages) & 1, err));
+        ok = __all_sync(0xffffffffu, mbarWait(&full[st], (gs / kStages) & 1, err, wait_limit));
       if (ok) {
         const int e = step_exp[step];
         const float sc = pow2(e), inv = pow2(-2 * e);
@@ -476,7 +482,8 @@ void launchDirectTc(const G4Args& a, const float2* G, long g_sector_stride, cons
   const unsigned grid = static_cast<unsigned>(std::max(1L, std::min<long>(tiles, n_sm)));
   updateG4DirectMma<<<grid, kThreads, kSmem, stream>>>(d, G, g_sector_stride, a.signs, a.n_slots, a.k_sub,
                                                        a.q_list, a.wex_list, a.gmax, a.tile_order, disc, a.G4,
-                                                       a.atomic, a.err);
+                                                       a.atomic, a.err, a.wait_limit ? a.wait_limit : kWaitLimit,
+                                                       a.fault_stop_step);
   DCAACC_LAUNCH_CHECK();
 }
 

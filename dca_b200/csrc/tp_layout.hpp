@@ -62,6 +62,12 @@ struct SectorDesc {
   int orb_off;      // offset of this sector in the packed orbital-start arrays ((n_orb + 1) each)
   int spin;         // 0 or 1
   int slot;         // measurement slot inside the batch
+  int m_f32;        // 1: M holds float elements (the reference's SpScalar = float), else double
 };
+
+// Element (i, j) of a sector's M, read in its stored precision.
+__host__ __device__ inline double loadM(const SectorDesc& sd, long idx) {
+  return sd.m_f32 ? static_cast<double>(reinterpret_cast<const float*>(sd.M)[idx]) : sd.M[idx];
+}
 
 }  // namespace dcaacc

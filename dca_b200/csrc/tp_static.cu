@@ -128,6 +128,31 @@ void computeGNoAlloc(const dcaacc_tp_config& c, const double* G0_dev, const dcaa
   const int n_vtx = n[0] + n[1];
   const bool non_density = c.non_density != 0;
   const int R = n_orb;
+  TpDims d{};
+  d.nb = nb;
+  d.nc = nc;
+  d.nw = 2 * c.n_w_half;
+  d.ext = ext;
+  d.nw_ext = nw_ext;
+  d.n_orb = n_orb;
+  d.R = R;
+  d.beta = c.beta;
+  // The FP64 front-end keeps per-CTA tiles of the cluster transform in shared memory; their size
+  // grows with nb * Nc (for one band it passes 227 KB above Nc = 43).
+  if (frontendSmemRequirement(d, std::max(n[0], n[1]), true) > 227 * 1024)
+    throw Error(DCAACC_INVALID_ARG, "nb * Nc too large for the FP64 front-end's shared-memory tiles "
+                                    "(more than 227 KB per block)");
+  // Each call uploads its sorted vertex tables from stack memory: such copies cannot be recorded
+  // into a graph (a replay would read a dead stack frame), so a capturing stream is refused.
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t ce = cudaStreamIsCapturing(stream, &cs);
+    if (ce == cudaErrorStreamCaptureImplicit || (ce == cudaSuccess && cs != cudaStreamCaptureStatusNone)) {
+      cudaGetLastError();
+      throw Error(DCAACC_INVALID_ARG, "the allocation-free entry point cannot be called during stream capture");
+    }
+    DCAACC_CUDA_CHECK(ce);
+  }
 
   // ---- carve the static scratch ----
   size_t off = 0;
@@ -215,15 +240,6 @@ void computeGNoAlloc(const dcaacc_tp_config& c, const double* G0_dev, const dcaa
                                        reinterpret_cast<double2*>(base + o_fb), nb, nc);
   DCAACC_LAUNCH_CHECK();
 
-  TpDims d{};
-  d.nb = nb;
-  d.nc = nc;
-  d.nw = 2 * c.n_w_half;
-  d.ext = ext;
-  d.nw_ext = nw_ext;
-  d.n_orb = n_orb;
-  d.R = R;
-  d.beta = c.beta;
   FrontendArgs fa{};
   fa.dims = d;
   fa.sectors = reinterpret_cast<const SectorDesc*>(base + o_sec);

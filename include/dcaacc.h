@@ -121,12 +121,16 @@ int dcaacc_tp_reset(dcaacc_tp* acc);
  * tp_accumulator_gpu.hpp:493-497), updated atomically when there are several
  * (tp_accumulator_kernels.cu:677-680), zeroed once per DCA loop (callOncePerLoop,
  * tp_accumulator_gpu.hpp:271-296), and sumTo has nothing to add for it (:487-491).  Here each handle
- * owns its G4 unless share_g4 makes acc accumulate into owner's (same G4 shape and device; acc's
- * own is released; both switch to atomic updates).  reset_loop is resetAccumulation(dca_loop): a
- * shared G4 is zeroed only by the first handle that resets for a given dca_loop (synchronously),
- * a private one on every call.  sum_to between handles sharing G4 moves only the sign sums and
- * orders the target's later reads (finalize, peek) after the source's updates; without it, a
- * handle's reads of a shared G4 see another handle's updates once that handle has synchronized. */
+ * owns its G4 unless share_g4 makes acc accumulate into owner's (same G4 shape, transfer lists,
+ * channels, beta, mirror mode and device, else DCAACC_INVALID_ARG; what acc has accumulated so
+ * far is added into owner's G4 and acc's own is released; both switch to atomic updates).
+ * reset_loop is resetAccumulation(dca_loop): a shared G4 is zeroed only by the first handle that
+ * resets for a given dca_loop, after the updates already launched on every sharing handle's
+ * stream and before any later one (measurements a handle has queued but not launched, see flush,
+ * count toward the new loop); a private G4 is zeroed on every call.  sum_to between handles
+ * sharing G4 moves only the sign sums and orders the target's later reads (finalize, peek) after
+ * the source's updates; without it, a handle's reads of a shared G4 see another handle's updates
+ * once that handle has synchronized. */
 int dcaacc_tp_share_g4(dcaacc_tp* acc, dcaacc_tp* owner);
 int dcaacc_tp_reset_loop(dcaacc_tp* acc, int32_t dca_loop);
 
@@ -135,6 +139,16 @@ int dcaacc_tp_reset_loop(dcaacc_tp* acc, int32_t dca_loop);
  * reference's flop estimate for the call.  In FP64 mode the measurement is processed
  * immediately; in mixed mode it is queued and processed with its batch (see flush). */
 int dcaacc_tp_accumulate(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t sign, double* flops_out);
+
+/* accumulate for the reference's other instantiations, accumulate<Configuration, SpScalar, SignType>
+ * (tp_accumulator_gpu.hpp:118-125, 322-325): M of element type m_scalar (DCAACC_SCALAR_*) in both
+ * sectors, each M pointer read as that type, and the sign as (sign_re, sign_im) for a SignType that
+ * may be std::complex.  Real M in float or double with a real sign +1 / -1 is accumulated (float M
+ * is widened to double as it is read); complex M, which only complex-valued (e.g. spin-orbit)
+ * models produce, and a sign with a non-zero imaginary part return DCAACC_UNSUPPORTED. */
+enum { DCAACC_SCALAR_F64 = 0, DCAACC_SCALAR_F32 = 1, DCAACC_SCALAR_C128 = 2, DCAACC_SCALAR_C64 = 3 };
+int dcaacc_tp_accumulate_typed(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t m_scalar, double sign_re,
+                               double sign_im, double* flops_out);
 
 /* Batched form: n_meas measurements, sectors [2 * n_meas], signs [n_meas]. */
 int dcaacc_tp_accumulate_batch(dcaacc_tp* acc, int32_t n_meas, const dcaacc_sector* sectors,
@@ -155,7 +169,10 @@ int dcaacc_tp_get_g4(const dcaacc_tp* acc, int32_t channel, double* out, size_t 
 size_t dcaacc_tp_g4_size(const dcaacc_tp* acc);
 
 /* sumTo(other) — the CPU accumulator adds its G4 into other's and clears its own
- * (tp_accumulator_cpu.hpp:896-904).  Here: other.G4 += this.G4 on the device, this.G4 = 0. */
+ * (tp_accumulator_cpu.hpp:896-904).  Here: other.G4 += this.G4 on the device, this.G4 = 0.  Both
+ * handles must accumulate the same G4 (sizes, transfer lists, channels, beta), else
+ * DCAACC_INVALID_ARG; their precisions and mirror modes may differ (a half-G4 source is completed
+ * from its mirror before it is added into a full-G4 target). */
 int dcaacc_tp_sum_to(dcaacc_tp* acc, dcaacc_tp* other);
 
 /* Debug / parity: copies the last measurement's G for one spin (complex, layout
@@ -256,14 +273,35 @@ int dcaacc_tp_peek_g4_async(dcaacc_tp* acc, int32_t channel, size_t offset, size
  *             index b + nb k) at ((w_r NwExt + w_c) R^2); entry (r, c) of block (w_r, w_c) is the
  *             reference's G_(b_r, b_c, s, k_r, k_c, w_r, w_c)
  *   stream    cudaStream_t (as void*), may be null
- * Limits: n <= 512 per spin sector, nb Nc <= 64, and all scratch (about 16 R NwExt (n_0 + n_1)
- * bytes plus small tables) within 48 MiB; larger problems return DCAACC_INVALID_ARG.
+ * Limits: n <= 512 per spin sector, nb Nc <= 64 with the FP64 front-end's shared-memory tiles
+ * within 227 KB per block (for one band: Nc <= 43), and all scratch (about 16 R NwExt (n_0 + n_1)
+ * bytes plus small tables) within 48 MiB; larger problems return DCAACC_INVALID_ARG before any
+ * GPU work is enqueued.
  * The scratch's device address is looked up on the first call made on each device (with that
- * device current); make that first call before any stream capture.  All calls share the one
- * scratch array: calls whose GPU work overlaps (different streams, or host threads without
- * ordering) race on it.  Work is enqueued on the stream; synchronise it before reading G_out. */
+ * device current).  Each call uploads its sorted vertex tables from host stack memory, so it must
+ * not be called while its stream is being captured into a CUDA graph; such a call returns
+ * DCAACC_INVALID_ARG.  All calls share the one scratch array: calls whose GPU work overlaps
+ * (different streams, or host threads without ordering) race on it.  Work is enqueued on the
+ * stream; synchronise it before reading G_out. */
 int dcaacc_tp_compute_g_noalloc(const dcaacc_tp_config* cfg, const double* G0,
                                 const dcaacc_sector* sectors, double* G_out, void* stream);
+
+/* Error-path testing (no reference counterpart; the reference has no device-side failure
+ * detection on this path).  Every device wait of the library's kernels is bounded and, when it
+ * runs out, sets an error word that the next synchronize / finalize turns into
+ * DCAACC_DEVICE_INDEX_ERR while the CUDA context stays usable.
+ *
+ * set_fault_injection: from the handle's next batch on, the mixed path's tensor-core direct G4
+ * term (one band, Nc = 16, all momentum transfers) stops feeding its consumers in its first
+ * thread block before pipeline step stop_step (-1: never), and the bounded waits give up after
+ * wait_polls polls of up to 2 microseconds each (0: the built-in limit of 2^20 polls).  Drops the
+ * handle's CUDA graphs.  G4 is then incomplete: resetAccumulation before measuring again.
+ *
+ * set_allocation_failure: process-wide; the nth device or pinned-host buffer allocation from now
+ * on fails as if memory were exhausted (0 turns it off).  A create call that meets it returns
+ * DCAACC_OOM and leaves nothing allocated. */
+int dcaacc_tp_set_fault_injection(dcaacc_tp* acc, int32_t stop_step, uint32_t wait_polls);
+int dcaacc_set_allocation_failure(int64_t nth);
 
 /* ---------------------------------------------------------------------------------------------
  * Single-particle accumulator (delayed NFFT): SpAccumulator / Dnfft1DGpu.

@@ -25,11 +25,14 @@
 // Parity is pinned against the reference's own CPU accumulators built by oracle/refbuild.
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -42,6 +45,31 @@ namespace oracle {
 using cd = std::complex<double>;
 
 static thread_local std::string g_error;
+
+// Runs body(i) for i in [0, n) on a few host threads (ORACLE_THREADS, else the hardware's count).
+// Callers split only loops whose iterations write disjoint outputs, so every output is the same
+// sum in the same order as in a single-threaded run.
+template <class F>
+void parallelFor(int n, F&& body) {
+  int threads = static_cast<int>(std::thread::hardware_concurrency());
+  if (const char* e = std::getenv("ORACLE_THREADS"))
+    threads = std::atoi(e);
+  threads = std::max(1, std::min(threads, n));
+  if (threads == 1) {
+    for (int i = 0; i < n; ++i)
+      body(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t)
+    pool.emplace_back([&] {
+      for (int i = next++; i < n; i = next++)
+        body(i);
+    });
+  for (auto& th : pool)
+    th.join();
+}
 
 // ------------------------------------------------------------------------------------------------
 // Two-particle accumulator
@@ -190,13 +218,15 @@ private:
       }
     auto Mval = [&](int i, int j) { return sec.M[i + std::size_t(sec.ldm) * j]; };
 
-    std::vector<cd> X;
-    for (int oj = 0; oj < n_orb; ++oj) {
-      const int j0 = cols.second[oj], j1 = cols.second[oj + 1];
-      for (int oi = 0; oi < n_orb; ++oi) {
+    // Threads split the output blocks (orbital pairs); every entry keeps its own summation order.
+    parallelFor(n_orb * n_orb, [&](int pair) {
+      const int oj = pair / n_orb, oi = pair % n_orb;
+      {
+        const int j0 = cols.second[oj], j1 = cols.second[oj + 1];
+        std::vector<cd> X;
         const int i0 = rows.second[oi], i1 = rows.second[oi + 1];
         if (i1 == i0 || j1 == j0)
-          continue;  // setToZero: out is already zero
+          return;  // setToZero: out is already zero
         // X = T_l * M_ij   (NwExt x n_j)
         X.assign(std::size_t(nw_ext) * (j1 - j0), cd(0));
         for (int jj = j0; jj < j1; ++jj)
@@ -218,17 +248,18 @@ private:
             out[midx(r1, r2, b1, b2, w1, w2)] = acc;
           }
       }
-    }
+    });
   }
 
   // SpaceTransform2D::execute (space_transform_2D.hpp:60-91): in place, from the
   // (r1,r2,b1,b2,w1,w2) layout to (b1,b2,k1,k2,w1,w2).
   void spaceTransform(std::vector<cd>& f) {
     std::vector<cd> out(g_size);
-    std::vector<cd> tmp(nc * nc), frr(nc * nc);
     const double norm = 1.0 / nc;
-    for (int w2 = 0; w2 < nw_ext; ++w2)
-      for (int w1 = 0; w1 < nw_ext; ++w1)
+    parallelFor(nw_ext * nw_ext, [&](int ww) {
+      const int w2 = ww / nw_ext, w1 = ww % nw_ext;
+      {
+        std::vector<cd> tmp(nc * nc), frr(nc * nc);
         for (int b2 = 0; b2 < nb; ++b2)
           for (int b1 = 0; b1 < nb; ++b1) {
             for (int r2 = 0; r2 < nc; ++r2)
@@ -252,6 +283,8 @@ private:
                     norm * acc * phase[b1 + nb * k1] * std::conj(phase[b2 + nb * k2]);
               }
           }
+      }
+    });
     f.swap(out);
   }
 
@@ -259,11 +292,11 @@ private:
   // G <- -G0(k1,w1) G G0(k2,w2) + beta G0(k1,w1) delta_{k1 k2} delta_{w1 w2}.
   void computeG(int s) {
     auto& g = G[s];
-    std::vector<cd> blk(nb * nb), g0m(nb * nb);
-    for (int w2 = 0; w2 < nw_ext; ++w2)
+    parallelFor(nw_ext, [&](int w2) {
       for (int w1 = 0; w1 < nw_ext; ++w1)
         for (int k2 = 0; k2 < nc; ++k2)
           for (int k1 = 0; k1 < nc; ++k1) {
+            cd blk[64], g0m[64];
             const cd* g01 = &G0[g0idx(0, 0, s, k1, w1)];
             const cd* g02 = &G0[g0idx(0, 0, s, k2, w2)];
             cd* m = &g[gidx(0, 0, k1, k2, w1, w2)];
@@ -293,8 +326,9 @@ private:
               for (int b2 = 0; b2 < nb; ++b2)
                 for (int b1 = 0; b1 < nb; ++b1)
                   blk[b1 + nb * b2] += g01[b1 + nb * b2] * beta;
-            std::copy(blk.begin(), blk.end(), m);
+            std::copy(blk, blk + nb * nb, m);
           }
+    });
   }
 
   // getGMultiband (tp_accumulator_cpu.hpp:389-405): G_a(b1, b2) = G_(b2, b1, s, k1, k2, w1e, w2e)
@@ -311,11 +345,14 @@ private:
     auto add = [&](int k, int q) { return k_add[k + nc * q]; };
     auto q_minus_k = [&](int k, int q) { return k_sub[k + nc * q]; };  // index of q - k
     const int nq = k_ex.size(), nwq = w_ex.size();
-    for (int iwq = 0; iwq < nwq; ++iwq) {
-      const int wex = w_ex[iwq];
-      for (int iq = 0; iq < nq; ++iq) {
+    if (channel < DCAACC_PH_TRANSVERSE || channel > DCAACC_PP_UP_DOWN)
+      throw std::logic_error("Specified four point type not implemented.");
+    // Threads split (transfer, w2); every G4 entry is written by one thread in the same order.
+    parallelFor(nwq * nq * nw, [&](int job) {
+      const int w2 = job % nw, iq = (job / nw) % nq, iwq = job / (nw * nq);
+      {
+        const int wex = w_ex[iwq];
         const int q = k_ex[iq];
-        for (int w2 = 0; w2 < nw; ++w2)
           for (int k2 = 0; k2 < nc; ++k2)
             for (int w1 = 0; w1 < nw; ++w1)
               for (int k1 = 0; k1 < nc; ++k1) {
@@ -395,12 +432,12 @@ private:
                                   Gm(!s, q_minus_k(k1, q), q_minus_k(k2, q), wm1, wm2, b2, b4);
                     break;
                   }
-                  default:
-                    throw std::logic_error("Specified four point type not implemented.");
+                  default:  // rejected before the loops
+                    break;
                 }
               }
       }
-    }
+    });
   }
 };
 

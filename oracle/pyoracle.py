@@ -10,6 +10,8 @@ from __future__ import annotations
 
 import ctypes
 import os
+import sys
+import time
 import subprocess
 from ctypes import POINTER, c_double, c_int32, c_void_p
 
@@ -201,8 +203,14 @@ class OracleSp:
         return out
 
 
-def run_case(case_path, out_path, tp=True, sp=True):
+def run_case(case_path, out_path, tp=True, sp=True, warmup=0, report=False):
+    """Runs the restatement on a case file.  report: prints the wall-clock window of the whole run
+    on stderr in tp_ref's --time format (warm-up measurements are inside it: the restatement has
+    no per-measurement timer)."""
+    t0 = time.time()
     _check(lib().oracle_run_case(str(case_path).encode(), str(out_path).encode(), int(tp), int(sp)))
+    if report:
+        print(f"tp_epoch_start={t0!r} tp_epoch_end={time.time()!r} blas=none", file=sys.stderr)
 
 
 def run_reference(case_path, out_path, tp=True, sp=True, timeout=3600):

@@ -16,6 +16,7 @@
 //   measurements after the first W.
 #include <array>
 #include <chrono>
+#include <iomanip>
 #include <cstdlib>
 #include <complex>
 #include <cstdint>
@@ -223,6 +224,16 @@ public:
 }  // namespace phys
 }  // namespace dca
 
+#ifndef DCA_REF_BLAS_NAME
+#define DCA_REF_BLAS_NAME "naive-zgemm"
+#endif
+constexpr const char* kBlasName = DCA_REF_BLAS_NAME;
+
+// Wall-clock seconds since the epoch: comparable across the processes of a parallel timing run.
+inline double epochSeconds() {
+  return std::chrono::duration<double>(std::chrono::system_clock::now().time_since_epoch()).count();
+}
+
 namespace harness {
 
 template <int NB>
@@ -277,7 +288,7 @@ int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool d
                                 sec.right_site[i]};
     }
 
-  double tp_seconds = 0, sp_seconds = 0;
+  double tp_seconds = 0, sp_seconds = 0, tp_epoch_start = 0, tp_epoch_end = 0;
   if (do_tp) {
     func::function<std::complex<double>, func::dmn_variadic<NuDmn, NuDmn, KDmn, WDmn>> G0("G0");
     if (G0.size() != c.G0.size())
@@ -288,12 +299,16 @@ int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool d
     phys::solver::accumulator::TpAccumulator<P, DistType::NONE, linalg::CPU> acc(G0, pars);
     acc.resetAccumulation();
     auto t0 = std::chrono::steady_clock::now();
+    tp_epoch_start = epochSeconds();
     for (int m = 0; m < n_meas; ++m) {
-      if (m == warmup)
+      if (m == warmup) {
         t0 = std::chrono::steady_clock::now();
+        tp_epoch_start = epochSeconds();
+      }
       acc.accumulate(Ms[m], confs[m], static_cast<std::int8_t>(c.meas[m].sign));
     }
     tp_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    tp_epoch_end = epochSeconds();
     for (const auto& g4 : acc.get_G4()) {
       res.G4.emplace_back(g4.size());
       for (std::size_t i = 0; i < g4.size(); ++i)
@@ -329,8 +344,9 @@ int run(const casefile::Case& c, const std::string& out_path, bool do_tp, bool d
 
   casefile::writeResult(out_path, res);
   if (timing)
-    std::cerr << "tp_seconds=" << tp_seconds << " sp_seconds=" << sp_seconds
-              << " n_meas=" << n_meas << "\n";
+    std::cerr << std::setprecision(17) << "tp_seconds=" << tp_seconds << " sp_seconds=" << sp_seconds
+              << " n_meas=" << n_meas << " tp_epoch_start=" << tp_epoch_start << " tp_epoch_end=" << tp_epoch_end
+              << " blas=" << kBlasName << "\n";
   return 0;
 }
 

@@ -79,10 +79,28 @@ def test_bench_reference_arm_prints_one_contract_line():
                            "d2h_bytes_per_step": 0}
 
 
-def test_integration_notes_cover_every_entry_point():
-    """Every entry point the header declares has its row (reference counterpart or none) in the
-    integration notes."""
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    doc = open(os.path.join(root, "INTEGRATION.md")).read()
-    missing = [s for s in declared_symbols() if s not in doc]
-    assert not missing, missing
+# The C ABI's entry points.  A change to the header must be made here too (and in the Python
+# binding), so that an entry point cannot appear or disappear unnoticed.
+ENTRY_POINTS = """
+dcaacc_last_error dcaacc_set_allocation_failure
+dcaacc_tp_create dcaacc_tp_destroy dcaacc_tp_reset dcaacc_tp_reset_loop dcaacc_tp_share_g4
+dcaacc_tp_accumulate dcaacc_tp_accumulate_typed dcaacc_tp_accumulate_batch dcaacc_tp_flush dcaacc_tp_finalize
+dcaacc_tp_get_g4 dcaacc_tp_g4_size dcaacc_tp_sum_to dcaacc_tp_get_g dcaacc_tp_set_stream
+dcaacc_tp_get_stream dcaacc_tp_synchronize dcaacc_tp_device_fingerprint dcaacc_tp_kernel_launches
+dcaacc_tp_sign_sum dcaacc_tp_get_g4_normalized dcaacc_tp_static_device_fingerprint
+dcaacc_tp_mirror_mode dcaacc_tp_enable_timing dcaacc_tp_stage_times dcaacc_tp_set_graphs
+dcaacc_tp_graph_stats dcaacc_tp_tuning_settled dcaacc_tp_tuning_report dcaacc_tp_peek_g4
+dcaacc_tp_peek_g4_async dcaacc_tp_compute_g_noalloc dcaacc_tp_set_fault_injection
+dcaacc_sp_create dcaacc_sp_destroy dcaacc_sp_reset dcaacc_sp_accumulate dcaacc_sp_finalize
+dcaacc_sp_get_m_r_w dcaacc_sp_get_m_r_w_sqr dcaacc_sp_sum_to dcaacc_sp_get_single_measurement_m_r_w
+dcaacc_sp_get_single_measurement_f_tau dcaacc_sp_clear_single_measurement dcaacc_sp_f_tau_size
+dcaacc_sp_set_stream dcaacc_sp_synchronize dcaacc_sp_device_fingerprint dcaacc_sp_kernel_launches
+""".split()
+
+
+def test_header_declares_exactly_the_known_entry_points():
+    """The header's declarations are the list above, and the Python binding types each of them."""
+    from dca_b200 import _native
+    assert sorted(ENTRY_POINTS) == declared_symbols()
+    for s in ENTRY_POINTS:
+        assert getattr(_native.lib, s).argtypes is not None, s

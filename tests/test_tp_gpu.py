@@ -446,3 +446,127 @@ def test_lifecycle_and_errors():
     acc.finalize()
     assert rel_err(acc.get_G4()[0], one) <= 1e-15
     assert acc.kernel_launches() > 0 and acc.deviceFingerprint() > 0
+
+
+def test_sum_to_across_mirror_modes(monkeypatch):
+    """sumTo between handles whose mirror modes differ: a half-G4 mixed handle (c3-like) adds into
+    a full-G4 mixed handle (DCAACC_TP_FULL_G=1) and into an FP64 handle (its lower half is filled
+    from the mirror first), and a full handle adds into a half one; each sum equals one FP64 handle
+    fed every measurement.  Handles of different transfer lists or channels are refused."""
+    import dataclasses
+
+    from dca_b200.accumulators import LogicError, TpAccumulator
+    case = case_from_workload(_small("c3", n_range=(40, 80)), 6)
+    ms = case.measurements
+
+    def make(precision, full=False, **kw):
+        monkeypatch.setenv("DCAACC_TP_FULL_G", "1" if full else "0")
+        acc = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=4, **kw))
+        acc.resetAccumulation(0)
+        return acc
+
+    def feed(acc, sub):
+        for m in sub:
+            acc.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+        return acc
+
+    whole = feed(make(0), ms)
+    whole.finalize()
+    pairs = [(feed(make(1), ms[:3]), feed(make(1, full=True), ms[3:])),   # half -> full
+             (feed(make(1), ms[:3]), feed(make(0), ms[3:])),              # half -> FP64
+             (feed(make(1, full=True), ms[:3]), feed(make(1), ms[3:]))]   # full -> half
+    assert pairs[0][0].mirror_mode() == 3 and pairs[0][1].mirror_mode() == 0
+    for src, dst in pairs:
+        src.sumTo(dst)
+        dst.finalize()
+        for got, want in zip(dst.get_G4(), whole.get_G4()):
+            print("sumTo across mirror modes:", src.mirror_mode(), "->", dst.mirror_mode(), rel_err(got, want))
+            assert rel_err(got, want) <= MIXED_TOL
+    other_q = make(1, k_ex=[0])
+    with pytest.raises(LogicError):
+        make(1).sumTo(other_q)
+    with pytest.raises(LogicError):
+        make(1).share_G4_with(make(1, channels=[2]))
+    with pytest.raises(LogicError):  # different mirror modes cannot share one G4
+        make(1).share_G4_with(make(1, full=True))
+
+
+def test_share_g4_keeps_what_was_accumulated_before():
+    """A handle that has accumulated on its own and then starts sharing another handle's G4 adds
+    what it has into the shared one: nothing is dropped, and the sum equals one handle fed every
+    measurement."""
+    from dca_b200.accumulators import TpAccumulator
+    case = case_from_workload(_small("c3", n_range=(30, 60)), 6)
+    ms = case.measurements
+    single = run_gpu(case, precision=0, max_batch=1)
+    a = TpAccumulator(case.G0, case.tp_params(precision=0, max_batch=1))
+    b = TpAccumulator(case.G0, case.tp_params(precision=0, max_batch=1))
+    a.resetAccumulation(3)
+    b.resetAccumulation(3)
+    for m in ms[:2]:
+        b.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    a.accumulate([s.M for s in ms[2].sectors], list(ms[2].sectors), ms[2].sign)
+    b.share_G4_with(a)
+    for i, m in enumerate(ms[3:]):
+        (a if i % 2 else b).accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    b.sumTo(a)
+    a.finalize()
+    assert a.sign_sum() == (float(sum(m.sign for m in ms)), 6)
+    for got, want in zip(a.get_G4(), single.get_G4()):
+        assert rel_err(got, want) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_non_density_vertices_match_oracle(oracle_lib, precision):
+    """Vertices whose left and right band / site differ (non-density-density interactions): the rows
+    of M are ordered by the right orbital and the columns by the left one
+    (cached_ndft_base.hpp:97-103), both sorted on the device.  Three bands on the Betts 8 cluster,
+    all four channels, against the oracle."""
+    w = _small("c4", nw_half=4, n_sp=64, n_range=(20, 40), freq_transfer=1, channels=(1, 2, 3, 4))
+    case = case_from_workload(w, 3)
+    rng = np.random.default_rng(5)
+    for m in case.measurements:
+        for s in m.sectors:
+            s.left_band = rng.integers(0, w.nb, s.n).astype(np.int32)
+            s.left_site = rng.integers(0, case.nc, s.n).astype(np.int32)
+    acc = run_gpu(case, precision=precision, max_batch=2, non_density=True)
+    ora = run_oracle(oracle_lib, case, non_density=True)
+    tol = FP64_TOL if precision == 0 else MIXED_TOL
+    for got, want in zip(acc.get_G4(), ora.get_G4()):
+        print("non-density", precision, rel_err(got, want))
+        assert rel_err(got, want) <= tol
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_float_m_and_sign_types(precision):
+    """accumulate for the reference's other SpScalar / SignType instantiations: float M (host and
+    device) gives the G4 of the same M widened to double, a complex sign with zero imaginary part is
+    the real sign, and complex M or a complex sign are refused (DCAACC_UNSUPPORTED)."""
+    import torch
+    from dca_b200.accumulators import LogicError, TpAccumulator
+    case = case_from_workload(_small("c3", n_range=(40, 80)), 4)
+    ms = case.measurements
+    widened = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=2))
+    typed = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=2))
+    for acc in (widened, typed):
+        acc.resetAccumulation(0)
+    alive = []  # device M stays valid until the queued batch has run (synchronizeCopy)
+    for i, m in enumerate(ms):
+        m32 = [np.asfortranarray(s.M.astype(np.float32)) for s in m.sectors]
+        widened.accumulate([x.astype(np.float64) for x in m32], list(m.sectors), m.sign)
+        if i % 2:  # device float M
+            src = [torch.from_numpy(np.ascontiguousarray(x.T)).cuda().t() for x in m32]
+        else:
+            src = m32
+        alive.append(src)
+        typed.accumulate_typed(src, list(m.sectors), complex(m.sign, 0.0))
+    for acc in (widened, typed):
+        acc.finalize()
+    for a, b in zip(typed.get_G4(), widened.get_G4()):
+        assert rel_err(a, b) <= 1e-15
+    typed.resetAccumulation(1)
+    m = ms[0]
+    with pytest.raises(LogicError, match="UNSUPPORTED"):
+        typed.accumulate_typed([s.M.astype(np.complex128) for s in m.sectors], list(m.sectors), 1)
+    with pytest.raises(LogicError, match="UNSUPPORTED"):
+        typed.accumulate_typed([s.M for s in m.sectors], list(m.sectors), 1j)

@@ -107,3 +107,63 @@ def test_noalloc_rejects_oversized_problem():
     rc = N.lib.dcaacc_tp_compute_g_noalloc(ctypes.byref(cfg), ctypes.c_void_p(G0_dev.data_ptr()), secs,
                                            ctypes.c_void_p(out.data_ptr()), None)
     assert rc == 1 and b"512" in N.lib.dcaacc_last_error()
+
+
+def test_noalloc_rejects_cluster_beyond_shared_memory_tiles():
+    """nb * Nc = 64 (one band on an 8 x 8 cluster) is within the orbital limit but needs more than
+    227 KB of shared memory per block in the FP64 front-end: rejected before any GPU work."""
+    import dataclasses
+
+    import torch
+
+    from dca_b200 import _native as N
+    from dca_b200 import workloads as W
+    from dca_b200.accumulators import TpParameters, _make_sectors
+
+    w = dataclasses.replace(W.WORKLOADS["c1"], cluster_kind=("square", 8), n_range=(8, 8))
+    cl = w.cluster()
+    p = TpParameters.from_workload(w, cl)
+    keep = []
+    cfg = _config(p, keep)
+    m = W.make_measurements(w, 1)[0]
+    M_dev = [torch.from_numpy(np.ascontiguousarray(s.M.T)).cuda().t() for s in m.sectors]
+    secs = _make_sectors(M_dev, list(m.sectors), keep)
+    g0 = W.make_g0(w.model, cl, w.beta, w.chemical_potential(), w.n_sp).reshape(-1)
+    G0_dev = torch.from_numpy(g0.view(np.float64).copy()).cuda()
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc = N.lib.dcaacc_tp_compute_g_noalloc(ctypes.byref(cfg), ctypes.c_void_p(G0_dev.data_ptr()), secs,
+                                           ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 1 and b"shared-memory" in N.lib.dcaacc_last_error()
+    torch.cuda.synchronize()
+    assert not torch.any(out)
+
+
+def test_noalloc_refuses_stream_capture():
+    """A call on a stream that is being captured returns DCAACC_INVALID_ARG without enqueueing
+    anything (its uploads come from host stack memory, which a replayed graph could not read)."""
+    import torch
+
+    from dca_b200 import _native as N
+    from dca_b200.accumulators import _make_sectors
+
+    case, _ = golden("c1_mag")
+    p = case.tp_params()
+    keep = []
+    cfg = _config(p, keep)
+    m = case.measurements[0]
+    M_dev = [torch.from_numpy(np.ascontiguousarray(s.M.T)).cuda().t() for s in m.sectors]
+    secs = _make_sectors(M_dev, list(m.sectors), keep)
+    G0_dev = torch.from_numpy(case.G0.view(np.float64).copy()).cuda()
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        rc = N.lib.dcaacc_tp_compute_g_noalloc(ctypes.byref(cfg), ctypes.c_void_p(G0_dev.data_ptr()), secs,
+                                               ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s.cuda_stream))
+        out.add_(1.0)  # the capture stays valid: nothing of the refused call was recorded
+    assert rc == 1 and b"stream capture" in N.lib.dcaacc_last_error()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.all(out == 1.0)
