@@ -62,6 +62,14 @@ def parse_args():
     p.add_argument("--workload", default="c3")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison leg")
+    p.add_argument("--batch", type=int, default=None, help="measurements per step (default: the workload's)")
+    p.add_argument("--nw-half", type=int, default=None,
+                   help="positive four-point frequencies (default: the workload's; smaller only for profiling)")
+    p.add_argument("--n-range", type=int, nargs=2, default=None, metavar=("LO", "HI"),
+                   help="expansion orders per spin (default: the workload's)")
+    p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed",
+                   help="path timed as the main leg: the batched mixed path, or the plain FP64 path "
+                        "(one measurement at a time; a step is still one batch of measurements)")
     return p.parse_args()
 
 
@@ -180,6 +188,23 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
+
+
+def workload(args):
+    """The named workload with the command line's size overrides (if any) applied."""
+    import dataclasses
+
+    from dca_b200 import workloads as W
+    w = W.WORKLOADS[args.workload]
+    kw = {}
+    if args.batch:
+        kw["batch"] = args.batch
+    if args.nw_half:
+        kw["nw_half"] = args.nw_half
+        kw["n_sp"] = max(w.n_sp, args.nw_half + w.freq_transfer + 8)
+    if args.n_range:
+        kw["n_range"] = tuple(args.n_range)
+    return dataclasses.replace(w, **kw) if kw else w
 
 
 def dist_setup(n_gpus):
@@ -307,7 +332,7 @@ def run_ours(args, world, rank, local):
     from dca_b200.accumulators import TpAccumulator, TpParameters
 
     torch.cuda.set_device(local)
-    w = W.WORKLOADS[args.workload]
+    w = workload(args)
     cl = w.cluster()
     g0 = W.make_g0(w.model, cl, w.beta, w.chemical_potential(), w.n_sp)
     B = w.batch
@@ -336,7 +361,8 @@ def run_ours(args, world, rank, local):
                 off += n * n
             pinned.append(pair)
 
-    params = TpParameters.from_workload(w, cl, precision=1, max_batch=B)
+    fp64_main = args.precision == "fp64"
+    params = TpParameters.from_workload(w, cl, precision=0 if fp64_main else 1, max_batch=1 if fp64_main else B)
     acc = TpAccumulator(g0, params)
     acc.resetAccumulation(0)
     stream = torch.cuda.ExternalStream(acc.get_stream())
@@ -350,7 +376,8 @@ def run_ours(args, world, rank, local):
     # shape (each candidate timed three times on real batches) and until both device input sets
     # have their CUDA graph (captured after a batch of the shape ran without tuning probes).
     warmup = 0
-    while warmup < args.warmup or ((not acc.tuning_settled() or acc.graph_stats()[0] < 2) and warmup < 64):
+    while warmup < args.warmup or ((not acc.tuning_settled() or (acc.graph_stats()[0] < 2 and not fp64_main))
+                                   and warmup < 64):
         step(warmup, dev_M)
         warmup += 1
     torch.cuda.synchronize()
@@ -421,7 +448,7 @@ def run_ours(args, world, rank, local):
     fp64 = None
     fp64_stages = None
     err = None
-    if not args.no_fp64:
+    if not args.no_fp64 and not fp64_main:
         n_cmp = B
         ref_acc = TpAccumulator(g0, TpParameters.from_workload(w, cl, precision=0, max_batch=1))
         ref_acc.resetAccumulation(0)
@@ -476,15 +503,21 @@ def run_ours(args, world, rank, local):
         "row_transform": per_step * float(np.sum(8.0 * nwe * ns * ns + 8.0 * nc * D * D)),
         "col_transform": per_step * float(np.sum(8.0 * nwe * nwe * n_orb * ns + 8.0 * nc * D * D + epi * D * D)),
     }
-    g4_alg_bytes = len(w.channels) * n_g4 * 32 + B * 2 * D * D * 8
+    # (plain FP64 path: every measurement reads and writes all of G4 and reads its FP64 G)
+    g4_alg_bytes = (B * (len(w.channels) * n_g4 * 32 + 2 * D * D * 16) if fp64_main
+                    else len(w.channels) * n_g4 * 32 + B * 2 * D * D * 8)
     g4_sec = stages["update_g4"][0] / args.steps / 1e3  # the stage's time per batch
     g4_paths = {"direct_tc": "discPlanesKernel + frontGemmKernel<2> (disconnected terms) + updateG4DirectMma "
                              "(direct term, G4 flush)",
                 "split36": "discPlanesKernel + frontGemmKernel<2> (disconnected terms) + "
                            "updateG4SinglebandOuterSplit (direct term, G4 flush)",
                 "staged": "updateG4StagedKernel (all terms, G blocks staged in shared memory)",
-                "simt": "updateG4SinglebandBatched"}
-    if simt:
+                "simt": "updateG4SinglebandBatched",
+                "stream": "updateG4SinglebandStream (one measurement, G4 streamed in memory order)",
+                "fp64_other": "updateG4SinglebandPH / updateG4Kernel (one measurement)"}
+    if fp64_main:
+        g4_path = "stream" if nb == 1 and nc * nc <= 256 and set(w.channels) <= {2, 3} else "fp64_other"
+    elif simt:
         g4_path = "simt"
     elif nb > 1:
         g4_path = "staged"
@@ -495,7 +528,8 @@ def run_ours(args, world, rank, local):
     stage_kernels = {"update_g4": {"direct_tc": ["discPlanesKernel", "frontGemmKernel<2>", "updateG4DirectMma"],
                                    "split36": ["discPlanesKernel", "frontGemmKernel<2>",
                                                "updateG4SinglebandOuterSplit"],
-                                   "staged": ["updateG4StagedKernel"]}.get(g4_path, []),
+                                   "staged": ["updateG4StagedKernel"],
+                                   "stream": ["updateG4SinglebandStream"]}.get(g4_path, []),
                      "col_transform": ["frontGemmKernel<1>"], "row_transform": ["frontGemmKernel<0>"],
                      "twiddle": ["twiddleWiKernel", "buildMOperandKernel", "buildPhasePairKernel"]}
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of each stage's kernels per launch of
@@ -503,7 +537,7 @@ def run_ours(args, world, rank, local):
     traffic = {}
     try:
         with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
-            tk = json.load(f)["workloads"].get(w.name, {})
+            tk = json.load(f)["workloads"].get(w.name + ("-fp64" if fp64_main else ""), {})
         for st, ks in stage_kernels.items():
             if ks and not simt and all(k in tk for k in ks):
                 traffic[st] = sum(tk[k]["dram_read_bytes"] + tk[k]["dram_write_bytes"] for k in ks)
@@ -522,11 +556,14 @@ def run_ours(args, world, rank, local):
         g4_roof["dram_gbs"] = traffic["update_g4"] / g4_sec / 1e9
         g4_roof["dram_frac"] = g4_roof["dram_gbs"] / hbm_gbs
 
-    # Roofline of the dominant stage (its kernels' CUDA-event time per launch of the stage).
+    # Roofline of the dominant stage: its algorithmic work per step (one batch) over its kernels'
+    # CUDA-event time per step (the stage's launches: one per batch for the tensor-core GEMMs, one
+    # per measurement on the plain FP64 path).
     dom = max(stages, key=lambda k: stages[k][0])
     dom_ms, dom_launches = stages[dom]
-    per_launch_ms = dom_ms / max(dom_launches, 1)
+    per_launch_ms = dom_ms / args.steps
     sec = per_launch_ms / 1e3
+    tc_front = not simt and not fp64_main
     if dom == "update_g4":
         roof = {"kernel": "update_g4 stage: " + g4_roof["kernels"], "bound": "hbm",
                 "achieved": g4_alg_bytes / sec / 1e9, "peak": hbm_gbs, "unit": "GB/s",
@@ -534,7 +571,7 @@ def run_ours(args, world, rank, local):
         for k in ("dram_gbs", "dram_frac"):
             if k in g4_roof:
                 roof[k] = g4_roof[k]
-    elif dom in ("col_transform", "row_transform") and not simt:
+    elif dom in ("col_transform", "row_transform") and tc_front:
         # Tensor-core front-end: the survey's algorithmic flops against the measured dense BF16 peak.
         # Beside it, the work the kernel is built to do (the dense complex product over all vertices,
         # split FP16: three MMAs per complex multiply-add pair) and its issued MMA rate (128 x 128
@@ -558,14 +595,17 @@ def run_ours(args, world, rank, local):
                 "dense_form_flops": dense, "dense_form_tflops": dense / sec / 1e12,
                 "mma_issued_tflops": mma / sec / 1e12, "mma_frac_of_bf16_peak": mma / sec / 1e12 / bf16_tf}
     else:
-        # SIMT front-end stages are dominated by their global traffic (M / X' / G, FP32 complex).
+        # SIMT front-end stages are dominated by their global traffic (M / X' / G, complex of the
+        # path's precision).
         mean_n = float(np.mean(ns))
+        cs = 16 if fp64_main else 8
+        real = "double" if fp64_main else "float"
         if dom == "col_transform":
-            alg_bytes = 2 * B * (D * mean_n * 8 + D * D * 8)
-            kern = "colTransformKernel<float>"
+            alg_bytes = 2 * B * (D * mean_n * cs + D * D * cs)
+            kern = f"colTransformKernel<{real}>"
         elif dom == "row_transform":
-            alg_bytes = 2 * B * (mean_n * mean_n * 8 + D * mean_n * 8)
-            kern = "rowTransformKernel<float,8,8>"
+            alg_bytes = 2 * B * (mean_n * mean_n * 8 + D * mean_n * cs)
+            kern = f"rowTransformKernel<{real}>"
         else:
             alg_bytes = 2 * B * mean_n * nwe * 16
             kern = "twiddleKernel"
@@ -573,7 +613,8 @@ def run_ours(args, world, rank, local):
                 "peak": hbm_gbs, "unit": "GB/s"}
     roof["frac"] = roof["achieved"] / roof["peak"]
     roof["peak_source"] = peak_src + " (MEASURED_PEAKS.json)" if peak_src == "measured" else peak_src
-    roof["ms_per_launch"] = per_launch_ms
+    roof["ms_per_step"] = per_launch_ms
+    roof["launches_per_step"] = dom_launches / args.steps
     roof["traffic"] = traffic.get(dom)
     if roof["traffic"] is not None:
         roof["traffic_unit"] = "DRAM bytes per launch of the stage (ncu, profiles/dram_traffic.json)"
@@ -588,10 +629,12 @@ def run_ours(args, world, rank, local):
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (G, G4 partials) + fp64 (running G4)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp64" if fp64_main else "fp32 (G, G4 partials) + fp64 (running G4)",
         "data": "synthetic (seeded; dca_b200.workloads)",
         "config": {"workload": w.describe(),
-                   "measurements_per_step": B, "precision": "mixed", "parallelism": f"replicas x{world}",
+                   "measurements_per_step": B, "precision": args.precision,
+                   "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2 (G4 {len(w.channels) * n_g4 * 16 / 1e6:.0f} MB, "
                          f"G {B * 2 * D * D * 8 / 1e9:.1f} GB per batch)"},
         "e2e": e2e,
@@ -626,7 +669,7 @@ def run_reference_arm(args, world, rank):
     P processes.  The run is bounded to a few minutes: at most 2 warm-up and 6 timed steps, and
     the line reports the steps actually timed."""
     from dca_b200 import workloads as W
-    w = W.WORKLOADS[args.workload]
+    w = workload(args)
     if rank != 0:
         return None
     timed = max(1, min(args.steps, 6))

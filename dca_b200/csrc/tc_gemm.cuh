@@ -132,6 +132,8 @@ struct GemmParams {
   const int* eV;        // [problem][Dp] row exponents of V
   float2* disc;         // [problem][n][m] FP32 result
   int* gmax;            // column step: [2 slot + spin] largest |G| of the sector (float bits), or null
+  int order;            // persistent tile order within a sector: 0 the built-in one, 1 the two tile
+                        // indices swapped (chosen by the launch-shape tuner; results are identical)
 };
 
 // Column step, bands beyond those preloaded: adds beta G0_s(b1, b2; k2, w2) to v when column rho1
@@ -153,20 +155,22 @@ __device__ inline float2 addDeltaInPlace(const GemmParams& p, const SectorDesc& 
 // the tile has no work (row step: columns j beyond the sector's order).
 template <int MODE>
 __device__ inline void tileOf(const GemmParams& p, int t, int& sec, int& mt, int& nt, int& chunks) {
-  if (MODE == 0) {
-    // Row step: (sector, column tile, row tile), row tiles fastest.  The eight row tiles that
-    // share an M tile run at once, and the few column tiles of a sector, which re-read its P row
-    // tiles, follow each other closely enough for those reads to hit L2.  Tiles with j beyond a
-    // sector's order are skipped; a CTA's tiles (stride = grid) still visit every column tile.
-    const int per = p.mt * p.nt;
-    sec = t / per;
-    nt = (t % per) / p.mt;
-    mt = p.mt0 + t % p.mt;
+  // Within a sector the tiles go either row-tile fastest or column-tile fastest; which one reuses
+  // L2 better depends on the shape, so both are launch-shape tuner candidates (order 0 is the
+  // built-in one per mode).  Every output tile is computed the same way in either order.
+  const int per = p.mt * p.nt;
+  sec = t / per;
+  const int rem = t % per;
+  const bool rows_fastest = (MODE == 0) != (p.order != 0);
+  if (rows_fastest) {
+    // Row step default: (sector, column tile, row tile).  The eight row tiles that share an M tile
+    // run at once, and the few column tiles of a sector, which re-read its P row tiles, follow each
+    // other closely enough for those reads to hit L2.  Tiles with j beyond a sector's order are
+    // skipped; a CTA's tiles (stride = grid) still visit every column tile.
+    nt = p.nt0 + rem / p.mt;
+    mt = p.mt0 + rem % p.mt;
   }
   else {
-    const int per = p.mt * p.nt;
-    sec = t / per;
-    const int rem = t % per;
     mt = p.mt0 + rem / p.nt;
     nt = p.nt0 + rem % p.nt;
   }

@@ -94,7 +94,7 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
   // -k for the mirror-symmetric G of the mixed path: the identity z of the momentum group
   // (k_add[z + Nc k] = k for all k), then -k = z - k = k_sub[k + Nc z].
   std::vector<int> kneg;
-  if (nc <= kMaxMirrorNc)
+  if (nc <= kMaxKneg)
     for (int z = 0; z < nc && kneg.empty(); ++z) {
       bool id = true;
       for (int k = 0; k < nc; ++k)
@@ -260,9 +260,10 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
         discInit(disc_ws_, dims_, max_batch_, disc_.get(), disc_.bytes());
         have_disc_ = true;
       }
-      // Half G (mirror symmetry) when the tensor-core direct term reads every G of the batch:
-      // one band, Nc = 16, all momentum transfers, and half of D a whole number of 128-row tiles.
-      // DCAACC_TP_FULL_G=1 computes the whole of G instead (for comparisons).
+      // Half G (mirror symmetry) when the direct-term kernel reads mirrored G blocks: one band,
+      // all momentum transfers, Nc = 16 (tensor-core direct term) or Nc = 36 (split FP32 direct
+      // term), and half of D a whole number of 128-row tiles.  DCAACC_TP_FULL_G=1 computes the
+      // whole of G instead (for comparisons).
       std::vector<int> seen(nc, 0);
       int distinct = 0;
       for (int q : q_list_)
@@ -270,7 +271,8 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       const bool q_all = distinct == nc && int(q_list_.size()) == nc;
       const char* full_env = std::getenv("DCAACC_TP_FULL_G");
       const bool full_g = full_env && std::strcmp(full_env, "1") == 0;
-      if (have_disc_ && mirror_ok && !full_g && nb == 1 && nc == kMaxMirrorNc && q_all && c.n_channels <= 2 &&
+      if (have_disc_ && mirror_ok && !full_g && nb == 1 && (nc == kMaxMirrorNc || nc == 36) && q_all &&
+          c.n_channels <= 2 &&
           nw_ext % 2 == 0 && (long(R) * nw_ext / 2) % 128 == 0) {
         dims_.half_g = 1;
         for (int k = 0; k < nc; ++k)

@@ -490,7 +490,12 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
   p.mt0 = a.dims.half_g ? s.D / 2 / kBM : 0;  // half G: X' rows of the upper frequency half only
   p.mt = s.Dp / kBM - p.mt0;
   p.nt = (a.n_max + kBN - 1) / kBN;
+  const TpDims& d = a.dims;
+  const auto pk = tunePick(a.tuner, tuneKey("tc_row_order", d.nb, d.nc, d.nw_ext, a.n_max, a.n_sectors, 2), 2,
+                           stream);
+  p.order = pk.choice;
   launchGemm<0>(p, w.tm_pr, w.tm_mb, w.n_sm, stream);
+  tuneEnd(a.tuner, pk, stream);
 }
 
 void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
@@ -505,7 +510,12 @@ void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float
   p.mt = s.Dq / kBM;                          // rows of G^T: rho2
   p.nt0 = a.dims.half_g ? s.D / 2 / kBN : 0;  // columns of G^T: rho1 (half G: the upper half)
   p.nt = s.Dp / kBN - p.nt0;
+  const TpDims& d = a.dims;
+  const auto pk = tunePick(a.tuner, tuneKey("tc_col_order", d.nb, d.nc, d.nw_ext, a.n_max, a.n_sectors, 2), 2,
+                           stream);
+  p.order = pk.choice;
   launchGemm<1>(p, w.tm_bq, w.tm_ac, w.n_sm, stream);
+  tuneEnd(a.tuner, pk, stream);
 }
 
 }  // namespace dcaacc

@@ -606,31 +606,34 @@ updateG4SinglebandPH(const TpDims dims, const GT* __restrict__ G, long g_sector_
 // case (the plain FP64 path feeds measurements one at a time).  Persistent CTAs walk the (w1, w2,
 // wq) tiles; per tile the eight R x R blocks (A, B, C, E of both spins, see updateG4SinglebandPH)
 // are bulk-copied into one of two shared-memory stages while the previous tile is processed, and
-// the tile's G4 entries are streamed in memory order (k1 contiguous, then k2, then q): a thread
-// takes 8 entries of one channel at a time, issues their 8 loads, then adds and stores them.  A's
-// rows are staged with a one-element pad (row stride R + 1) so that lanes of consecutive k1 read
-// distinct banks.  Each G4 entry is read and written once; G is read from L2 once per tile.
-template <typename GT, typename AT>
-__global__ void __launch_bounds__(256, 3)
+// the tile's G4 entries are streamed in memory order (k1 contiguous, then k2, then q).  With NC
+// (= Nc) a power of two and NC^2 <= 256, thread t keeps k1 = t % NC and k2 = (t / NC) % NC for every
+// tile (so A_s(k1, k2) is one shared-memory read per tile) and walks the transfers q = t / NC^2,
+// + 256 / NC^2, ...: kRound entries at a time it issues their G4 loads, then adds and stores them.
+// A's rows are staged with a one-element pad (row stride R + 1) so that lanes of consecutive k1
+// read distinct banks.  Each G4 entry is read and written once; G is read from L2 once per tile.
+template <typename GT, typename AT, int NC>
+__global__ void __launch_bounds__(256, sizeof(GT) == 16 ? 2 : 3)
 updateG4SinglebandStream(const TpDims dims, const GT* __restrict__ G, long g_sector_stride,
                          const int* __restrict__ signs, const int* __restrict__ k_add,
                          const int* __restrict__ q_list, const int* __restrict__ wex_list,
                          double2* const* __restrict__ G4, bool atomic, int* __restrict__ err) {
   using C = cplx_t<AT>;
-  constexpr int kRound = 8;  // entries in flight per thread
-  const int nc = dims.nc, nw = dims.nw, nw_ext = dims.nw_ext, R = dims.R, nq = dims.nq, ext = dims.ext;
+  constexpr int kRound = 4;            // transfers in flight per thread (two channels each)
+  constexpr int R = NC, RP = NC + 1;   // one band
+  constexpr int blk = R * R, blkA = R * RP;
+  constexpr int stage_elems = 2 * (blkA + 3 * blk);  // per spin: A (padded), B, C, E
+  constexpr int QSTEP = 256 / (NC * NC);             // transfers between a thread's entries
+  const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq, ext = dims.ext;
   const int n_tiles = nw * nw * dims.nwq;
   const int t = threadIdx.x;
-  const int RP = R + 1;                        // padded row stride of A
-  const int blk = R * R, blkA = R * RP;
-  const int stage_elems = 2 * (blkA + 3 * blk);  // per spin: A (padded), B, C, E
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);  // [2]
-  int* kadd = reinterpret_cast<int*>(smem_raw + 16);      // [nc][nc]
-  int* qtab = kadd + nc * nc;                             // [nq]
-  GT* stage = reinterpret_cast<GT*>(smem_raw + 16 + ((sizeof(int) * (nc * nc + nq) + 15) / 16) * 16);
+  int* kadd = reinterpret_cast<int*>(smem_raw + 16);      // [NC][NC]
+  int* qtab = kadd + NC * NC;                             // [nq]
+  GT* stage = reinterpret_cast<GT*>(smem_raw + 16 + ((sizeof(int) * (NC * NC + nq) + 15) / 16) * 16);
 
-  for (int i = t; i < nc * nc; i += blockDim.x)
+  for (int i = t; i < NC * NC; i += blockDim.x)
     kadd[i] = k_add[i];
   for (int i = t; i < nq; i += blockDim.x)
     qtab[i] = q_list[i];
@@ -641,16 +644,10 @@ updateG4SinglebandStream(const TpDims dims, const GT* __restrict__ G, long g_sec
   }
   __syncthreads();
 
-  auto tileOf = [&](int tile, int& w1, int& w2, int& iwq) {
-    w1 = tile % nw;
-    w2 = (tile / nw) % nw;
-    iwq = tile / (nw * nw);
-  };
   // Warp 0 issues a tile's copies: per spin, A row by row (padded), then B, C, E whole.
-  const uint32_t row_bytes = static_cast<uint32_t>(R * sizeof(GT)), blk_bytes = row_bytes * R;
+  constexpr uint32_t row_bytes = R * sizeof(GT), blk_bytes = row_bytes * R;
   auto issue = [&](int tile, int st) {
-    int w1, w2, iwq;
-    tileOf(tile, w1, w2, iwq);
+    const int w1 = tile % nw, w2 = (tile / nw) % nw, iwq = tile / (nw * nw);
     const int wex = wex_list[iwq];
     const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
     const long bA = (static_cast<long>(w1e) * nw_ext + w2e) * blk, bB = (static_cast<long>(w2x) * nw_ext + w1x) * blk,
@@ -673,16 +670,31 @@ updateG4SinglebandStream(const TpDims dims, const GT* __restrict__ G, long g_sec
     }
   };
 
-  // Bit c: channel c is PH-magnetic (else PH-charge); static indices keep dims in registers.
-  int mag_bits = 0;
+  // Positions of the PH-magnetic and PH-charge channels in G4 (-1: not accumulated); static
+  // indices keep dims in registers.
+  int c_mag = -1, c_chg = -1;
 #pragma unroll
-  for (int c = 0; c < kMaxChannels; ++c)
-    mag_bits |= (c < dims.n_channels && dims.channels[c] == 2) << c;
-  const int n_ch = dims.n_channels;
+  for (int c = 0; c < kMaxChannels; ++c) {
+    if (c < dims.n_channels && dims.channels[c] == 2)
+      c_mag = c;
+    if (c < dims.n_channels && dims.channels[c] == 3)
+      c_chg = c;
+  }
   const AT hs = AT(0.5) * static_cast<AT>(signs[0]);
-  const long s_w2 = long(nc) * nw * nc, s_wq = s_w2 * nw * nq;
-  const int s_w1 = nc, s_k2 = nc * nw, s_q = nc * nw * nc * nw;  // < 2^31 for R <= 16, Nw <= 2048
-  const int per_tile = nc * nc * nq;
+  const int k1 = t % NC, k2 = (t / NC) % NC, q0 = t / (NC * NC);
+  // k1 + q and k2 + q of this thread's transfers (at most 16, each < NC <= 16): 4 bits apiece.
+  uint64_t kq1p = 0, kq2p = 0;
+  for (int iq = q0, m = 0; iq < nq; iq += QSTEP, ++m) {
+    const int q = qtab[iq];
+    kq1p |= static_cast<uint64_t>(kadd[k1 + NC * q]) << (4 * m);
+    kq2p |= static_cast<uint64_t>(kadd[k2 + NC * q]) << (4 * m);
+  }
+  // G4 offsets: s_k2 = Nc Nw, s_q = (Nc Nw)^2 (< 2^31 for Nc <= 16, Nw <= 2048), tile base long.
+  const int s_k2 = NC * nw, s_q = NC * nw * NC * nw;
+  const long s_w2 = static_cast<long>(s_k2) * NC, s_wq = static_cast<long>(s_q) * nq;
+  const int own = k1 + k2 * s_k2;  // this thread's entry inside a (tile, q)
+  double2* const g4m = c_mag >= 0 ? G4[c_mag] : nullptr;
+  double2* const g4c = c_chg >= 0 ? G4[c_chg] : nullptr;
 
   int it = 0;
   if (t < 32 && blockIdx.x < n_tiles)
@@ -697,9 +709,8 @@ updateG4SinglebandStream(const TpDims dims, const GT* __restrict__ G, long g_sec
       __syncwarp();
       issue(tile + gridDim.x, st ^ 1);
     }
-    int w1, w2, iwq;
-    tileOf(tile, w1, w2, iwq);
-    const long base = long(w1) * s_w1 + w2 * s_w2 + iwq * s_wq;
+    const int w1 = tile % nw, w2 = (tile / nw) % nw, iwq = tile / (nw * nw);
+    const long base = static_cast<long>(w1) * NC + w2 * s_w2 + iwq * s_wq + own;
     const bool ok = mbarWait(&bar[st], (it >> 1) & 1, err);
     if (!__syncthreads_and(ok)) {
       // Give up; the copies of the other stage (if issued) land before the CTA exits.
@@ -712,39 +723,50 @@ updateG4SinglebandStream(const TpDims dims, const GT* __restrict__ G, long g_sec
     const GT *A0 = S, *B0 = S + blkA, *C0 = B0 + blk, *E0 = C0 + blk;
     const GT *A1 = S + blkA + 3 * blk, *B1 = A1 + blkA, *C1 = B1 + blk, *E1 = C1 + blk;
     auto ld = [](const GT* p) { return mk(static_cast<AT>(p->x), static_cast<AT>(p->y)); };
-    for (int c = 0; c < n_ch; ++c) {
-      const bool mag = (mag_bits >> c) & 1;
-      double2* g4 = G4[c] + base;
-      for (int e0 = t; e0 < per_tile; e0 += kRound * blockDim.x) {
-        double2 old[kRound];
+    const C a0 = ld(A0 + k1 * RP + k2), a1 = ld(A1 + k1 * RP + k2);
+    // Both channels per entry: they share D = sum_s A_s B_s and u_s, v_s up to the spin signs.
+    for (int iq0 = q0, m0 = 0; iq0 < nq; iq0 += kRound * QSTEP, m0 += kRound) {
+      double2 om[kRound], oc[kRound];
 #pragma unroll
-        for (int r = 0; r < kRound; ++r) {
-          const int e = e0 + r * blockDim.x;
-          if (!atomic && e < per_tile) {
-            const int k1 = e % nc, k2 = (e / nc) % nc, iq = e / (nc * nc);
-            old[r] = g4[k1 + k2 * s_k2 + iq * s_q];
-          }
+      for (int r = 0; r < kRound; ++r) {
+        const long o = static_cast<long>(iq0 + r * QSTEP) * s_q;
+        if (!atomic && iq0 + r * QSTEP < nq) {
+          if (g4m)
+            om[r] = g4m[base + o];
+          if (g4c)
+            oc[r] = g4c[base + o];
         }
+      }
 #pragma unroll
-        for (int r = 0; r < kRound; ++r) {
-          const int e = e0 + r * blockDim.x;
-          if (e >= per_tile)
-            break;
-          const int k1 = e % nc, k2 = (e / nc) % nc, iq = e / (nc * nc), q = qtab[iq];
-          const int kq1 = kadd[k1 + nc * q], kq2 = kadd[k2 + nc * q];
-          C d = cmul(ld(A0 + k1 * RP + k2), ld(B0 + kq2 * R + kq1));
-          cfma(d, ld(A1 + k1 * RP + k2), ld(B1 + kq2 * R + kq1));
-          const C u0 = ld(C0 + k1 * R + kq1), u1 = ld(C1 + k1 * R + kq1);
-          const C v0 = ld(E0 + kq2 * R + k2), v1 = ld(E1 + kq2 * R + k2);
-          const C u = mag ? csub(u0, u1) : cadd(u0, u1), v = mag ? csub(v0, v1) : cadd(v0, v1);
-          const C val = cscale(csub(cmul(u, v), d), hs);
-          double2* p = g4 + (k1 + k2 * s_k2 + iq * s_q);
+      for (int r = 0; r < kRound; ++r) {
+        const int iq = iq0 + r * QSTEP;
+        if (iq >= nq)
+          break;
+        const int kq1 = static_cast<int>((kq1p >> (4 * (m0 + r))) & 15u);
+        const int kq2 = static_cast<int>((kq2p >> (4 * (m0 + r))) & 15u);
+        C d = cmul(a0, ld(B0 + kq2 * R + kq1));
+        cfma(d, a1, ld(B1 + kq2 * R + kq1));
+        const C u0 = ld(C0 + k1 * R + kq1), u1 = ld(C1 + k1 * R + kq1);
+        const C v0 = ld(E0 + kq2 * R + k2), v1 = ld(E1 + kq2 * R + k2);
+        const long o = base + static_cast<long>(iq) * s_q;
+        if (g4m) {
+          const C val = cscale(csub(cmul(csub(u0, u1), csub(v0, v1)), d), hs);
           if (atomic) {
-            atomicAdd(&p->x, static_cast<double>(val.x));
-            atomicAdd(&p->y, static_cast<double>(val.y));
+            atomicAdd(&g4m[o].x, static_cast<double>(val.x));
+            atomicAdd(&g4m[o].y, static_cast<double>(val.y));
           }
           else {
-            *p = make_double2(old[r].x + static_cast<double>(val.x), old[r].y + static_cast<double>(val.y));
+            g4m[o] = make_double2(om[r].x + static_cast<double>(val.x), om[r].y + static_cast<double>(val.y));
+          }
+        }
+        if (g4c) {
+          const C val = cscale(csub(cmul(cadd(u0, u1), cadd(v0, v1)), d), hs);
+          if (atomic) {
+            atomicAdd(&g4c[o].x, static_cast<double>(val.x));
+            atomicAdd(&g4c[o].y, static_cast<double>(val.y));
+          }
+          else {
+            g4c[o] = make_double2(oc[r].x + static_cast<double>(val.x), oc[r].y + static_cast<double>(val.y));
           }
         }
       }
@@ -810,20 +832,21 @@ static bool launchSinglebandPH(const G4Args& a, const GT* G, long g_sector_strid
   return true;
 }
 
-// The streaming single-measurement kernel: one band, PH channels, R <= 16 (two stages of eight
-// blocks in shared memory).
+// The streaming single-measurement kernel: one band, PH channels, Nc in {4, 8, 16} (two stages of
+// eight blocks in shared memory; Nc a compile-time power of two).
 template <typename GT>
 static bool launchSinglebandStream(const G4Args& a, const GT* G, long g_sector_stride, cudaStream_t stream) {
   const TpDims& d = a.dims;
-  if (a.n_slots != 1 || !singlebandPHApplies<GT>(d) || d.R > 16 || a.n_sm <= 0)
+  if (a.n_slots != 1 || !singlebandPHApplies<GT>(d) || a.n_sm <= 0 || (d.nc != 4 && d.nc != 8 && d.nc != 16))
     return false;
   using AT = std::conditional_t<std::is_same_v<GT, double2>, double, float>;
   const size_t tables = ((sizeof(int) * (d.nc * d.nc + d.nq) + 15) / 16) * 16;
   const size_t smem = 16 + tables + 2 * sizeof(GT) * 2 * (size_t(d.R) * (d.R + 1) + 3 * size_t(d.R) * d.R);
-  auto k = updateG4SinglebandStream<GT, AT>;
+  auto k = d.nc == 16 ? updateG4SinglebandStream<GT, AT, 16>
+           : d.nc == 8 ? updateG4SinglebandStream<GT, AT, 8> : updateG4SinglebandStream<GT, AT, 4>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const long tiles = long(d.nw) * d.nw * d.nwq;
-  const int grid = int(std::max(1L, std::min<long>(tiles, 3L * a.n_sm)));
+  const int grid = int(std::max(1L, std::min<long>(tiles, (sizeof(GT) == 16 ? 2L : 3L) * a.n_sm)));
   k<<<grid, 256, smem, stream>>>(d, G, g_sector_stride, a.signs, a.k_add, a.q_list, a.wex_list, a.G4, a.atomic,
                                  a.err);
   DCAACC_LAUNCH_CHECK();

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "async_copy.cuh"
 #include "common.cuh"
@@ -592,13 +593,18 @@ updateG4SinglebandOuter(const TpDims dims, const float2* __restrict__ G, long g_
 // measurements deep); thread (d, k1 block, l1 block) keeps a TA x TB tile of sums in registers.
 // The flush table T[k2][k1 - g KG][q] covers the CTA's entries, and lanes write runs of KG
 // consecutive k1 of G4 (and read the disconnected terms in the same order).
+// Half G (dims.half_g): a block in the lower frequency half is read as the conjugate of its mirror
+// block with k -> -k (G(k1 w; k2 w') = conj G(-k1 w*; -k2 w'*), w* = NwExt - 1 - w): the A rows are
+// staged one by one (row -k1 of the mirror block into the slot of k1), the B block whole, and the
+// gather offsets take -k on the mirrored indices.  Half G4 (tile_order non-null): only the tiles
+// listed there (w1 >= Nw / 2) run.
 template <int NC, int KG, int TA, int TB, int DEPTH>
 __global__ void __launch_bounds__(NC * (KG / TA) * (NC / TB), 1)
 updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
                              const int* __restrict__ signs, int n_slots, const int* __restrict__ k_sub,
                              const int* __restrict__ q_list, const int* __restrict__ wex_list,
-                             const float2* __restrict__ disc, double2* const* __restrict__ G4, bool atomic,
-                             int* __restrict__ err) {
+                             const unsigned* __restrict__ tile_order, const float2* __restrict__ disc,
+                             double2* const* __restrict__ G4, bool atomic, int* __restrict__ err) {
   constexpr int BLK = NC * NC;
   constexpr int AR = KG * NC;         // staged rows of A
   constexpr int SP = AR + BLK;        // one spin's staged A rows + B block
@@ -610,9 +616,17 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
   const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq;
   const int grp = blockIdx.x % KSPLIT;
   const int tile = blockIdx.x / KSPLIT;  // the KSPLIT CTAs of a tile run next to each other
+  const int per_wq = tile_order ? nw * nw / 2 : nw * nw;
   int w1, w2;
-  tileOfIndex(tile % (nw * nw), nw, w1, w2);
-  const int iwq = tile / (nw * nw);
+  if (tile_order) {
+    const unsigned v = tile_order[tile % per_wq];
+    w1 = static_cast<int>(v & 0xffffu);
+    w2 = static_cast<int>(v >> 16);
+  }
+  else {
+    tileOfIndex(tile % per_wq, nw, w1, w2);
+  }
+  const int iwq = tile / per_wq;
   const int wex = wex_list[iwq];
   const int ext = dims.ext;
   const int t = threadIdx.x;
@@ -621,34 +635,59 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
   const int k1_0 = kg0 + (sub / NLB) * TA, l1_0 = (sub % NLB) * TB;
 
   const int w1e = w1 + ext, w2e = w2 + ext, w1x = w1e + wex, w2x = w2e + wex;
-  const long b_A = (static_cast<long>(w1e) * nw_ext + w2e) * BLK + static_cast<long>(kg0) * NC;
-  const long b_B = (static_cast<long>(w2x) * nw_ext + w1x) * BLK;
+  const bool mir_a = dims.half_g && 2 * w1e < nw_ext, mir_b = dims.half_g && 2 * w2x < nw_ext;
+  // A: the KG rows of block (w1e, w2e) from row kg0 on, or (mirrored) rows -k1 of block
+  // (w1e*, w2e*); B: block (w2x, w1x) or its mirror (w2x*, w1x*).
+  const long b_A = mir_a ? (static_cast<long>(nw_ext - 1 - w1e) * nw_ext + nw_ext - 1 - w2e) * BLK
+                         : (static_cast<long>(w1e) * nw_ext + w2e) * BLK + static_cast<long>(kg0) * NC;
+  const long b_B = mir_b ? (static_cast<long>(nw_ext - 1 - w2x) * nw_ext + nw_ext - 1 - w1x) * BLK
+                         : (static_cast<long>(w2x) * nw_ext + w1x) * BLK;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);     // [DEPTH] copies landed
   uint64_t* empty = full + DEPTH;                              // [DEPTH] all warps done reading
   int* ksub = reinterpret_cast<int*>(smem_raw + 16 * DEPTH);  // [NC * NC]
   int* qinv = ksub + BLK;                                     // [NC]
-  constexpr int kHead = (16 * DEPTH + 4 * (BLK + NC) + 15) / 16 * 16;
+  int* kneg = qinv + NC;                                      // [NC] index of -k (half G)
+  int* arow = kneg + NC;                                      // [KG] mirrored A: offset of row -k1
+  constexpr int kHead = (16 * DEPTH + 4 * (BLK + 2 * NC + KG) + 15) / 16 * 16;
   float2* stage = reinterpret_cast<float2*>(smem_raw + kHead);  // [DEPTH][A0 rows, B0, A1 rows, B1]
   float2* T = stage;                                           // flush table, after the batch loop
   const int lane = t % 32;
 
   for (int e = t; e < BLK; e += NT)
     ksub[e] = k_sub[e];
-  for (int e = t; e < NC; e += NT)
+  // -k = k_z - k with z = k_0 - k_0 the zero momentum: k_sub gives it without reading dims' table.
+  const int z0 = k_sub[0];
+  for (int e = t; e < NC; e += NT) {
     qinv[q_list[e]] = e;
+    kneg[e] = k_sub[e + NC * z0];
+  }
+  for (int r = t; r < KG; r += NT)
+    arow[r] = k_sub[kg0 + r + NC * z0] * NC;
+  __syncthreads();
+  auto kn = [&](int k) { return kneg[k]; };
 
-  constexpr uint32_t a_bytes = AR * sizeof(float2), b_bytes = BLK * sizeof(float2);
+  constexpr uint32_t a_bytes = AR * sizeof(float2), b_bytes = BLK * sizeof(float2), row_bytes = NC * sizeof(float2);
+  static_assert(row_bytes % 16 == 0, "bulk copies of single rows");
   auto issue = [&](int slot) {
     const int st = slot % DEPTH;
     float2* dst = stage + st * 2 * SP;
     mbarArriveExpectTx(&full[st], 2 * (a_bytes + b_bytes));
     const float2* src0 = G + g_sector_stride * (2 * slot);
     const float2* src1 = src0 + g_sector_stride;
-    bulkCopyG2S(dst, src0 + b_A, a_bytes, &full[st]);
+    if (mir_a) {
+      for (int r = 0; r < KG; ++r) {  // row -k1 of the mirror block into the slot of k1
+        const float2* row = src0 + b_A + arow[r];
+        bulkCopyG2S(dst + r * NC, row, row_bytes, &full[st]);
+        bulkCopyG2S(dst + SP + r * NC, row + g_sector_stride, row_bytes, &full[st]);
+      }
+    }
+    else {
+      bulkCopyG2S(dst, src0 + b_A, a_bytes, &full[st]);
+      bulkCopyG2S(dst + SP, src1 + b_A, a_bytes, &full[st]);
+    }
     bulkCopyG2S(dst + AR, src0 + b_B, b_bytes, &full[st]);
-    bulkCopyG2S(dst + SP, src1 + b_A, a_bytes, &full[st]);
     bulkCopyG2S(dst + SP + AR, src1 + b_B, b_bytes, &full[st]);
   };
   if (t == 0) {
@@ -672,12 +711,16 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
   for (int i = 0; i < (TA + TB + 1) / 2; ++i)
     oab[i] = 0;
 #pragma unroll
-  for (int a = 0; a < TA; ++a)
-    oab[a / 2] |= static_cast<uint32_t>((k1_0 + a - kg0) * NC + ksub[d + NC * (k1_0 + a)]) << (16 * (a & 1));
+  for (int a = 0; a < TA; ++a) {
+    const int k2 = ksub[d + NC * (k1_0 + a)];  // k1 - d
+    oab[a / 2] |= static_cast<uint32_t>((k1_0 + a - kg0) * NC + (mir_a ? kn(k2) : k2)) << (16 * (a & 1));
+  }
 #pragma unroll
-  for (int b = 0; b < TB; ++b)
-    oab[(TA + b) / 2] |= static_cast<uint32_t>(AR + ksub[d + NC * (l1_0 + b)] * NC + l1_0 + b)
+  for (int b = 0; b < TB; ++b) {
+    const int l1 = l1_0 + b, lr = ksub[d + NC * l1];  // row l1 - d, column l1
+    oab[(TA + b) / 2] |= static_cast<uint32_t>(AR + (mir_b ? kn(lr) * NC + kn(l1) : lr * NC + l1))
                          << (16 * ((TA + b) & 1));
+  }
   auto off = [&](int i) { return static_cast<int>((oab[i / 2] >> (16 * (i & 1))) & 0xffffu); };
 
   float2 acc[TA][TB];
@@ -687,6 +730,7 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
     for (int b = 0; b < TB; ++b)
       acc[a][b] = make_float2(0.f, 0.f);
 
+  const float ca = mir_a ? -1.f : 1.f, cb = mir_b ? -1.f : 1.f;  // conjugation of mirrored blocks
   bool ok = true;
   int sg = n_slots > 0 ? signs[0] : 1;
   for (int m = 0; m < n_slots; ++m) {
@@ -701,12 +745,15 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
       const float2* S = stage + (st * 2 + spin) * SP;
       float2 av[TA];
 #pragma unroll
-      for (int a = 0; a < TA; ++a)
+      for (int a = 0; a < TA; ++a) {
         av[a] = S[off(a)];
+        av[a].y *= ca;
+      }
       // One beta at a time: TA complex FMAs per beta load.
 #pragma unroll
       for (int b = 0; b < TB; ++b) {
-        const float2 bv = S[off(TA + b)];
+        float2 bv = S[off(TA + b)];
+        bv.y *= cb;
         if (add) {
 #pragma unroll
           for (int a = 0; a < TA; ++a)
@@ -802,7 +849,7 @@ constexpr int kSplitNc = 36, kSplitKG = 12, kSplitTB = 9, kSplitDepth = 6;
 
 size_t outerSplitSmem() {
   constexpr int BLK = kSplitNc * kSplitNc;
-  constexpr size_t head = (16 * kSplitDepth + 4 * (BLK + kSplitNc) + 15) / 16 * 16;
+  constexpr size_t head = (16 * kSplitDepth + 4 * (BLK + 2 * kSplitNc + kSplitKG) + 15) / 16 * 16;
   const size_t loop = sizeof(float2) * kSplitDepth * 2 * (kSplitKG * kSplitNc + BLK);
   const size_t table = sizeof(float2) * size_t(kSplitNc) * kSplitKG * (kSplitNc + 1);
   return head + std::max(loop, table);
@@ -814,11 +861,12 @@ void launchOuterSplitTA(const G4Args& a, const float2* G, long stride, const flo
   const size_t smem = outerSplitSmem();
   auto k = updateG4SinglebandOuterSplit<kSplitNc, kSplitKG, TA, kSplitTB, kSplitDepth>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const long blocks = long(d.nw) * d.nw * d.nwq * (kSplitNc / kSplitKG);
+  const long tiles = long(d.nw) * d.nw * d.nwq / (a.tile_order ? 2 : 1);  // half G4: w1 >= Nw / 2 only
+  const long blocks = tiles * (kSplitNc / kSplitKG);
   constexpr int threads = kSplitNc * (kSplitKG / TA) * (kSplitNc / kSplitTB);
   k<<<static_cast<unsigned>(blocks), threads, smem, stream>>>(d, G, stride, a.signs, a.n_slots, a.k_sub,
-                                                              a.q_list, a.wex_list, disc, a.G4, a.atomic,
-                                                              a.err);
+                                                              a.q_list, a.wex_list, a.tile_order, disc, a.G4,
+                                                              a.atomic, a.err);
   DCAACC_LAUNCH_CHECK();
 }
 
@@ -942,9 +990,11 @@ int launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sec
     case 8:
       return launchForNc<8>(a, G, g_sector_stride, mag, charge, stream);
     case kSplitNc:
-      // Disconnected terms on the tensor cores and the split direct term; without the workspace
-      // or with a subset of the transfers, the general one-band kernel (return 0).
-      if (!a.q_all || a.dims.half_g4)
+      // Disconnected terms on the tensor cores and the split direct term (both read mirrored
+      // blocks for half G and run the w1 >= Nw / 2 tiles for half G4); without the workspace or
+      // with a subset of the transfers, the general one-band kernel (return 0; half G is never
+      // enabled then).
+      if (!a.q_all)
         return 0;
       if (const float2* disc = launchDiscGemm(a, G, g_sector_stride, stream)) {
         launchOuterSplit(a, G, g_sector_stride, disc, stream);

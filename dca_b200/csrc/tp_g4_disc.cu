@@ -218,7 +218,11 @@ const float2* launchDiscGemm(const G4Args& a, const float2* G, long g_sector_str
   p.eU = w->eU;
   p.eV = w->eV;
   p.disc = w->out;
+  const auto pk = tunePick(a.tuner, tuneKey("tc_disc_order", d.nb, d.nc, d.nw_ext, a.n_slots, s.probs, 2), 2,
+                           stream);
+  p.order = pk.choice;
   launchGemm<2>(p, w->tm_u, w->tm_v, w->n_sm, stream);
+  tuneEnd(a.tuner, pk, stream);
   return w->out;
 }
 

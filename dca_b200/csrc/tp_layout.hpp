@@ -30,14 +30,15 @@ struct TpDims {
   // are not computed; G(k1 w1; k2 w2) = conj G(-k1 w1'; -k2 w2') with w' = nw_ext - 1 - w (real M
   // and G0(-k, -w) = conj G0(k, w)), and the consumers read that mirror instead.
   int half_g;
-  unsigned char kneg[16];  // index of -k (half_g only)
+  unsigned char kneg[64];  // index of -k (half_g only; Nc <= kMaxKneg)
   // With half_g, and momentum and frequency transfers closed under negation, G4 itself obeys
   // G4(-k1 w1', -k2 w2', -q, -wq) = conj G4(k1 w1, k2 w2, q, wq) (w' = Nw - 1 - w): the update
   // accumulates the frequency tiles with w1 >= Nw / 2 only and the rest is filled from them when
   // G4 is read (finalize, peek).
   int half_g4;
 };
-constexpr int kMaxMirrorNc = 16;
+constexpr int kMaxMirrorNc = 16;  // cluster of the tensor-core direct G4 term
+constexpr int kMaxKneg = 64;      // clusters whose -k table TpDims carries
 
 // Index of element (k1 w1; k2 w2) of a one-band block-layout G (R = Nc) and whether it is stored
 // conjugated there (half_g: the lower-half rows are read from their mirror).

@@ -570,3 +570,22 @@ def test_float_m_and_sign_types(precision):
         typed.accumulate_typed([s.M.astype(np.complex128) for s in m.sectors], list(m.sectors), 1)
     with pytest.raises(LogicError, match="UNSUPPORTED"):
         typed.accumulate_typed([s.M for s in m.sectors], list(m.sectors), 1j)
+
+
+def test_large_cluster_half_g_matches_full_g(monkeypatch):
+    """6x6 single band (t' = -0.15), Nw = 64, all 36 momentum transfers: the mixed path computes
+    the upper frequency half of G and accumulates the G4 tiles with w1 >= Nw/2 only (the split
+    direct term reads lower-half blocks as conjugated mirrors with k -> -k); against
+    DCAACC_TP_FULL_G=1 and the FP64 GPU path."""
+    w = _small("c5", nw_half=32, n_sp=128, n_range=(30, 60))
+    case = case_from_workload(w, 5)
+    monkeypatch.setenv("DCAACC_TP_FULL_G", "0")
+    half = _run_timed(case, False, monkeypatch, max_batch=4)
+    monkeypatch.setenv("DCAACC_TP_FULL_G", "1")
+    full = _run_timed(case, False, monkeypatch, max_batch=4)
+    exact = run_gpu(case, precision=0, max_batch=1)
+    assert half.mirror_mode() == 3 and full.mirror_mode() == 0
+    for h, f, want in zip(half.get_G4(), full.get_G4(), exact.get_G4()):
+        print("6x6 half / full G relative errors:", rel_err(h, want), rel_err(f, want))
+        assert rel_err(h, want) <= MIXED_TOL
+        assert rel_err(f, want) <= MIXED_TOL
