@@ -443,6 +443,46 @@ def run_ours(args, world, rank, local):
            "d2h_bytes_per_step": 256 * 16,
            "readback": "every step, asynchronous into pinned host memory; all landed before the clock stops",
            "value_blocking_readback": n_meas_total / e2e_block_s}
+    # The same loop with M in single precision in pinned host memory (a walker run with SpScalar =
+    # float hands over float M; dcaacc_tp_accumulate_typed widens it as it is read): half the bytes
+    # cross PCIe.  Reported beside the FP64 figure, which stays the headline.
+    pinned32, arenas32 = [], []
+    if not fp64_main:
+        for b0 in range(0, len(pool), B):
+            mats = [s.M for m in pool[b0:b0 + B] for s in m.sectors]
+            arena = torch.empty(max(1, sum(M.shape[0] ** 2 for M in mats)), dtype=torch.float32, pin_memory=True)
+            arenas32.append(arena)
+            flat = arena.numpy()
+            off = 0
+            for m in pool[b0:b0 + B]:
+                pair = []
+                for sec in m.sectors:
+                    n = sec.n
+                    view = flat[off:off + n * n].reshape(n, n)
+                    view[...] = sec.M.T
+                    pair.append(view.T)
+                    off += n * n
+                pinned32.append(pair)
+
+        def step32(i):
+            base = (i % 2) * B
+            acc.accumulate_batch_typed(pinned32[base:base + B], configs[base:base + B], signs[base:base + B],
+                                       np.float32)
+            acc.flush()
+
+        step32(0)  # first host-float batch outside the clock
+        acc.synchronizeCopy()
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            step32(i)
+            acc.peek_G4_async(0, 0, res_np[i])
+        acc.synchronizeCopy()
+        torch.cuda.synchronize()
+        e2e32_s = max_over_ranks(time.perf_counter() - t0, world)
+        e2e["value_fp32_host_m"] = n_meas_total / e2e32_s
+        e2e["h2d_bytes_per_step_fp32_host_m"] = int(h2d / 2)
 
     # Plain FP64, unbatched (the path the mixed one is compared with) and the error between them.
     fp64 = None
@@ -481,6 +521,12 @@ def run_ours(args, world, rank, local):
         acc.accumulate_batch(dev_M[:n_cmp], configs[:n_cmp], signs[:n_cmp])
         acc.finalize()
         err = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(acc.get_G4(), ref_acc.get_G4())]
+        if pinned32:  # and from the single-precision host M of the e2e variant
+            acc.resetAccumulation(2)
+            acc.accumulate_batch_typed(pinned32[:n_cmp], configs[:n_cmp], signs[:n_cmp], np.float32)
+            acc.finalize()
+            e2e["rel_err_vs_fp64_fp32_host_m"] = [float(np.linalg.norm(a - b) / np.linalg.norm(b))
+                                                  for a, b in zip(acc.get_G4(), ref_acc.get_G4())]
         del ref_acc
 
     hbm_gbs, bf16_tf, peak_src = peaks()

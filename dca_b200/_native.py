@@ -102,7 +102,8 @@ def _load():
         "dcaacc_tp_destroy": (None, [p]),
         "dcaacc_tp_reset": (i, [p]),
         "dcaacc_tp_accumulate": (i, [p, POINTER(Sector), i, POINTER(c_double)]),
-        "dcaacc_tp_accumulate_typed": (i, [p, POINTER(Sector), i, c_double, c_double, POINTER(c_double)]),
+        "dcaacc_tp_accumulate_typed": (i, [p, i, POINTER(Sector), i, POINTER(c_double), POINTER(c_double),
+                                           POINTER(c_double)]),
         "dcaacc_tp_accumulate_batch": (i, [p, i, POINTER(Sector), POINTER(c_int32), POINTER(c_double)]),
         "dcaacc_tp_flush": (i, [p]),
         "dcaacc_tp_finalize": (i, [p]),

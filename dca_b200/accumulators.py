@@ -259,20 +259,29 @@ class TpAccumulator:
     _SCALARS = {np.dtype(np.float64): 0, np.dtype(np.float32): 1, np.dtype(np.complex128): 2,
                 np.dtype(np.complex64): 3}
 
+    @staticmethod
+    def _m_dtype(M0):
+        return np.dtype(str(M0.dtype).replace("torch.", "")) if hasattr(M0, "is_cuda") else np.asarray(M0).dtype
+
     def accumulate_typed(self, M_pair, configs, sign, m_dtype=None) -> float:
         """accumulate for the reference's other SpScalar / SignType instantiations
         (dcaacc_tp_accumulate_typed): M of element type m_dtype (by default that of M_pair[0]:
         float64, float32, complex128 or complex64) and a sign that may be complex.  Complex M or a
         sign with an imaginary part raise LogicError (DCAACC_UNSUPPORTED)."""
-        if m_dtype is None:
-            M0 = M_pair[0]
-            m_dtype = np.dtype(str(M0.dtype).replace("torch.", "")) if hasattr(M0, "is_cuda") else np.asarray(M0).dtype
-        m_dtype = np.dtype(m_dtype)
+        return self.accumulate_batch_typed([M_pair], [configs], [sign], m_dtype)
+
+    def accumulate_batch_typed(self, Ms, configs, signs, m_dtype=None) -> float:
+        """accumulate_typed for several measurements in one call (Ms[m], configs[m]: measurement m's
+        pairs, signs[m] its sign)."""
+        count = len(signs)
+        m_dtype = np.dtype(m_dtype if m_dtype is not None else self._m_dtype(Ms[0][0]))
         keep: list = []
-        secs = _make_sectors(M_pair, configs, keep, m_dtype=m_dtype)
+        secs = _make_sectors([M for pair in Ms for M in pair], [c for pair in configs for c in pair], keep, count,
+                             m_dtype=m_dtype)
+        sg = np.asarray(signs, np.complex128)
+        sr, si = np.ascontiguousarray(sg.real), np.ascontiguousarray(sg.imag)
         flops = ctypes.c_double(0)
-        sg = complex(sign)
-        _check(N.lib.dcaacc_tp_accumulate_typed(self._h, secs, self._SCALARS[m_dtype], sg.real, sg.imag,
+        _check(N.lib.dcaacc_tp_accumulate_typed(self._h, count, secs, self._SCALARS[m_dtype], _dptr(sr), _dptr(si),
                                                 ctypes.byref(flops)))
         self._last_inputs = keep
         return flops.value

@@ -106,20 +106,26 @@ int dcaacc_tp_accumulate(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t s
   });
 }
 
-int dcaacc_tp_accumulate_typed(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t m_scalar, double sign_re,
-                               double sign_im, double* flops_out) {
+int dcaacc_tp_accumulate_typed(dcaacc_tp* acc, int32_t n_meas, const dcaacc_sector* sectors, int32_t m_scalar,
+                               const double* signs_re, const double* signs_im, double* flops_out) {
   if (!acc)
     return null_handle();
   return guard([&] {
+    if (n_meas < 0 || (n_meas && (!sectors || !signs_re)))
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "invalid batch");
     if (m_scalar == DCAACC_SCALAR_C64 || m_scalar == DCAACC_SCALAR_C128)
       throw dcaacc::Error(DCAACC_UNSUPPORTED, "complex M (complex-valued models) is not implemented");
     if (m_scalar != DCAACC_SCALAR_F64 && m_scalar != DCAACC_SCALAR_F32)
       throw dcaacc::Error(DCAACC_INVALID_ARG, "unknown M scalar type");
-    if (sign_im != 0.)
-      throw dcaacc::Error(DCAACC_UNSUPPORTED, "complex measurement signs are not implemented");
-    if (sign_re != 1. && sign_re != -1.)
-      throw dcaacc::Error(DCAACC_INVALID_ARG, "sign must be +1 or -1");
-    const double f = acc->impl.accumulate(sectors, sign_re > 0 ? 1 : -1, m_scalar == DCAACC_SCALAR_F32);
+    for (int m = 0; m < n_meas; ++m) {
+      if (signs_im && signs_im[m] != 0.)
+        throw dcaacc::Error(DCAACC_UNSUPPORTED, "complex measurement signs are not implemented");
+      if (signs_re[m] != 1. && signs_re[m] != -1.)
+        throw dcaacc::Error(DCAACC_INVALID_ARG, "sign must be +1 or -1");
+    }
+    double f = 0;
+    for (int m = 0; m < n_meas; ++m)
+      f += acc->impl.accumulate(sectors + 2 * m, signs_re[m] > 0 ? 1 : -1, m_scalar == DCAACC_SCALAR_F32);
     if (flops_out)
       *flops_out = f;
   });

@@ -154,6 +154,7 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
   }
   // ---- cluster transform with band phases: Fb(r, k, b) = e^{i k.r} e^{i k.a_b}
   // (space_transform_2D.hpp:93-140) ----
+  ColFft fft{};
   {
     std::vector<double2> fb(size_t(nb) * nc * nc);
     for (int b = 0; b < nb; ++b)
@@ -170,6 +171,53 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       }
     Fb_.alloc(fb.size());
     DCAACC_CUDA_CHECK(cudaMemcpy(Fb_.get(), fb.data(), Fb_.bytes(), cudaMemcpyHostToDevice));
+    // A 4 x 4 square cluster (integer sites (a, b), momenta 2 pi (m, n) / 4) makes the one-band
+    // cluster transform a 2D FFT: Fb(r, k) = e^{i 2 pi (m a + n b) / 4} Fb(r0, k), r0 the origin.
+    // Checked entry by entry; the column step uses it when it holds.
+    if (nb == 1 && nc == 16) {
+      int rmap[16], kmap[16], r0 = -1, ra[16], rb[16], km[16], kn[16];
+      std::fill(rmap, rmap + 16, -1);
+      std::fill(kmap, kmap + 16, -1);
+      bool ok = true;
+      for (int r = 0; r < 16 && ok; ++r) {
+        const double x = c.r_vecs[2 * r], y = c.r_vecs[2 * r + 1];
+        const long a = std::lround(x), b = std::lround(y);
+        ok = std::abs(x - a) < 1e-9 && std::abs(y - b) < 1e-9;
+        ra[r] = int(((a % 4) + 4) % 4);
+        rb[r] = int(((b % 4) + 4) % 4);
+        const int g = ra[r] + 4 * rb[r];
+        ok = ok && rmap[g] < 0;
+        rmap[g] = r;
+        if (a == 0 && b == 0)
+          r0 = r;
+      }
+      for (int k = 0; k < 16 && ok; ++k) {
+        const double m = c.k_vecs[2 * k] * 4 / (2 * M_PI), n = c.k_vecs[2 * k + 1] * 4 / (2 * M_PI);
+        const long mi = std::lround(m), ni = std::lround(n);
+        ok = std::abs(m - mi) < 1e-9 && std::abs(n - ni) < 1e-9;
+        km[k] = int(((mi % 4) + 4) % 4);
+        kn[k] = int(((ni % 4) + 4) % 4);
+        const int g = km[k] + 4 * kn[k];
+        ok = ok && kmap[g] < 0;
+        kmap[g] = k;
+      }
+      ok = ok && r0 >= 0;
+      for (int k = 0; k < 16 && ok; ++k)
+        for (int r = 0; r < 16 && ok; ++r) {
+          const std::complex<double> f0(fb[size_t(k) * nc + r0].x, fb[size_t(k) * nc + r0].y);
+          const std::complex<double> want =
+              std::exp(std::complex<double>(0, 2 * M_PI * (km[k] * ra[r] + kn[k] * rb[r]) / 4.0)) * f0;
+          ok = std::abs(want - std::complex<double>(fb[size_t(k) * nc + r].x, fb[size_t(k) * nc + r].y)) < 1e-9;
+        }
+      if (ok) {
+        fft.on = 1;
+        fft.r0 = r0;
+        for (int g = 0; g < 16; ++g) {
+          fft.rmap[g] = static_cast<unsigned char>(rmap[g]);
+          fft.kmap[g] = static_cast<unsigned char>(kmap[g]);
+        }
+      }
+    }
     // The cluster transform must map -k to the conjugate phases as well.
     if (mirror_ok)
       for (int k = 0; k < nc; ++k)
@@ -249,6 +297,15 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       // Padding rows stay zero; ordered before the scale kernel frontTcInit launches on stream_.
       DCAACC_CUDA_CHECK(cudaMemsetAsync(ftc_mem_.get(), 0, ftc_mem_.bytes(), stream_));
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
+      // One band, Nc = 16: DCAACC_TP_FACTORED_COL=1 runs the column step factored by orbital (12x
+      // fewer flops than the dense GEMM, FP32 on the CUDA cores); the dense tensor-core GEMM stays
+      // the default while it is the faster of the two.
+      const char* fact_env = std::getenv("DCAACC_TP_FACTORED_COL");
+      ftc_.factored_col = colFactorApplies(dims_) && fact_env && std::strcmp(fact_env, "1") == 0;
+      ftc_.fft = fft;
+      const char* fft_env = std::getenv("DCAACC_TP_COL_FFT");  // =0: the 16 x 16 matrix transform
+      if (fft_env && std::strcmp(fft_env, "0") == 0)
+        ftc_.fft.on = 0;
       for (auto& d : dstage_) {
         d.orb_r.alloc(n_vtx);
         if (non_density_)
@@ -292,6 +349,10 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
           dims_.half_g4 = 1;
           upload_ints(q_mirror_d_, qm);
           upload_ints(wq_mirror_d_, wm);
+          // Device window for reads of the running G4 (peek), whose lower half comes from the
+          // mirror: allocated now, so that reads of up to kPeekWindow entries between batches
+          // neither allocate nor synchronise.
+          peek_d_.alloc(kPeekWindow);
           // Tiles (w1, w2) with w1 >= Nw / 2, each next to the tile that reads its B block as A:
           // (w2, w1) if w2 >= Nw / 2, else the mirror (Nw - 1 - w2, Nw - 1 - w1).
           std::vector<char> seen(size_t(nw) * nw, 0);

@@ -237,6 +237,7 @@ private:
   DevBuf<int> q_mirror_d_, wq_mirror_d_;
   DevBuf<unsigned> tile_order_d_;
   DevBuf<double2> peek_d_;
+  static constexpr size_t kPeekWindow = size_t(1) << 16;  // entries allocated with a half-G4 handle
   // Pinned staging of the batch being assembled, double-buffered: the host fills one set while the
   // uploads from the other (queued behind the previous batch's kernels) are still pending.
   struct HostStage {

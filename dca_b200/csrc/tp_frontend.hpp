@@ -51,6 +51,15 @@ struct FrontTcShape {
   int n_sectors;
   size_t pr_elems, mb_elems, ac_elems, bq_elems;  // FP16 elements of P, M, X' and Q planes
 };
+// The cluster transform of a 4 x 4 square cluster as a 2D FFT: grid point g = a + 4 b is site
+// rmap[g] (coordinates (a, b)) and momentum kmap[g] (2 pi (a, b) / 4); r0 is the site at the
+// origin.  Set up on the host when the cluster's phase table has exactly that structure.
+struct ColFft {
+  int on;
+  int r0;
+  unsigned char rmap[16], kmap[16];
+};
+
 struct FrontTcWorkspace {
   FrontTcShape shape;
   void* pr = nullptr;
@@ -62,6 +71,8 @@ struct FrontTcWorkspace {
   float* mInv = nullptr;   // [sector][Kr] inverse scales of M's rows j
   float* xInv = nullptr;   // [sector][Dp][Kr / 32] inverse scales of X' row chunks
   int n_sm = 0;            // SMs of the device (persistent GEMM grids)
+  bool factored_col = false;  // the column step runs factored by orbital (tp_colfactor.cu), not as a GEMM
+  ColFft fft{};               // ... with its cluster transform as a 4 x 4 FFT (when fft.on)
   CUtensorMap tm_pr, tm_mb, tm_ac, tm_bq;  // TMA descriptors of the four plane arrays
 };
 FrontTcShape frontTcShape(const TpDims& d, int n_sectors, int max_order);
@@ -80,5 +91,9 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
 // gmax (or null): [2 slot + spin] set to each sector's largest |G| (float bits).
 void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
                          int* gmax, int* err, cudaStream_t stream);
+// The same G through the orbital-factored column step (tp_colfactor.cu): one band, Nc = 16.
+bool colFactorApplies(const TpDims& d);
+void launchColFactor(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride, int* gmax,
+                     cudaStream_t stream);
 
 }  // namespace dcaacc

@@ -458,6 +458,13 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
                         stream>>>(a.sectors, a.perm_r, a.perm_c, s.Kr, static_cast<__half*>(w.mb), w.mInv);
   DCAACC_LAUNCH_CHECK();
   tuneEnd(a.tuner, pm, stream);
+  if (w.factored_col) {  // the factored column step reads X' and the twiddles, not Q: P only
+    const long groups = (a.n_max + kBK - 1) / kBK * (kBK / 8);
+    buildPhaseOperandKernel<true><<<dim3(gridX(groups * d.nw_ext), a.n_sectors), 256, 0, stream>>>(
+        d, a.sectors, a.Tr, orb_r, a.Fb, a.G0, w.eP, s.D, s.Dp, s.Dp, s.Kr, static_cast<__half*>(w.pr));
+    DCAACC_LAUNCH_CHECK();
+    return launches + 2;
+  }
   if (a.Tc == a.Tr && orb_c == orb_r) {  // density-density: one pass for P and Q
     // 256 or 128 threads per block (grid-stride loop over independent elements).
     const long groups4 = (a.n_max + kBK - 1) / kBK * (kBK / 4);
@@ -501,6 +508,10 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
 void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
                          int* gmax, int* err, cudaStream_t stream) {
   const FrontTcShape& s = w.shape;
+  if (w.factored_col) {  // one band: the orbital-factored column step (tp_colfactor.cu)
+    launchColFactor(a, w, G, g_sector_stride, gmax, stream);
+    return;
+  }
   GemmParams p = gemmParams(a, w, err);
   p.G = G;
   p.g_sector_stride = g_sector_stride;

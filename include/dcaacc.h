@@ -141,14 +141,16 @@ int dcaacc_tp_reset_loop(dcaacc_tp* acc, int32_t dca_loop);
 int dcaacc_tp_accumulate(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t sign, double* flops_out);
 
 /* accumulate for the reference's other instantiations, accumulate<Configuration, SpScalar, SignType>
- * (tp_accumulator_gpu.hpp:118-125, 322-325): M of element type m_scalar (DCAACC_SCALAR_*) in both
- * sectors, each M pointer read as that type, and the sign as (sign_re, sign_im) for a SignType that
- * may be std::complex.  Real M in float or double with a real sign +1 / -1 is accumulated (float M
- * is widened to double as it is read); complex M, which only complex-valued (e.g. spin-orbit)
- * models produce, and a sign with a non-zero imaginary part return DCAACC_UNSUPPORTED. */
+ * (tp_accumulator_gpu.hpp:118-125, 322-325), for n_meas measurements (sectors [2 n_meas]): M of
+ * element type m_scalar (DCAACC_SCALAR_*) in every sector, each M pointer read as that type, and
+ * measurement m's sign as (signs_re[m], signs_im[m]) for a SignType that may be std::complex
+ * (signs_im may be null).  Real M in float or double with real signs +1 / -1 is accumulated (float
+ * M is widened to double as it is read, and a host float M crosses PCIe at half the bytes); complex
+ * M, which only complex-valued (e.g. spin-orbit) models produce, and a sign with a non-zero
+ * imaginary part return DCAACC_UNSUPPORTED before anything is staged. */
 enum { DCAACC_SCALAR_F64 = 0, DCAACC_SCALAR_F32 = 1, DCAACC_SCALAR_C128 = 2, DCAACC_SCALAR_C64 = 3 };
-int dcaacc_tp_accumulate_typed(dcaacc_tp* acc, const dcaacc_sector* sectors, int32_t m_scalar, double sign_re,
-                               double sign_im, double* flops_out);
+int dcaacc_tp_accumulate_typed(dcaacc_tp* acc, int32_t n_meas, const dcaacc_sector* sectors, int32_t m_scalar,
+                               const double* signs_re, const double* signs_im, double* flops_out);
 
 /* Batched form: n_meas measurements, sectors [2 * n_meas], signs [n_meas]. */
 int dcaacc_tp_accumulate_batch(dcaacc_tp* acc, int32_t n_meas, const dcaacc_sector* sectors,

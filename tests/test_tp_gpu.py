@@ -564,6 +564,14 @@ def test_float_m_and_sign_types(precision):
         acc.finalize()
     for a, b in zip(typed.get_G4(), widened.get_G4()):
         assert rel_err(a, b) <= 1e-15
+    # The batched form gives the same bits as one call per measurement.
+    batched = TpAccumulator(case.G0, case.tp_params(precision=precision, max_batch=2))
+    batched.resetAccumulation(0)
+    batched.accumulate_batch_typed([[np.asfortranarray(s.M.astype(np.float32)) for s in m.sectors] for m in ms],
+                                   [list(m.sectors) for m in ms], [m.sign for m in ms])
+    batched.finalize()
+    for a, b in zip(batched.get_G4(), typed.get_G4()):
+        assert np.array_equal(a, b)
     typed.resetAccumulation(1)
     m = ms[0]
     with pytest.raises(LogicError, match="UNSUPPORTED"):
@@ -589,3 +597,26 @@ def test_large_cluster_half_g_matches_full_g(monkeypatch):
         print("6x6 half / full G relative errors:", rel_err(h, want), rel_err(f, want))
         assert rel_err(h, want) <= MIXED_TOL
         assert rel_err(f, want) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("full_g,fft", [("0", "1"), ("1", "1"), ("0", "0")])
+def test_factored_column_step_matches_dense(monkeypatch, full_g, fft):
+    """One band, Nc = 16: the column step factored by orbital (the column NDFT per orbital, then the
+    cluster transform as a 4 x 4 FFT, or with DCAACC_TP_COL_FFT=0 as a 16 x 16 matrix, FP32 on the
+    CUDA cores; DCAACC_TP_FACTORED_COL=1) against the dense tensor-core GEMM and the FP64 path, with
+    half G (mirror symmetry) and with all of G; an empty spin sector included."""
+    w = _small("c3", n_range=(40, 300))
+    case = case_from_workload(w, 9)
+    case.measurements[3] = W.make_measurement(w, 3, n_override=(0, 57))
+    monkeypatch.setenv("DCAACC_TP_FULL_G", full_g)
+    monkeypatch.setenv("DCAACC_TP_COL_FFT", fft)
+    monkeypatch.setenv("DCAACC_TP_FACTORED_COL", "1")
+    fact = _run_timed(case, False, monkeypatch, max_batch=4)
+    monkeypatch.setenv("DCAACC_TP_FACTORED_COL", "0")
+    dense = _run_timed(case, False, monkeypatch, max_batch=4)
+    exact = run_gpu(case, precision=0, max_batch=1)
+    assert fact.mirror_mode() == dense.mirror_mode() == (0 if full_g == "1" else 3)
+    for f, d, want in zip(fact.get_G4(), dense.get_G4(), exact.get_G4()):
+        print("factored / dense column step, relative errors:", rel_err(f, want), rel_err(d, want))
+        assert rel_err(f, want) <= MIXED_TOL
+        assert rel_err(d, want) <= MIXED_TOL
