@@ -298,14 +298,22 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       DCAACC_CUDA_CHECK(cudaMemsetAsync(ftc_mem_.get(), 0, ftc_mem_.bytes(), stream_));
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
       // One band, Nc = 16: DCAACC_TP_FACTORED_COL=1 runs the column step factored by orbital (12x
-      // fewer flops than the dense GEMM, FP32 on the CUDA cores); the dense tensor-core GEMM stays
-      // the default while it is the faster of the two.
+      // fewer flops than the dense GEMM): on the tensor cores with the 4 x 4 FFT cluster transform
+      // where the cluster has that structure (unless DCAACC_TP_COL_FFT=0), else on the CUDA cores
+      // with the 16 x 16 matrix transform.  Both are slower than the dense tcgen05 GEMM, which is the
+      // default: the factored form's on-chip Z tile (rows x w2 x 16 sites) limits its CTA tiles, so
+      // the operands are re-read many times with too few bytes in flight.
       const char* fact_env = std::getenv("DCAACC_TP_FACTORED_COL");
-      ftc_.factored_col = colFactorApplies(dims_) && fact_env && std::strcmp(fact_env, "1") == 0;
+      const char* fft_env = std::getenv("DCAACC_TP_COL_FFT");
       ftc_.fft = fft;
-      const char* fft_env = std::getenv("DCAACC_TP_COL_FFT");  // =0: the 16 x 16 matrix transform
       if (fft_env && std::strcmp(fft_env, "0") == 0)
         ftc_.fft.on = 0;
+      const bool fact_on = fact_env && std::strcmp(fact_env, "1") == 0;
+      ftc_.factored_col = colFactorApplies(dims_) && fact_on;
+      if (ftc_.factored_col && ftc_.fft.on) {
+        col_tp_.alloc(colTwiddlePlaneBytes(dims_, int(n_sec), fs.Kr));
+        ftc_.tp = col_tp_.get();
+      }
       for (auto& d : dstage_) {
         d.orb_r.alloc(n_vtx);
         if (non_density_)
@@ -807,18 +815,19 @@ int TpAccumulator::launchBatch(const FrontendArgs& fa, const G4Args& ga, DevStag
     launchRowTransform<double>(fa, X64_.get(), stream_);
   timeEnd(DCAACC_STAGE_ROW, b, 1);
   timeBegin(DCAACC_STAGE_COL, &b);
+  int col_launches = 1;
   if (tc_front_)
-    launchFrontendTcCol(fa, ftc_, G32_.get(), g_sector_stride_, gmax_d_.get(), err_d_.get(), stream_);
+    col_launches = launchFrontendTcCol(fa, ftc_, G32_.get(), g_sector_stride_, gmax_d_.get(), err_d_.get(), stream_);
   else if (mixed_)
     launchColTransform<float>(fa, X32_.get(), G32_.get(), g_sector_stride_, stream_);
   else
     launchColTransform<double>(fa, X64_.get(), G64_.get(), g_sector_stride_, stream_);
-  timeEnd(DCAACC_STAGE_COL, b, 1);
+  timeEnd(DCAACC_STAGE_COL, b, col_launches);
   timeBegin(DCAACC_STAGE_G4, &b);
   const int g4_launches = mixed_ ? launchUpdateG4<float2>(ga, G32_.get(), g_sector_stride_, stream_)
                                  : launchUpdateG4<double2>(ga, G64_.get(), g_sector_stride_, stream_);
   timeEnd(DCAACC_STAGE_G4, b, g4_launches);
-  return launched + 2 + g4_launches;
+  return launched + 1 + col_launches + g4_launches;
 }
 
 // Replays the batch's kernel sequence from a CUDA graph keyed by (device input set, batch size,

@@ -230,6 +230,7 @@ private:
   // vertex in row / column order.
   bool tc_front_ = false;
   DevBuf<unsigned char> ftc_mem_;
+  DevBuf<unsigned char> col_tp_;  // factored column step, FFT form: FP16 planes of the column twiddles
   FrontTcWorkspace ftc_{};
   DevBuf<int> gmax_d_;  // [2 slot + spin] largest |G| per sector (column step -> G4 kernel)
   // Half G4 (dims_.half_g4): positions of -q / -wq in the transfer lists, the tiles the update

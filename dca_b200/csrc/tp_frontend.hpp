@@ -73,6 +73,7 @@ struct FrontTcWorkspace {
   int n_sm = 0;            // SMs of the device (persistent GEMM grids)
   bool factored_col = false;  // the column step runs factored by orbital (tp_colfactor.cu), not as a GEMM
   ColFft fft{};               // ... with its cluster transform as a 4 x 4 FFT (when fft.on)
+  void* tp = nullptr;         // ... FFT form: FP16 planes of the column twiddles (colTwiddlePlaneBytes)
   CUtensorMap tm_pr, tm_mb, tm_ac, tm_bq;  // TMA descriptors of the four plane arrays
 };
 FrontTcShape frontTcShape(const TpDims& d, int n_sectors, int max_order);
@@ -87,13 +88,16 @@ int launchFrontendTcPrep(const FrontendArgs& a, const FrontTcWorkspace& w, const
                          cudaStream_t stream);
 // X' = P M (one launch).
 void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* err, cudaStream_t stream);
-// G = X' Q^H + beta G0 delta into the block-layout G (one launch).
+// G = X' Q^H + beta G0 delta into the block-layout G; returns the number of kernels launched.
 // gmax (or null): [2 slot + spin] set to each sector's largest |G| (float bits).
-void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
+int launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
                          int* gmax, int* err, cudaStream_t stream);
 // The same G through the orbital-factored column step (tp_colfactor.cu): one band, Nc = 16.
+// With the FFT cluster transform it runs on the tensor cores and needs colTwiddlePlaneBytes of
+// workspace (FrontTcWorkspace::tp); otherwise on the CUDA cores.
 bool colFactorApplies(const TpDims& d);
-void launchColFactor(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride, int* gmax,
+size_t colTwiddlePlaneBytes(const TpDims& d, int n_sectors, int Kr);
+int launchColFactor(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride, int* gmax,
                      cudaStream_t stream);
 
 }  // namespace dcaacc

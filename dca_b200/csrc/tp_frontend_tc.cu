@@ -505,13 +505,11 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
   tuneEnd(a.tuner, pk, stream);
 }
 
-void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
-                         int* gmax, int* err, cudaStream_t stream) {
+int launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
+                        int* gmax, int* err, cudaStream_t stream) {
   const FrontTcShape& s = w.shape;
-  if (w.factored_col) {  // one band: the orbital-factored column step (tp_colfactor.cu)
-    launchColFactor(a, w, G, g_sector_stride, gmax, stream);
-    return;
-  }
+  if (w.factored_col)  // one band: the orbital-factored column step (tp_colfactor.cu)
+    return launchColFactor(a, w, G, g_sector_stride, gmax, stream);
   GemmParams p = gemmParams(a, w, err);
   p.G = G;
   p.g_sector_stride = g_sector_stride;
@@ -527,6 +525,7 @@ void launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float
   p.order = pk.choice;
   launchGemm<1>(p, w.tm_bq, w.tm_ac, w.n_sm, stream);
   tuneEnd(a.tuner, pk, stream);
+  return 1;
 }
 
 }  // namespace dcaacc
