@@ -28,6 +28,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 
 #include "async_copy.cuh"
 #include "common.cuh"
@@ -858,6 +860,9 @@ int launchUpdateG4(const G4Args& a, const GT* G, long g_sector_stride, cudaStrea
   if constexpr (std::is_same_v<GT, float2>) {
     if (const int n = launchUpdateG4SinglebandBatched(a, G, g_sector_stride, stream))
       return n;
+    const char* pp_env = std::getenv("DCAACC_TP_PP_GENERIC");  // =1: the generic staged kernel instead
+    if (!(pp_env && std::strcmp(pp_env, "1") == 0) && launchUpdateG4PPMultiband(a, G, g_sector_stride, stream))
+      return 1;
   }
   if (launchSinglebandStream<GT>(a, G, g_sector_stride, stream))
     return 1;

@@ -61,6 +61,10 @@ bool singlebandBatchedApplies(const TpDims& d);
 int launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sector_stride,
                                     cudaStream_t stream);
 
+// Multiband particle-particle up-down update, mixed path (tp_g4_pp.cu): three bands, that channel
+// alone, full G and G4.  Returns false (nothing launched) when the configuration is not covered.
+bool launchUpdateG4PPMultiband(const G4Args& a, const float2* G, long g_sector_stride, cudaStream_t stream);
+
 // Tensor-core disconnected terms (tp_g4_disc.cu): one band, PH channels, batches of at most 256.
 // discInit carves `mem` (discScratchBytes) and builds the descriptors; launchDiscGemm returns the
 // device result (per problem an M x M FP32 matrix), or null without a workspace.

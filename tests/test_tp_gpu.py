@@ -363,6 +363,27 @@ def test_multiband_batched_matches_oracle(oracle_lib, channels, precision):
         assert rel_err(got, want) <= tol
 
 
+@pytest.mark.parametrize("all_transfers", [True, False])
+def test_pp_multiband_kernel_matches_generic_and_oracle(oracle_lib, monkeypatch, all_transfers):
+    """Three bands, particle-particle up-down alone, mixed path: the PP kernel (a thread keeps the
+    27 band entries of one (k1, k2, q, b4) over the batch) against the generic staged kernel
+    (DCAACC_TP_PP_GENERIC=1) and the oracle.  With all 8 x 2 transfers its items fill three passes
+    of the CTA; with one momentum transfer they fill part of one pass."""
+    w = _small("c4", nw_half=4, n_sp=64, n_range=(20, 60), channels=(4,), freq_transfer=1,
+               all_transfers=all_transfers, k_transfer=3)
+    case = case_from_workload(w, 7)
+    monkeypatch.setenv("DCAACC_TP_PP_GENERIC", "0")
+    pp = run_gpu(case, precision=1, max_batch=4)
+    monkeypatch.setenv("DCAACC_TP_PP_GENERIC", "1")
+    generic = run_gpu(case, precision=1, max_batch=4)
+    ora = run_oracle(oracle_lib, case)
+    for a, g, want in zip(pp.get_G4(), generic.get_G4(), ora.get_G4()):
+        print("PP kernel / generic staged kernel, relative errors:", rel_err(a, want), rel_err(g, want))
+        assert rel_err(a, want) <= MIXED_TOL
+        assert rel_err(g, want) <= MIXED_TOL
+        assert rel_err(a, g) <= MIXED_TOL
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_sum_to_equals_single_accumulator(precision):
     case, _ = golden("sq2_all")
