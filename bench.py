@@ -558,13 +558,20 @@ def run_ours(args, world, rank, local):
                 "split36": "discPlanesKernel + frontGemmKernel<2> (disconnected terms) + "
                            "updateG4SinglebandOuterSplit (direct term, G4 flush)",
                 "staged": "updateG4StagedKernel (all terms, G blocks staged in shared memory)",
+                "pp3": "updateG4PPMultibandKernel (particle-particle up-down, 27 band entries per thread)",
                 "simt": "updateG4SinglebandBatched",
                 "stream": "updateG4SinglebandStream (one measurement, G4 streamed in memory order)",
                 "fp64_other": "updateG4SinglebandPH / updateG4Kernel (one measurement)"}
+    # Column step and G4 kernels as the accumulator selects them (environment switches included).
+    half_any = bool(mirror & 1) or bool(mirror & 2)
+    factored_col = (os.environ.get("DCAACC_TP_FACTORED_COL") == "1" and nb == 1 and nc == 16
+                    and os.environ.get("DCAACC_TP_COL_FFT") != "0" and not fp64_main and not simt)
     if fp64_main:
         g4_path = "stream" if nb == 1 and nc * nc <= 256 and set(w.channels) <= {2, 3} else "fp64_other"
     elif simt:
         g4_path = "simt"
+    elif nb == 3 and tuple(w.channels) == (4,) and not half_any and os.environ.get("DCAACC_TP_PP_GENERIC") != "1":
+        g4_path = "pp3"
     elif nb > 1:
         g4_path = "staged"
     elif nc == 36:
@@ -575,8 +582,11 @@ def run_ours(args, world, rank, local):
                                    "split36": ["discPlanesKernel", "frontGemmKernel<2>",
                                                "updateG4SinglebandOuterSplit"],
                                    "staged": ["updateG4StagedKernel"],
+                                   "pp3": ["updateG4PPMultibandKernel"],
                                    "stream": ["updateG4SinglebandStream"]}.get(g4_path, []),
-                     "col_transform": ["frontGemmKernel<1>"], "row_transform": ["frontGemmKernel<0>"],
+                     "col_transform": (["colTwiddlePlanesKernel", "colFactorMmaKernel"] if factored_col
+                                       else ["frontGemmKernel<1>"]),
+                     "row_transform": ["frontGemmKernel<0>"],
                      "twiddle": ["twiddleWiKernel", "buildMOperandKernel", "buildPhasePairKernel"]}
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of each stage's kernels per launch of
     # the stage, from the committed ncu capture of this workload (cold caches).
@@ -626,7 +636,13 @@ def run_ours(args, world, rank, local):
         Dp = -(-D // 128) * 128
         mma_flop = 2.0 * 128 * 128 * 16
         rows_done = 0.5 if mirror & 1 else 1.0  # half G: the upper frequency half of the rows
-        if dom == "col_transform":
+        if dom == "col_transform" and factored_col:
+            # The orbital-factored column step (mma.sync m16n8k16, no dense product): its work is
+            # the algorithmic one, so only the algorithmic rate is reported.
+            dense = alg_flops[dom]
+            mma = 0.0
+            kern = "colTwiddlePlanesKernel + colFactorMmaKernel (orbital-factored column step)"
+        elif dom == "col_transform":
             dense = per_step * float(np.sum(8.0 * D * D * ns)) * rows_done
             mma = per_step * float(np.sum((Dp // 128) ** 2 * rows_done * chunks * 24 * mma_flop))
             kern = "frontGemmKernel<1> (column step, G = X' Q^H + beta G0 delta)"
