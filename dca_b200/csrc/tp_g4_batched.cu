@@ -598,6 +598,8 @@ updateG4SinglebandOuter(const TpDims dims, const float2* __restrict__ G, long g_
 // staged one by one (row -k1 of the mirror block into the slot of k1), the B block whole, and the
 // gather offsets take -k on the mirrored indices.  Half G4 (tile_order non-null): only the tiles
 // listed there (w1 >= Nw / 2) run.
+constexpr int kSplitMaxSlots = 256;  // measurements per launch (the signs sit in shared memory)
+
 template <int NC, int KG, int TA, int TB, int DEPTH>
 __global__ void __launch_bounds__(NC * (KG / TA) * (NC / TB), 1)
 updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
@@ -650,7 +652,8 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
   int* qinv = ksub + BLK;                                     // [NC]
   int* kneg = qinv + NC;                                      // [NC] index of -k (half G)
   int* arow = kneg + NC;                                      // [KG] mirrored A: offset of row -k1
-  constexpr int kHead = (16 * DEPTH + 4 * (BLK + 2 * NC + KG) + 15) / 16 * 16;
+  int* sgn = arow + KG;                                       // [kSplitMaxSlots] measurement signs
+  constexpr int kHead = (16 * DEPTH + 4 * (BLK + 2 * NC + KG + kSplitMaxSlots) + 15) / 16 * 16;
   float2* stage = reinterpret_cast<float2*>(smem_raw + kHead);  // [DEPTH][A0 rows, B0, A1 rows, B1]
   float2* T = stage;                                           // flush table, after the batch loop
   const int lane = t % 32;
@@ -665,6 +668,8 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
   }
   for (int r = t; r < KG; r += NT)
     arow[r] = k_sub[kg0 + r + NC * z0] * NC;
+  for (int m = t; m < n_slots; m += NT)
+    sgn[m] = signs[m];
   __syncthreads();
   auto kn = [&](int k) { return kneg[k]; };
 
@@ -703,25 +708,27 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
       issue(m);
 
   // Fixed gather offsets: alpha from the staged A rows (row k1 - kg0, column k1 - d), beta from B
-  // (row l1 - d, column l1); two 16-bit offsets per register (SP < 2^16), so that the TA x TB sums
-  // stay in registers.
+  // (row l1 - d, column l1).
+  // The beta offsets two to a register (SP < 2^16), so that the TA x TB sums stay in registers.
   static_assert(SP < 65536, "16-bit gather offsets");
-  uint32_t oab[(TA + TB + 1) / 2];
-#pragma unroll
-  for (int i = 0; i < (TA + TB + 1) / 2; ++i)
-    oab[i] = 0;
+  int oa[TA];
+  uint32_t ob2[(TB + 1) / 2];
 #pragma unroll
   for (int a = 0; a < TA; ++a) {
     const int k2 = ksub[d + NC * (k1_0 + a)];  // k1 - d
-    oab[a / 2] |= static_cast<uint32_t>((k1_0 + a - kg0) * NC + (mir_a ? kn(k2) : k2)) << (16 * (a & 1));
+    oa[a] = (k1_0 + a - kg0) * NC + (mir_a ? kn(k2) : k2);
   }
+#pragma unroll
+  for (int i = 0; i < (TB + 1) / 2; ++i)
+    ob2[i] = 0;
 #pragma unroll
   for (int b = 0; b < TB; ++b) {
     const int l1 = l1_0 + b, lr = ksub[d + NC * l1];  // row l1 - d, column l1
-    oab[(TA + b) / 2] |= static_cast<uint32_t>(AR + (mir_b ? kn(lr) * NC + kn(l1) : lr * NC + l1))
-                         << (16 * ((TA + b) & 1));
+    ob2[b / 2] |= static_cast<uint32_t>(AR + (mir_b ? kn(lr) * NC + kn(l1) : lr * NC + l1)) << (16 * (b & 1));
   }
-  auto off = [&](int i) { return static_cast<int>((oab[i / 2] >> (16 * (i & 1))) & 0xffffu); };
+  auto ob = [&](int b) {
+    return static_cast<int>((b & 1) ? (ob2[b / 2] >> 16) : __byte_perm(ob2[b / 2], 0u, 0x4410u));
+  };
 
   float2 acc[TA][TB];
 #pragma unroll
@@ -730,59 +737,61 @@ updateG4SinglebandOuterSplit(const TpDims dims, const float2* __restrict__ G, lo
     for (int b = 0; b < TB; ++b)
       acc[a][b] = make_float2(0.f, 0.f);
 
-  const float ca = mir_a ? -1.f : 1.f, cb = mir_b ? -1.f : 1.f;  // conjugation of mirrored blocks
+  // acc += alpha' beta with alpha' = -s (conj if mirrored) alpha, folded into the TA alphas once per
+  // spin; a mirrored B block's conjugation is a compile-time variant of the product (CB).
   bool ok = true;
-  int sg = n_slots > 0 ? signs[0] : 1;
-  for (int m = 0; m < n_slots; ++m) {
-    const int st = m % DEPTH;
-    const int sg_next = m + 1 < n_slots ? signs[m + 1] : 1;
-    ok = __all_sync(0xffffffffu, mbarWait(&full[st], (m / DEPTH) & 1, err));
-    if (!ok)
-      break;
-    const bool add = sg < 0;
+  auto run = [&](auto cb_tag) {
+    constexpr bool CB = decltype(cb_tag)::value;
+    const float ia = mir_a ? -1.f : 1.f;
+    for (int m = 0; m < n_slots; ++m) {
+      const int st = m % DEPTH;
+      ok = __all_sync(0xffffffffu, mbarWait(&full[st], (m / DEPTH) & 1, err));
+      if (!ok)
+        break;
+      const float ns = -static_cast<float>(sgn[m]);
 #pragma unroll
-    for (int spin = 0; spin < 2; ++spin) {
-      const float2* S = stage + (st * 2 + spin) * SP;
-      float2 av[TA];
+      for (int spin = 0; spin < 2; ++spin) {
+        const float2* S = stage + (st * 2 + spin) * SP;
+        float2 av[TA];
 #pragma unroll
-      for (int a = 0; a < TA; ++a) {
-        av[a] = S[off(a)];
-        av[a].y *= ca;
-      }
-      // One beta at a time: TA complex FMAs per beta load.
-#pragma unroll
-      for (int b = 0; b < TB; ++b) {
-        float2 bv = S[off(TA + b)];
-        bv.y *= cb;
-        if (add) {
-#pragma unroll
-          for (int a = 0; a < TA; ++a)
-            cfma(acc[a][b], av[a], bv);
+        for (int a = 0; a < TA; ++a) {
+          const float2 x = S[oa[a]];
+          av[a] = make_float2(ns * x.x, ns * ia * x.y);
         }
-        else {
+#pragma unroll
+        for (int b = 0; b < TB; ++b) {
+          const float2 bv = S[ob(b)];
 #pragma unroll
           for (int a = 0; a < TA; ++a) {
             float2& c = acc[a][b];
-            c.x = fmaf(-av[a].x, bv.x, c.x);
-            c.x = fmaf(av[a].y, bv.y, c.x);
-            c.y = fmaf(-av[a].x, bv.y, c.y);
-            c.y = fmaf(-av[a].y, bv.x, c.y);
+            if constexpr (CB) {  // av conj(bv)
+              c.x = fmaf(av[a].x, bv.x, c.x);
+              c.x = fmaf(av[a].y, bv.y, c.x);
+              c.y = fmaf(av[a].y, bv.x, c.y);
+              c.y = fmaf(-av[a].x, bv.y, c.y);
+            }
+            else {
+              cfma(c, av[a], bv);
+            }
           }
         }
       }
-    }
-    sg = sg_next;
-    __syncwarp();
-    if (lane == 0)
-      mbarArrive(&empty[st]);  // release: this warp's reads of the stage are done
-    if (t == 0 && m + DEPTH < n_slots) {
-      if (!mbarWait(&empty[st], (m / DEPTH) & 1, err)) {
-        ok = false;  // the other warps see the missing copy as a timeout of their own
-        break;
+      __syncwarp();
+      if (lane == 0)
+        mbarArrive(&empty[st]);  // release: this warp's reads of the stage are done
+      if (t == 0 && m + DEPTH < n_slots) {
+        if (!mbarWait(&empty[st], (m / DEPTH) & 1, err)) {
+          ok = false;  // the other warps see the missing copy as a timeout of their own
+          break;
+        }
+        issue(m + DEPTH);
       }
-      issue(m + DEPTH);
     }
-  }
+  };
+  if (mir_b)
+    run(std::true_type{});
+  else
+    run(std::false_type{});
   if (__syncthreads_or(!ok))
     return;  // uniform bail-out; the host reports the error word
 
@@ -849,7 +858,7 @@ constexpr int kSplitNc = 36, kSplitKG = 12, kSplitTB = 9, kSplitDepth = 6;
 
 size_t outerSplitSmem() {
   constexpr int BLK = kSplitNc * kSplitNc;
-  constexpr size_t head = (16 * kSplitDepth + 4 * (BLK + 2 * kSplitNc + kSplitKG) + 15) / 16 * 16;
+  constexpr size_t head = (16 * kSplitDepth + 4 * (BLK + 2 * kSplitNc + kSplitKG + kSplitMaxSlots) + 15) / 16 * 16;
   const size_t loop = sizeof(float2) * kSplitDepth * 2 * (kSplitKG * kSplitNc + BLK);
   const size_t table = sizeof(float2) * size_t(kSplitNc) * kSplitKG * (kSplitNc + 1);
   return head + std::max(loop, table);
@@ -994,7 +1003,7 @@ int launchUpdateG4SinglebandBatched(const G4Args& a, const float2* G, long g_sec
       // blocks for half G and run the w1 >= Nw / 2 tiles for half G4); without the workspace or
       // with a subset of the transfers, the general one-band kernel (return 0; half G is never
       // enabled then).
-      if (!a.q_all)
+      if (!a.q_all || a.n_slots > kSplitMaxSlots)
         return 0;
       if (const float2* disc = launchDiscGemm(a, G, g_sector_stride, stream)) {
         launchOuterSplit(a, G, g_sector_stride, disc, stream);
