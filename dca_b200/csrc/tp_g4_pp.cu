@@ -31,17 +31,19 @@ namespace {
 constexpr int kPPThreads = 512;
 constexpr int kPPStages = 4;  // ring of per-measurement block sets: copies run three steps ahead
 
-template <int NB>
+template <int NB, int NC>
 __global__ void __launch_bounds__(kPPThreads, 1)
 updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long g_sector_stride,
                           const int* __restrict__ signs, int n_slots, const int* __restrict__ k_sub,
                           const int* __restrict__ q_list, const int* __restrict__ wex_list,
                           double2* const* __restrict__ G4, bool atomic, int* __restrict__ err, uint32_t wait_limit) {
   constexpr int NB2 = NB * NB, NB3 = NB2 * NB, NB4 = NB3 * NB;
-  const int nc = dims.nc, nw = dims.nw, nw_ext = dims.nw_ext, R = dims.R, nq = dims.nq, ext = dims.ext;
-  const int w1 = blockIdx.x, w2 = blockIdx.y, iwq = blockIdx.z;
+  constexpr int nc = NC, R = NB * NC;  // compile-time block shape: the band offsets are immediates
+  const int nw = dims.nw, nw_ext = dims.nw_ext, nq = dims.nq, ext = dims.ext;
+  // wq fastest: the CTAs that read the same A block G(w1; w2) run side by side (one L2 fetch).
+  const int iwq = blockIdx.x, w2 = blockIdx.y, w1 = blockIdx.z;
   const int wex = wex_list[iwq];
-  const long blk = static_cast<long>(R) * R;
+  constexpr long blk = static_cast<long>(R) * R;
   const int n_items = nc * nc * nq * NB;
   const int n_passes = (n_items + kPPThreads - 1) / kPPThreads;
   const long n_steps = static_cast<long>(n_passes) * n_slots;
@@ -50,7 +52,8 @@ updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long 
   const long offP = (static_cast<long>(m1) * nw_ext + m2) * blk;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);     // [kPPStages]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);     // [kPPStages] a stage's copies landed
+  uint64_t* empty = bar + kPPStages;                         // [kPPStages] every warp is done with it
   float2* stage = reinterpret_cast<float2*>(smem_raw + 64);  // [kPPStages][spin][A, P][R * R]
   const uint32_t blk_bytes = static_cast<uint32_t>(blk * sizeof(float2));
   auto issue = [&](long step) {
@@ -65,9 +68,12 @@ updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long 
     }
   };
   const int t = threadIdx.x;
+  const int lane = t % 32;
   if (t == 0) {
-    for (int i = 0; i < kPPStages; ++i)
+    for (int i = 0; i < kPPStages; ++i) {
       mbarInit(&bar[i], 1);
+      mbarInit(&empty[i], kPPThreads / 32);
+    }
     fenceBarrierInit();
   }
   __syncthreads();
@@ -87,6 +93,7 @@ updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long 
   int* sgn = reinterpret_cast<int*>(fb + NB3 * kPPThreads);  // [n_slots] the measurements' signs
   for (int i = t; i < n_slots; i += kPPThreads)
     sgn[i] = signs[i];
+  __syncthreads();  // the signs are in place before any warp's first step
   long pend = -1;  // G4 offset of this thread's pending item
   int fe = NB3;    // its next entry to write
   auto flushEntry = [&](double2* dst, float2 v, double2 old) {
@@ -120,6 +127,7 @@ updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long 
     }
   };
   long step = 0;
+  bool ok = true;
   for (int pass = 0; pass < n_passes; ++pass) {
     const int item = t + kPPThreads * pass;
     const bool live = item < n_items;
@@ -151,9 +159,10 @@ updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long 
         if (!atomic)
           fold = *fdst;
       }
-      const bool ok = mbarWait(&bar[st], static_cast<uint32_t>((step / kPPStages) & 1), err, limit);
-      if (!__syncthreads_and(ok))
-        return;  // uniform bail-out; the host reports the error word
+      const uint32_t phase = static_cast<uint32_t>((step / kPPStages) & 1);
+      ok = __all_sync(0xffffffffu, mbarWait(&bar[st], phase, err, limit));
+      if (!ok)
+        break;
       const float2* A0 = stage + st * 4 * blk;
       const float2* P0 = A0 + blk;
       const float2* A1 = A0 + 2 * blk;
@@ -183,12 +192,20 @@ updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long 
         flushEntry(fdst, fv, fold);
         ++fe;
       }
-      __syncthreads();  // stage st is free again
+      __syncwarp();
+      if (lane == 0)
+        mbarArrive(&empty[st]);  // release: this warp's reads of the stage are done
       if (t == 0 && step + kPPStages < n_steps) {
+        if (!mbarWait(&empty[st], phase, err, limit)) {
+          ok = false;  // the other warps see the missing copies as a timeout of their own
+          break;
+        }
         fenceProxyAsync();
         issue(step + kPPStages);
       }
     }
+    if (__syncthreads_or(!ok))
+      return;  // uniform bail-out; the host reports the error word
     flushRest();  // batches shorter than nb^3 measurements leave entries of the previous pass
     if (live) {
 #pragma unroll
@@ -213,15 +230,15 @@ updateG4PPMultibandKernel(const TpDims dims, const float2* __restrict__ G, long 
 bool launchUpdateG4PPMultiband(const G4Args& a, const float2* G, long g_sector_stride, cudaStream_t stream) {
   const TpDims& d = a.dims;
   if (d.n_channels != 1 || d.channels[0] != 4 /* PARTICLE_PARTICLE_UP_DOWN */ || d.nb != 3 || d.half_g4 || d.half_g ||
-      a.n_slots < 1 || (size_t(d.R) * d.R * sizeof(float2)) % 16 != 0)
+      a.n_slots < 1 || (d.nc != 4 && d.nc != 8))
     return false;
   const size_t smem = 64 + kPPStages * 4 * size_t(d.R) * d.R * sizeof(float2) +
                       27 * size_t(kPPThreads) * sizeof(float2) + sizeof(int) * size_t(a.n_slots);
   if (smem > 220 * 1024)
     return false;
-  auto k = updateG4PPMultibandKernel<3>;
+  auto k = d.nc == 4 ? updateG4PPMultibandKernel<3, 4> : updateG4PPMultibandKernel<3, 8>;
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  const dim3 grid(d.nw, d.nw, d.nwq);
+  const dim3 grid(d.nwq, d.nw, d.nw);
   k<<<grid, kPPThreads, smem, stream>>>(d, G, g_sector_stride, a.signs, a.n_slots, a.k_sub, a.q_list, a.wex_list,
                                          a.G4, a.atomic, a.err, a.wait_limit);
   DCAACC_LAUNCH_CHECK();
