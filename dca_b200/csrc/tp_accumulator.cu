@@ -298,19 +298,23 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       DCAACC_CUDA_CHECK(cudaMemsetAsync(ftc_mem_.get(), 0, ftc_mem_.bytes(), stream_));
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
       // One band, Nc = 16: DCAACC_TP_FACTORED_COL=1 runs the column step factored by orbital (12x
-      // fewer flops than the dense GEMM): on the tensor cores with the 4 x 4 FFT cluster transform
-      // where the cluster has that structure (unless DCAACC_TP_COL_FFT=0), else on the CUDA cores
-      // with the 16 x 16 matrix transform.  Both are slower than the dense tcgen05 GEMM, which is the
-      // default: the factored form's on-chip Z tile (rows x w2 x 16 sites) limits its CTA tiles, so
-      // the operands are re-read many times with too few bytes in flight.
+      // fewer flops than the dense GEMM): with mma.sync and the 4 x 4 FFT cluster transform where
+      // the cluster has that structure (unless DCAACC_TP_COL_FFT=0), else on the CUDA cores with the
+      // 16 x 16 matrix transform; =2 on tcgen05 with the per-site sums in tensor memory (4 x 4
+      // clusters).  All are slower than the dense tcgen05 GEMM, which is the default: in shared
+      // memory the per-site sums cap the CTA tiles (operands re-read with too few bytes in flight),
+      // in tensor memory each CTA's per-site operand chain is latency-bound.
       const char* fact_env = std::getenv("DCAACC_TP_FACTORED_COL");
       const char* fft_env = std::getenv("DCAACC_TP_COL_FFT");
       ftc_.fft = fft;
       if (fft_env && std::strcmp(fft_env, "0") == 0)
         ftc_.fft.on = 0;
       const bool fact_on = fact_env && std::strcmp(fact_env, "1") == 0;
-      ftc_.factored_col = colFactorApplies(dims_) && fact_on;
-      if (ftc_.factored_col && ftc_.fft.on) {
+      const bool fact_tc = fact_env && std::strcmp(fact_env, "2") == 0;  // the tensor-memory form
+      const int row0 = dims_.half_g ? fs.D / 2 : 0;
+      ftc_.col_tc = fact_tc && colFactorApplies(dims_) && ftc_.fft.on && colFactorTcApplies(dims_, fs.D, row0, max_order_);
+      ftc_.factored_col = colFactorApplies(dims_) && (fact_on || ftc_.col_tc);
+      if (ftc_.factored_col && ftc_.fft.on && !ftc_.col_tc) {
         col_tp_.alloc(colTwiddlePlaneBytes(dims_, int(n_sec), fs.Kr));
         ftc_.tp = col_tp_.get();
       }

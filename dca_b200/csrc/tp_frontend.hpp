@@ -74,6 +74,7 @@ struct FrontTcWorkspace {
   bool factored_col = false;  // the column step runs factored by orbital (tp_colfactor.cu), not as a GEMM
   ColFft fft{};               // ... with its cluster transform as a 4 x 4 FFT (when fft.on)
   void* tp = nullptr;         // ... FFT form: FP16 planes of the column twiddles (colTwiddlePlaneBytes)
+  bool col_tc = false;        // ... FFT form with the per-site sums in tensor memory (tp_colfactor_tc.cu)
   CUtensorMap tm_pr, tm_mb, tm_ac, tm_bq;  // TMA descriptors of the four plane arrays
 };
 FrontTcShape frontTcShape(const TpDims& d, int n_sectors, int max_order);
@@ -97,6 +98,10 @@ int launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2
 // workspace (FrontTcWorkspace::tp); otherwise on the CUDA cores.
 bool colFactorApplies(const TpDims& d);
 size_t colTwiddlePlaneBytes(const TpDims& d, int n_sectors, int Kr);
+// The tensor-memory form (tp_colfactor_tc.cu): one band, 4 x 4 cluster, rows in whole 128-row tiles.
+bool colFactorTcApplies(const TpDims& d, int D, int row0, int max_order);
+int launchColFactorTc(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride, int* gmax,
+                      int* err, cudaStream_t stream);
 int launchColFactor(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride, int* gmax,
                      cudaStream_t stream);
 

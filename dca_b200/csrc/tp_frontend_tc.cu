@@ -508,6 +508,8 @@ void launchFrontendTcRow(const FrontendArgs& a, const FrontTcWorkspace& w, int* 
 int launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride,
                         int* gmax, int* err, cudaStream_t stream) {
   const FrontTcShape& s = w.shape;
+  if (w.factored_col && w.col_tc)  // one band, 4 x 4: factored, the site sums in tensor memory
+    return launchColFactorTc(a, w, G, g_sector_stride, gmax, err, stream);
   if (w.factored_col)  // one band: the orbital-factored column step (tp_colfactor.cu)
     return launchColFactor(a, w, G, g_sector_stride, gmax, stream);
   GemmParams p = gemmParams(a, w, err);

@@ -620,18 +620,21 @@ def test_large_cluster_half_g_matches_full_g(monkeypatch):
         assert rel_err(f, want) <= MIXED_TOL
 
 
-@pytest.mark.parametrize("full_g,fft", [("0", "1"), ("1", "1"), ("0", "0")])
-def test_factored_column_step_matches_dense(monkeypatch, full_g, fft):
+@pytest.mark.parametrize("full_g,fft,mode", [("0", "1", "1"), ("1", "1", "1"), ("0", "0", "1"), ("0", "1", "2"),
+                                             ("1", "1", "2")])
+def test_factored_column_step_matches_dense(monkeypatch, full_g, fft, mode):
     """One band, Nc = 16: the column step factored by orbital (the column NDFT per orbital, then the
-    cluster transform as a 4 x 4 FFT, or with DCAACC_TP_COL_FFT=0 as a 16 x 16 matrix, FP32 on the
-    CUDA cores; DCAACC_TP_FACTORED_COL=1) against the dense tensor-core GEMM and the FP64 path, with
-    half G (mirror symmetry) and with all of G; an empty spin sector included."""
+    cluster transform as a 4 x 4 FFT, or with DCAACC_TP_COL_FFT=0 as a 16 x 16 matrix), with
+    DCAACC_TP_FACTORED_COL=1 on mma.sync / the CUDA cores and with =2 on tcgen05 with the per-site
+    sums in tensor memory, against the dense tensor-core GEMM and the FP64 path, with half G
+    (mirror symmetry) and with all of G; an empty spin sector included, orders up to 300 (ten
+    32-vertex chunks, sites straddling chunk and 16-vertex step boundaries)."""
     w = _small("c3", n_range=(40, 300))
     case = case_from_workload(w, 9)
     case.measurements[3] = W.make_measurement(w, 3, n_override=(0, 57))
     monkeypatch.setenv("DCAACC_TP_FULL_G", full_g)
     monkeypatch.setenv("DCAACC_TP_COL_FFT", fft)
-    monkeypatch.setenv("DCAACC_TP_FACTORED_COL", "1")
+    monkeypatch.setenv("DCAACC_TP_FACTORED_COL", mode)
     fact = _run_timed(case, False, monkeypatch, max_batch=4)
     monkeypatch.setenv("DCAACC_TP_FACTORED_COL", "0")
     dense = _run_timed(case, False, monkeypatch, max_batch=4)
