@@ -567,8 +567,10 @@ def run_ours(args, world, rank, local):
                 "fp64_other": "updateG4SinglebandPH / updateG4Kernel (one measurement)"}
     # Column step and G4 kernels as the accumulator selects them (environment switches included).
     half_any = bool(mirror & 1) or bool(mirror & 2)
-    factored_col = (os.environ.get("DCAACC_TP_FACTORED_COL") == "1" and nb == 1 and nc == 16
-                    and os.environ.get("DCAACC_TP_COL_FFT") != "0" and not fp64_main and not simt)
+    col_env = os.environ.get("DCAACC_TP_FACTORED_COL")
+    factorable = nb == 1 and nc == 16 and not fp64_main and not simt
+    col_tc = factorable and col_env not in ("0", "1") and os.environ.get("DCAACC_TP_COL_FFT") != "0"
+    factored_col = factorable and (col_tc or (col_env == "1" and os.environ.get("DCAACC_TP_COL_FFT") != "0"))
     if fp64_main:
         g4_path = "stream" if nb == 1 and nc * nc <= 256 and set(w.channels) <= {2, 3} else "fp64_other"
     elif simt:
@@ -587,10 +589,12 @@ def run_ours(args, world, rank, local):
                                    "staged": ["updateG4StagedKernel"],
                                    "pp3": ["updateG4PPMultibandKernel"],
                                    "stream": ["updateG4SinglebandStream"]}.get(g4_path, []),
-                     "col_transform": (["colTwiddlePlanesKernel", "colFactorMmaKernel"] if factored_col
+                     "col_transform": (["colFactorTcKernel"] if col_tc else
+                                       ["colTwiddlePlanesKernel", "colFactorMmaKernel"] if factored_col
                                        else ["frontGemmKernel<1>"]),
                      "row_transform": ["frontGemmKernel<0>"],
-                     "twiddle": ["twiddleWiKernel", "buildMOperandKernel", "buildPhasePairKernel"]}
+                     "twiddle": (["twiddleWiKernel", "buildMOperandKernel", "buildPhaseOperandKernel"] if factored_col
+                                 else ["twiddleWiKernel", "buildMOperandKernel", "buildPhasePairKernel"])}
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of each stage's kernels per launch of
     # the stage, from the committed ncu capture of this workload (cold caches).
     traffic = {}
@@ -640,11 +644,12 @@ def run_ours(args, world, rank, local):
         mma_flop = 2.0 * 128 * 128 * 16
         rows_done = 0.5 if mirror & 1 else 1.0  # half G: the upper frequency half of the rows
         if dom == "col_transform" and factored_col:
-            # The orbital-factored column step (mma.sync m16n8k16, no dense product): its work is
-            # the algorithmic one, so only the algorithmic rate is reported.
-            dense = alg_flops[dom]
-            mma = 0.0
-            kern = "colTwiddlePlanesKernel + colFactorMmaKernel (orbital-factored column step)"
+            # The orbital-factored column step (no dense product): its work is the algorithmic one
+            # (plus the site-masked zeros of its MMAs), so only the algorithmic rate is reported.
+            dense = mma = None
+            kern = ("colFactorTcKernel (column step factored by orbital: per-site sums in tensor memory, "
+                    "4 x 4 FFT, G0 factor)" if col_tc else
+                    "colTwiddlePlanesKernel + colFactorMmaKernel (orbital-factored column step)")
         elif dom == "col_transform":
             dense = per_step * float(np.sum(8.0 * D * D * ns)) * rows_done
             mma = per_step * float(np.sum((Dp // 128) ** 2 * rows_done * chunks * 24 * mma_flop))
@@ -657,8 +662,13 @@ def run_ours(args, world, rank, local):
                 "unit": "TFLOP/s", "algorithmic_flops": alg_flops[dom],
                 "peak_note": "measured dense BF16 burst peak; algorithmic flops per the survey's per-spin "
                              "count, so the dense reformulation's extra work is not credited",
-                "dense_form_flops": dense, "dense_form_tflops": dense / sec / 1e12,
-                "mma_issued_tflops": mma / sec / 1e12, "mma_frac_of_bf16_peak": mma / sec / 1e12 / bf16_tf}
+                }
+        if dense is not None:
+            roof.update({"dense_form_flops": dense, "dense_form_tflops": dense / sec / 1e12,
+                         "mma_issued_tflops": mma / sec / 1e12, "mma_frac_of_bf16_peak": mma / sec / 1e12 / bf16_tf})
+        else:
+            roof["work_note"] = ("factored by orbital: the column NDFT per site on the tensor cores, then the 4 x 4 "
+                                 "FFT over the sites; no dense product")
     else:
         # SIMT front-end stages are dominated by their global traffic (M / X' / G, complex of the
         # path's precision).

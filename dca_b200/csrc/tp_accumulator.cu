@@ -297,22 +297,21 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       // Padding rows stay zero; ordered before the scale kernel frontTcInit launches on stream_.
       DCAACC_CUDA_CHECK(cudaMemsetAsync(ftc_mem_.get(), 0, ftc_mem_.bytes(), stream_));
       frontTcInit(ftc_, fs, ftc_mem_.get(), dims_, G0_.get(), stream_);
-      // One band, Nc = 16: DCAACC_TP_FACTORED_COL=1 runs the column step factored by orbital (12x
-      // fewer flops than the dense GEMM): with mma.sync and the 4 x 4 FFT cluster transform where
-      // the cluster has that structure (unless DCAACC_TP_COL_FFT=0), else on the CUDA cores with the
-      // 16 x 16 matrix transform; =2 on tcgen05 with the per-site sums in tensor memory (4 x 4
-      // clusters).  All are slower than the dense tcgen05 GEMM, which is the default: in shared
-      // memory the per-site sums cap the CTA tiles (operands re-read with too few bytes in flight),
-      // in tensor memory each CTA's per-site operand chain is latency-bound.
+      // One band on a 4 x 4 cluster: the column step runs factored by orbital (12x fewer flops than
+      // the dense GEMM) on tcgen05 with the per-site sums in tensor memory (tp_colfactor_tc.cu),
+      // which also spares the dense step's Q operand.  DCAACC_TP_FACTORED_COL=0 keeps the dense
+      // GEMM; =1 selects the other factored forms (mma.sync with the 4 x 4 FFT, or the CUDA cores
+      // with the 16 x 16 matrix transform, which DCAACC_TP_COL_FFT=0 forces), both slower.
       const char* fact_env = std::getenv("DCAACC_TP_FACTORED_COL");
       const char* fft_env = std::getenv("DCAACC_TP_COL_FFT");
       ftc_.fft = fft;
       if (fft_env && std::strcmp(fft_env, "0") == 0)
         ftc_.fft.on = 0;
+      const bool fact_off = fact_env && std::strcmp(fact_env, "0") == 0;
       const bool fact_on = fact_env && std::strcmp(fact_env, "1") == 0;
-      const bool fact_tc = fact_env && std::strcmp(fact_env, "2") == 0;  // the tensor-memory form
       const int row0 = dims_.half_g ? fs.D / 2 : 0;
-      ftc_.col_tc = fact_tc && colFactorApplies(dims_) && ftc_.fft.on && colFactorTcApplies(dims_, fs.D, row0, max_order_);
+      ftc_.col_tc = !fact_off && !fact_on && colFactorApplies(dims_) && ftc_.fft.on &&
+                    colFactorTcApplies(dims_, fs.D, row0, max_order_);
       ftc_.factored_col = colFactorApplies(dims_) && (fact_on || ftc_.col_tc);
       if (ftc_.factored_col && ftc_.fft.on && !ftc_.col_tc) {
         col_tp_.alloc(colTwiddlePlaneBytes(dims_, int(n_sec), fs.Kr));

@@ -11,12 +11,16 @@
 // SM.  Warp roles:
 //   warp 0     TMA loads of the X' chunks (the row step's split-FP16 planes, 128 rows x 32 vertices
 //              per plane, 64-byte swizzle; the column GEMM's descriptors), two stages;
-//   warp 1     tensor-memory allocation and the MMA issue: per (chunk, site) item and 16-vertex step
-//              that overlaps the site, D_r += Xr B_re + Xi B_im with split FP16 (lo hi, hi lo, hi hi),
-//              six M128 N16 K16 MMAs;
-//   warps 2-5  build each item's B operands in shared memory: per 8 frequencies and 32 vertices
-//              B_re = [Tr; -Ti], B_im = [Ti; Tr] (rows 2 w, 2 w + 1), the vertices of other sites
-//              zeroed, split into FP16 hi / lo planes, in a ring of 2 items; then the epilogue.
+//   warp 1     tensor-memory allocation and the MMA issue: the sites a chunk touches are consecutive
+//              in site order, so their sums are contiguous columns and up to four of them take one
+//              MMA: per (chunk, site group) item and 16-vertex step, D += Xr B_re + Xi B_im with split
+//              FP16 (lo hi, hi lo, hi hi), six M128 x N(16 per site) x K16 MMAs (a tcgen05 MMA costs
+//              about as long to issue whatever its N, so the sites share instructions);
+//   warps 2-5  zero the tensor memory (so that every MMA accumulates), then build each item's B
+//              operands in shared memory: per site 8 frequencies x 32 vertices, B_re = [Tr; -Ti],
+//              B_im = [Ti; Tr] (rows 16 i + 2 w, + 1), the vertices of other sites zeroed, split into
+//              FP16 hi / lo planes, in a ring of 2 items; the chunk twiddles are loaded one chunk
+//              ahead; then the epilogue.
 // The X' chunk scales 2^-e_c fold into B exactly (T 2^12 s_c / s_max), so each site sums all of its
 // chunks in tensor memory without promotion: a site spans one or two 16-vertex steps per chunk, so
 // every tensor-memory sum is a short chain (the precision the dense GEMM gets from promoting every
@@ -24,10 +28,10 @@
 // 16 sites' Z in the FFT's slot order, runs the 4 x 4 FFT, applies the G0 factor and the delta
 // term, and writes its row of 16 momenta through a warp-private shared-memory transpose, so each
 // store instruction writes 512 contiguous bytes of G.
-// Measured on B200 (4x4 cluster, Nw = 64, n ~ U[50, 400]): 6.0 us per sector against 3.5 us for the
-// dense tcgen05 GEMM; the MMAs keep the tensor pipe 3 % busy and the per-CTA chain of TMA loads,
-// operand builds and mbarrier hand-offs per (chunk, site), then the FFT epilogue, sets the time.
-// Selected by DCAACC_TP_FACTORED_COL=2; the dense GEMM is the default.
+// Measured on B200 (c3: 4x4 cluster, Nw = 64, n ~ U[50, 400], batch 64): 0.44 ms per batch, the
+// same as the dense tcgen05 GEMM, and the batch saves the dense step's Q operand planes.  A CTA
+// (about 30 us) spends about 15 us issuing its MMAs and taking the builders' operands and 11 us in
+// the FFT epilogue; two CTAs per SM overlap those phases.
 #include <cuda.h>
 #include <algorithm>
 #include <cuda_fp16.h>
@@ -41,7 +45,6 @@
 #include "tp_layout.hpp"
 
 namespace dcaacc {
-
 namespace {
 
 constexpr int kW = 8;                         // frequencies w2 per CTA
@@ -51,7 +54,8 @@ constexpr uint32_t kTmemCols = kSites * kN;   // 256
 constexpr int kXStages = 2;
 constexpr uint32_t kXBox = 128 * 32 * 2;      // one X' plane box: 8 KB
 constexpr uint32_t kXStage = 4 * kXBox;       // re hi, re lo, im hi, im lo
-constexpr uint32_t kBTile = kN * 64;          // one B plane: 16 rows x 64 bytes
+constexpr int kMaxGroup = 4;                  // consecutive sites stacked into one MMA (N <= 64)
+constexpr uint32_t kBTile = kMaxGroup * kN * 64;  // one B plane: up to 64 rows x 64 bytes
 constexpr uint32_t kBItem = 4 * kBTile;       // B_re hi, B_re lo, B_im hi, B_im lo
 constexpr int kBSlots = 2;
 constexpr int kBuilders = 128;                // warps 2..5
@@ -59,18 +63,17 @@ constexpr int kThreads = 64 + kBuilders;
 constexpr float kTScale = 4096.f;
 // Shared memory (from a 1024-byte aligned base): X' stages, B ring, then the rest.
 constexpr uint32_t kOffB = kXStages * kXStage;                  // 64 KB
-constexpr uint32_t kOffC = kOffB + kBSlots * kBItem;            // Cs, Ds: float2 [kW][16] each
+constexpr uint32_t kOffT = kOffB + kBSlots * kBItem;            // chunk twiddles, float2 [2][kW][32]
+constexpr uint32_t kOffC = kOffT + 2 * kW * 32 * 8;             // Cg, Ds: float2 [kW][16] each
 constexpr uint32_t kOffTab = kOffC + 2 * kW * 16 * 8;           // cs[17], rm[16], km[16], smax
 constexpr uint32_t kOffBar = kOffTab + 4 * 64;                  // barriers, tensor-memory slot
-constexpr uint32_t kOffT = (kOffBar + 8 * (2 * kXStages + 2 * kBSlots + 1) + 16 + 15) / 16 * 16;  // twiddles
-// + the CTA's twiddles, float2 [kW][ts], ts = the batch's largest order rounded up to 32 (sized at
-// launch).
-__host__ __device__ constexpr size_t colFactorTcSmem(int ts) {
-  return 1024 + kOffT + sizeof(float2) * size_t(kW) * ts;
+constexpr uint32_t kSmemUsed = kOffBar + 8 * (2 * kXStages + 2 * kBSlots + 1) + 16;
+__host__ __device__ constexpr size_t colFactorTcSmem(int) {
+  return 1024 + kSmemUsed;
 }
 constexpr int kEpiRowB = 144;  // epilogue transpose: one row of 16 momenta (+16 bytes)
 static_assert(kXStages * kXStage >= 4 * 32 * kEpiRowB, "epilogue staging fits in the X' stages");
-static_assert(kOffT % 16 == 0, "twiddle table alignment");
+static_assert(kOffT % 16 == 0 && kOffC % 16 == 0, "table alignment");
 
 __device__ inline void ld32x32bx4(uint32_t taddr, float (&v)[4]) {
   uint32_t r[4];
@@ -80,6 +83,14 @@ __device__ inline void ld32x32bx4(uint32_t taddr, float (&v)[4]) {
 #pragma unroll
   for (int i = 0; i < 4; ++i)
     v[i] = __uint_as_float(r[i]);
+}
+
+// Zeros into 32 consecutive columns of the warp's 32 lanes.
+__device__ inline void stZero32x32bx32(uint32_t taddr) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+      "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr), "r"(0u)
+      : "memory");
 }
 
 __device__ inline void namedSync128() {
@@ -101,18 +112,32 @@ __device__ inline uint32_t sw64(int r, int q) {
   return static_cast<uint32_t>(r * 64 + ((q ^ ((r >> 1) & 3)) << 4));
 }
 
+// The sites whose vertex ranges meet chunk [c0, c0 + 32): ra .. rb (consecutive in site order;
+// sites without vertices in between are included and add nothing).
+__device__ inline void chunkSites(const int* cs, int c0, int n, int& ra, int& rb) {
+  const int c1 = min(c0 + 32, n);
+  ra = kSites;
+  rb = -1;
+  for (int r = 0; r < kSites; ++r) {
+    if (cs[r + 1] > c0 && ra == kSites)
+      ra = r;
+    if (cs[r] < c1 && cs[r + 1] > cs[r])
+      rb = r;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 2)
 colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, const SectorDesc* __restrict__ sectors,
                   const int* __restrict__ col_start, const double2* __restrict__ T, const float* __restrict__ xInv,
                   int Dp, int Kr, const double2* __restrict__ Fb, const double2* __restrict__ G0,
                   float2* __restrict__ G, long g_sector_stride, int* __restrict__ gmax, int row0, const ColFft fft,
-                  int ts, int* __restrict__ err) {
+                  int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  float2* Ts = reinterpret_cast<float2*>(base + kOffT);  // [kW][ts] T(w2, j) 2^12 s_c / s_max
-  float2* Cs = reinterpret_cast<float2*>(base + kOffC);  // [kW][16] -(1/Nc) G0 conj Fb(r0, k2)
-  float2* Ds = Cs + kW * 16;                             // [kW][16] beta G0, the delta term
+  float2* Ts = reinterpret_cast<float2*>(base + kOffT);  // [2][kW][32] a chunk's T 2^12 s_c / s_max
+  float2* Cg = reinterpret_cast<float2*>(base + kOffC);  // [kW][FFT slot g] -(1/Nc) G0 conj Fb(r0, km[g])
+  float2* Ds = Cg + kW * 16;                             // [kW][k2] beta G0, the delta term
   int* cs = reinterpret_cast<int*>(base + kOffTab);      // [17] site starts (column order)
   int* rm = cs + 17;                                     // [16] FFT slot -> site
   int* km = rm + 16;                                     // [16] FFT slot -> momentum
@@ -144,7 +169,7 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
       mbarInit(&empty_x[s], 1);
     }
     for (int s = 0; s < kBSlots; ++s) {
-      mbarInit(&full_b[s], kBuilders);
+      mbarInit(&full_b[s], kBuilders / 32);  // one arrival per builder warp
       mbarInit(&empty_b[s], 1);
     }
     mbarInit(acc_full, 1);
@@ -173,17 +198,34 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
   }
   for (int i = t; i < kW * 16; i += kThreads) {
     const int k = i % 16, w2 = w2_0 + i / 16;
-    double2 g0 = G0[static_cast<long>(sd.spin) * nw_ext * 16 + k + 16 * w2];  // G0_s(k, w2), one band
-    Ds[i] = make_float2(static_cast<float>(dims.beta * g0.x), static_cast<float>(dims.beta * g0.y));
-    const double2 f = Fb[k * 16 + fft.r0];  // the band phase e^{-i k a}: conj Fb(r0, k) (x_r0 = 0)
+    const double2 g0d = G0[static_cast<long>(sd.spin) * nw_ext * 16 + k + 16 * w2];  // G0_s(k, w2), one band
+    Ds[i] = make_float2(static_cast<float>(dims.beta * g0d.x), static_cast<float>(dims.beta * g0d.y));
+    // Slot order: entry (w, g) holds the factor of momentum km[g].
+    int kg = 0;
+#pragma unroll
+    for (int g = 0; g < 16; ++g)
+      if (g == k)
+        kg = fft.kmap[g];
+    double2 g0 = G0[static_cast<long>(sd.spin) * nw_ext * 16 + kg + 16 * w2];
+    const double2 f = Fb[kg * 16 + fft.r0];  // the band phase e^{-i k a}: conj Fb(r0, k) (x_r0 = 0)
     g0 = make_double2(g0.x * f.x + g0.y * f.y, g0.y * f.x - g0.x * f.y);
-    Cs[i] = make_float2(static_cast<float>(-g0.x / 16), static_cast<float>(-g0.y / 16));
+    Cg[i] = make_float2(static_cast<float>(-g0.x / 16), static_cast<float>(-g0.y / 16));
   }
   tc::fenceBeforeThreadSync();
   __syncthreads();
   tc::fenceAfterThreadSync();
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
+  if (warp >= 2) {  // every site's sums start at zero, so that each MMA accumulates
+    const uint32_t qa = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);
+#pragma unroll
+    for (uint32_t c = 0; c < kTmemCols; c += 32)
+      stZero32x32bx32(qa + c);
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  }
+  tc::fenceBeforeThreadSync();
+  __syncthreads();
+  tc::fenceAfterThreadSync();
 
   if (warp == 0) {
     if (lane == 0) {
@@ -202,6 +244,7 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
           tc::tmaLoad3d(st + (2 + pl) * kXBox, &tmX, Kr + c * 32, mt * 128, z, &full_x[s]);  // im
         }
       }
+
       // Loads still in flight are waited for (bounded) before the CTA can exit.
       for (int c = max(0, n_chunks - kXStages); c < n_chunks; ++c)
         mbarWait(&full_x[c % kXStages], (c / kXStages) & 1, err);
@@ -209,10 +252,15 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
   }
   else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = tc::instrDescF16F32(128, kN);
       const int pa[3] = {1, 0, 0};  // (A plane, B plane) products, smallest first: lo hi, hi lo, hi hi
       const int pb[3] = {0, 1, 0};
-      unsigned inited = 0;  // sites whose accumulator has been written
+      // Descriptors of stage 0 / slot 0; the others differ by the stage / slot stride (>> 4).
+      uint64_t dA[4], dB[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        dA[i] = tc::smemDescSw64(base + i * kXBox);
+        dB[i] = tc::smemDescSw64(base + kOffB + i * kBTile);
+      }
       int item = 0;
       for (int c = 0; c < n_chunks && ok; ++c) {
         const int s = c % kXStages;
@@ -221,34 +269,32 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
           break;
         }
         tc::fenceAfterThreadSync();
-        const unsigned char* xst = base + s * kXStage;
         const int c0 = c * 32;
-        for (int r = 0; r < kSites; ++r) {
-          const int lo = cs[r], hi = cs[r + 1];
-          if (lo >= hi || hi <= c0 || lo >= c0 + 32)
-            continue;
+        int ra, rb;
+        chunkSites(cs, c0, n, ra, rb);
+        for (int g0 = ra; g0 <= rb; g0 += kMaxGroup) {
+          const int ng = min(kMaxGroup, rb - g0 + 1);
+          const int lo = cs[g0], hi = cs[g0 + ng];
           const int slot = item % kBSlots;
           if (!mbarWait(&full_b[slot], (item / kBSlots) & 1, err)) {
             ok = false;
             break;
           }
           tc::fenceAfterThreadSync();
-          const unsigned char* bst = base + kOffB + slot * kBItem;
-          const uint32_t d = tmem + r * kN;
+          const uint32_t d = tmem + g0 * kN;
+          const uint32_t idesc = tc::instrDescF16F32(128, kN * ng);
+          // The small products of both 16-vertex steps first, then the hi x hi ones.
 #pragma unroll
-          for (int kk = 0; kk < 2; ++kk) {
-            if (hi <= c0 + 16 * kk || lo >= c0 + 16 * kk + 16)
-              continue;  // this 16-vertex step holds none of the site's vertices
+          for (int pp = 0; pp < 3; ++pp) {
 #pragma unroll
-            for (int pp = 0; pp < 3; ++pp) {
-              const uint32_t acc = ((inited >> r) & 1u) ? 1u : 0u;
-              const uint64_t ar = tc::descAdvance(tc::smemDescSw64(xst + (0 + pa[pp]) * kXBox), kk * 32);
-              const uint64_t ai = tc::descAdvance(tc::smemDescSw64(xst + (2 + pa[pp]) * kXBox), kk * 32);
-              const uint64_t br = tc::descAdvance(tc::smemDescSw64(bst + (0 + pb[pp]) * kBTile), kk * 32);
-              const uint64_t bi = tc::descAdvance(tc::smemDescSw64(bst + (2 + pb[pp]) * kBTile), kk * 32);
-              tc::mmaBf16(d, ar, br, idesc, acc);
+            for (int kk = 0; kk < 2; ++kk) {
+              if (hi <= c0 + 16 * kk || lo >= c0 + 16 * kk + 16)
+                continue;  // this 16-vertex step holds none of the group's vertices
+              const uint64_t xo = (s * kXStage + kk * 32) >> 4, bo = (slot * kBItem + kk * 32) >> 4;
+              const uint64_t ar = dA[0 + pa[pp]] + xo, ai = dA[2 + pa[pp]] + xo;
+              const uint64_t br = dB[0 + pb[pp]] + bo, bi = dB[2 + pb[pp]] + bo;
+              tc::mmaBf16(d, ar, br, idesc, 1);
               tc::mmaBf16(d, ai, bi, idesc, 1);
-              inited |= 1u << r;
             }
           }
           tc::commitTo(&empty_b[slot]);  // the builders may refill this slot once these MMAs finish
@@ -262,64 +308,76 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
     }
   }
   else {
-    // Builders: the same (chunk, site) item sequence as the MMA issuer.
+    // Builders: the same (chunk, site group) item sequence as the MMA issuer.
     const int bt = t - 64;
-    const int part = bt / 64, nrow = (bt / 4) % 16, q = bt % 4;  // B_re / B_im, row 2 w + p, vertices 8 q..
-    const int w = nrow / 2, p = nrow % 2;
     const float s_max = *smax;
-    // The CTA's twiddles T(w2, j) for all its vertices, scaled by their chunk's 2^12 s_c / s_max
-    // (exact: powers of two), into shared memory once, all loads of a thread in flight together.
-    {
-      const double2* Tsec = T + static_cast<long>(sd.vtx_off) * nw_ext + static_cast<long>(w2_0) * n;
-      const int total = kW * n_chunks * 32;
-      for (int i0 = bt; i0 < total; i0 += 4 * kBuilders) {
-        double2 v[4];
+    // A chunk's twiddles T(w2, j) (8 frequencies x 32 vertices, two per thread) are loaded one chunk
+    // ahead into registers, scaled by the chunk's 2^12 s_c / s_max (exact: powers of two) and
+    // stored into one of two buffers; one named barrier per chunk publishes them (and orders the
+    // reuse of the buffer the chunk before last read).
+    const double2* Tsec = T + static_cast<long>(sd.vtx_off) * nw_ext + static_cast<long>(w2_0) * n;
+    auto loadT = [&](int c, double2 (&v)[2]) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int i = i0 + u * kBuilders, wl = i / (n_chunks * 32), j = i % (n_chunks * 32);
-          v[u] = (i < total && j < n) ? Tsec[static_cast<long>(wl) * n + j] : make_double2(0., 0.);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int i = i0 + u * kBuilders, wl = i / (n_chunks * 32), j = i % (n_chunks * 32);
-          if (i < total) {
-            const float f = xs[j / 32] / s_max * kTScale;
-            Ts[wl * ts + j] = make_float2(static_cast<float>(v[u].x) * f, static_cast<float>(v[u].y) * f);
-          }
-        }
+      for (int u = 0; u < 2; ++u) {
+        const int i = bt + u * kBuilders, wl = i / 32, j = c * 32 + i % 32;
+        v[u] = (c < n_chunks && j < n) ? Tsec[static_cast<long>(wl) * n + j] : make_double2(0., 0.);
       }
-    }
-    namedSync128();
+    };
+    double2 tcur[2], tnext[2];
+    loadT(0, tcur);
+
     int item = 0;
     for (int c = 0; c < n_chunks; ++c) {
       const int c0 = c * 32;
-      for (int r = 0; r < kSites && ok; ++r) {
-        const int lo = cs[r], hi = cs[r + 1];
-        if (lo >= hi || hi <= c0 || lo >= c0 + 32)
-          continue;
+      loadT(c + 1, tnext);
+      {
+        const float f = xs[c] / s_max * kTScale;
+        float2* tb = Ts + (c & 1) * kW * 32;
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+          tb[bt + u * kBuilders] = make_float2(static_cast<float>(tcur[u].x) * f, static_cast<float>(tcur[u].y) * f);
+      }
+      namedSync128();
+      const float2* tb = Ts + (c & 1) * kW * 32;
+      int ra, rb;
+      chunkSites(cs, c0, n, ra, rb);
+      for (int g0 = ra; g0 <= rb && ok; g0 += kMaxGroup) {
+        const int ng = min(kMaxGroup, rb - g0 + 1);
         const int slot = item % kBSlots, use = item / kBSlots;
         if (use > 0 && !__all_sync(0xffffffffu, mbarWait(&empty_b[slot], (use - 1) & 1, err))) {
           ok = false;  // the issuer sees the missing item as a timeout of its own
           continue;
         }
-        // Row 2 w + p of B_re = (Tr, -Ti), of B_im = (Ti, Tr); vertices outside the site are zero.
-        float y[8];
+        // Units (part, row, 8 vertices): row 16 i + 2 w + p of B_re = (Tr, -Ti), of B_im = (Ti, Tr)
+        // for site g0 + i; vertices outside that site are zero.  ng units per thread.
+        for (int u = 0; u < ng; ++u) {
+          const int ui = bt + kBuilders * u;
+          const int q = ui % 4, row = (ui / 4) % (kN * ng), part = ui / (4 * kN * ng);
+          const int site = g0 + row / kN, w = (row % kN) / 2, p = row % 2;
+          const int lo = cs[site], hi = cs[site + 1];
+          float y[8];
 #pragma unroll
-        for (int x = 0; x < 8; ++x) {
-          const int jl = 8 * q + x, j = c0 + jl;
-          const float2 tv = Ts[w * ts + j];
-          const float val = part == 0 ? (p == 0 ? tv.x : -tv.y) : (p == 0 ? tv.y : tv.x);
-          y[x] = (j >= lo && j < hi) ? val : 0.f;
+          for (int x = 0; x < 8; ++x) {
+            const int jl = 8 * q + x, j = c0 + jl;
+            const float2 tv = tb[w * 32 + jl];
+            const float val = part == 0 ? (p == 0 ? tv.x : -tv.y) : (p == 0 ? tv.y : tv.x);
+            y[x] = (j >= lo && j < hi) ? val : 0.f;
+          }
+          tcg::Pack8 h, l;
+          tcg::split8(y, h, l);
+          unsigned char* bst = base + kOffB + slot * kBItem + (2 * part) * kBTile + sw64(row, q);
+          tcg::store8(reinterpret_cast<__half*>(bst), h);
+          tcg::store8(reinterpret_cast<__half*>(bst + kBTile), l);
         }
-        tcg::Pack8 h, l;
-        tcg::split8(y, h, l);
-        unsigned char* bst = base + kOffB + slot * kBItem + (2 * part) * kBTile + sw64(nrow, q);
-        tcg::store8(reinterpret_cast<__half*>(bst), h);
-        tcg::store8(reinterpret_cast<__half*>(bst + kBTile), l);
         fenceProxyAsync();  // generic-proxy writes -> the tensor core's reads
-        mbarArrive(&full_b[slot]);
+        __syncwarp();
+        if (lane == 0)
+          mbarArrive(&full_b[slot]);
         ++item;
       }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        tcur[u] = tnext[u];
     }
   }
 
@@ -336,15 +394,18 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
     unsigned char* stg = base + (warp - 2) * 32 * kEpiRowB;  // warp-private transpose buffer (X' stages)
     float2* gsec = G + g_sector_stride * (2 * sd.slot + sd.spin);
     float gabs = 0.f;
+    int kmr[16];  // FFT slot -> momentum, in registers
+#pragma unroll
+    for (int g = 0; g < 16; ++g)
+      kmr[g] = km[g];
     // The X' stages become the transpose buffers: every TMA load has landed and every MMA that
     // read them has completed (acc_full).
     for (int wp = 0; wp < kW / 2; ++wp) {
       float z4[16][4];  // slot g: (re, im) of w2 = 2 wp and 2 wp + 1
 #pragma unroll
       for (int g = 0; g < 16; ++g) {
-        const int r = rm[g];
-        if (cs[r] < cs[r + 1] && got)
-          ld32x32bx4(lane_addr + r * kN + 4 * wp, z4[g]);
+        if (got)  // every site's columns hold its sums (zero for sites without vertices)
+          ld32x32bx4(lane_addr + rm[g] * kN + 4 * wp, z4[g]);
         else
           z4[g][0] = z4[g][1] = z4[g][2] = z4[g][3] = 0.f;
       }
@@ -362,18 +423,19 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
 #pragma unroll
         for (int m = 0; m < 4; ++m)
           dft4tc(z[m], z[m + 4], z[m + 8], z[m + 12]);
-        const bool diag = w2 == w1;
-        const float2* cw = Cs + wl * 16;
-        const float2* dw = Ds + wl * 16;
+        const float2* cw = Cg + wl * 16;
         __syncwarp();  // the previous frequency's copy-out reads are done
 #pragma unroll
         for (int g = 0; g < 16; ++g) {
-          const int k2 = km[g];
-          float2 x = cmul(cw[k2], z[g]);
-          if (diag && k2 == k1)
-            x = cadd(x, dw[k2]);
+          const float2 x = cmul(cw[g], z[g]);
           gabs = fmaxf(gabs, fmaxf(fabsf(x.x), fabsf(x.y)));
-          *reinterpret_cast<float2*>(stg + lane * kEpiRowB + k2 * 8) = x;
+          *reinterpret_cast<float2*>(stg + lane * kEpiRowB + kmr[g] * 8) = x;
+        }
+        if (w2 == w1) {  // the delta term at k2 = k1 of the diagonal block
+          float2* e = reinterpret_cast<float2*>(stg + lane * kEpiRowB + k1 * 8);
+          const float2 x = cadd(*e, Ds[wl * 16 + k1]);
+          gabs = fmaxf(gabs, fmaxf(fabsf(x.x), fabsf(x.y)));
+          *e = x;
         }
         __syncwarp();
         // The warp's 32 rows (two (w1, w2) blocks of 16 k1 x 16 k2, 2 KB each, contiguous in G):
@@ -408,7 +470,7 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
 
 bool colFactorTcApplies(const TpDims& d, int D, int row0, int max_order) {
   return d.nb == 1 && d.nc == 16 && d.nw_ext % kW == 0 && D % 128 == 0 && row0 % 128 == 0 &&
-         colFactorTcSmem((max_order + 31) / 32 * 32) <= 227 * 1024;
+         colFactorTcSmem(max_order) <= 227 * 1024;
 }
 
 int launchColFactorTc(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G, long g_sector_stride, int* gmax,
@@ -418,17 +480,17 @@ int launchColFactorTc(const FrontendArgs& a, const FrontTcWorkspace& w, float2* 
   if (gmax)
     DCAACC_CUDA_CHECK(cudaMemsetAsync(gmax, 0, sizeof(int) * size_t(a.n_sectors), stream));
   const int row0 = d.half_g ? s.D / 2 : 0;
-  const int ts = std::max(32, (a.n_max + 31) / 32 * 32);  // at most the workspace's order bound
-  const size_t smem = colFactorTcSmem(ts);
+  const size_t smem = colFactorTcSmem(0);
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(colFactorTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   // Two CTAs per SM (their tensor memory halves fill it) need the largest shared-memory carveout.
   DCAACC_CUDA_CHECK(cudaFuncSetAttribute(colFactorTcKernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          int(cudaSharedmemCarveoutMaxShared)));
   const dim3 grid((s.D - row0) / 128, d.nw_ext / kW, a.n_sectors);
   colFactorTcKernel<<<grid, kThreads, smem, stream>>>(w.tm_ac, d, a.sectors, a.col_start, a.Tc, w.xInv, s.Dp, s.Kr,
-                                                       a.Fb, a.G0, G, g_sector_stride, gmax, row0, w.fft, ts, err);
+                                                       a.Fb, a.G0, G, g_sector_stride, gmax, row0, w.fft, err);
   DCAACC_LAUNCH_CHECK();
   return 1;
 }
 
 }  // namespace dcaacc
+
