@@ -216,6 +216,11 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
   tc::fenceAfterThreadSync();
   const uint32_t tmem = *tmem_slot;
   bool ok = true;
+  {  // the tile's scale s_max 2^-12 of the tensor-memory sums into the G0 factors (exact: powers of two)
+    const float zs = *smax * (1.f / kTScale);
+    for (int i = t; i < kW * 16; i += kThreads)
+      Cg[i] = make_float2(Cg[i].x * zs, Cg[i].y * zs);
+  }
   if (warp >= 2) {  // every site's sums start at zero, so that each MMA accumulates
     const uint32_t qa = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);
 #pragma unroll
@@ -390,7 +395,6 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
     const int rho = mt * 128 + row;
     const int k1 = rho % R, w1 = rho / R;
     const uint32_t lane_addr = tmem + (static_cast<uint32_t>(quarter * 32) << 16);
-    const float zs = *smax * (1.f / kTScale);
     unsigned char* stg = base + (warp - 2) * 32 * kEpiRowB;  // warp-private transpose buffer (X' stages)
     float2* gsec = G + g_sector_stride * (2 * sd.slot + sd.spin);
     float gabs = 0.f;
@@ -416,7 +420,7 @@ colFactorTcKernel(const __grid_constant__ CUtensorMap tmX, const TpDims dims, co
         float2 z[16];
 #pragma unroll
         for (int g = 0; g < 16; ++g)
-          z[g] = make_float2(z4[g][2 * h] * zs, z4[g][2 * h + 1] * zs);
+          z[g] = make_float2(z4[g][2 * h], z4[g][2 * h + 1]);
 #pragma unroll
         for (int b = 0; b < 4; ++b)
           dft4tc(z[4 * b], z[4 * b + 1], z[4 * b + 2], z[4 * b + 3]);
