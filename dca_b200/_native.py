@@ -149,6 +149,8 @@ def _load():
         "dcaacc_tp_get_g4_normalized": (i, [p, i, POINTER(c_double), sz]),
         "dcaacc_tp_set_fault_injection": (i, [p, i, ctypes.c_uint32]),
         "dcaacc_set_allocation_failure": (i, [ctypes.c_int64]),
+        "dcaacc_tp_g4_shard": (i, [i, i, i, POINTER(c_int32), POINTER(c_int32)]),
+        "dcaacc_tp_g4_place_shard": (i, [POINTER(TpConfig), i, i, POINTER(c_double), sz, POINTER(c_double), sz]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -300,6 +300,42 @@ int dcaacc_tp_compute_g_noalloc(const dcaacc_tp_config* cfg, const double* G0,
   return guard([&] { dcaacc::computeGNoAlloc(*cfg, G0, sectors, G_out, static_cast<cudaStream_t>(stream)); });
 }
 
+int dcaacc_tp_g4_shard(int32_t n_k_ex, int32_t rank, int32_t n_ranks, int32_t* first, int32_t* count) {
+  return guard([&] {
+    if (!first || !count)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "g4_shard: null output");
+    if (n_ranks < 1 || n_ranks > n_k_ex || rank < 0 || rank >= n_ranks)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "g4_shard: need 0 <= rank < n_ranks <= number of momentum transfers");
+    const int32_t base = n_k_ex / n_ranks, extra = n_k_ex % n_ranks;
+    *count = base + (rank < extra ? 1 : 0);
+    *first = rank * base + std::min(rank, extra);
+  });
+}
+
+int dcaacc_tp_g4_place_shard(const dcaacc_tp_config* cfg, int32_t rank, int32_t n_ranks, const double* shard,
+                             size_t shard_count, double* full, size_t full_count) {
+  if (!cfg)
+    return null_handle();
+  return guard([&] {
+    if (!shard || !full)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "g4_place_shard: null buffer");
+    if (cfg->n_bands < 1 || cfg->n_sites < 1 || cfg->n_w_half < 1 || cfg->n_w_ex < 1)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "g4_place_shard: bad sizes");
+    int32_t first = 0, count = 0;
+    if (dcaacc_tp_g4_shard(cfg->n_k_ex, rank, n_ranks, &first, &count) != DCAACC_OK)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, g_last_error);
+    // One (q, wq) slab: every entry with fixed transfers, contiguous since q and wq are the slowest indices.
+    const size_t nb = cfg->n_bands, nc = cfg->n_sites, nw = 2 * size_t(cfg->n_w_half);
+    const size_t slab = nb * nb * nb * nb * nc * nc * nw * nw;
+    const size_t nq = cfg->n_k_ex, nwq = cfg->n_w_ex;
+    if (full_count != slab * nq * nwq || shard_count != slab * size_t(count) * nwq)
+      throw dcaacc::Error(DCAACC_INVALID_ARG, "g4_place_shard: buffer sizes do not match the configuration");
+    for (size_t wq = 0; wq < nwq; ++wq)
+      std::memcpy(full + 2 * slab * (wq * nq + first), shard + 2 * slab * (wq * count),
+                  2 * slab * count * sizeof(double));
+  });
+}
+
 int dcaacc_tp_set_fault_injection(dcaacc_tp* acc, int32_t stop_step, uint32_t wait_polls) {
   if (!acc)
     return null_handle();

@@ -288,6 +288,27 @@ int dcaacc_tp_peek_g4_async(dcaacc_tp* acc, int32_t channel, size_t offset, size
 int dcaacc_tp_compute_g_noalloc(const dcaacc_tp_config* cfg, const double* G0,
                                 const dcaacc_sector* sectors, double* G_out, void* stream);
 
+/* Distributed G4: TpAccumulator<Parameters, DistType::LINEAR, GPU> (tp_accumulator_gpu.hpp:350-352,
+ * ringG :534-581; the slice bounds G4_[0].get_start() / get_end(), :421-423).  The reference gives
+ * each MPI rank one contiguous range of G4's linear index and passes every measurement's G around
+ * a ring of ranks so that each rank adds all of them into its range.  Here the ranges are whole
+ * momentum transfers: rank r of n_ranks owns the consecutive transfers [first, first + count) of
+ * the full transfer list (the first n_k_ex % n_ranks ranks one more), so that its slice is the G4
+ * of a handle created with k_ex = that sub-list (all frequency transfers, same channels); its
+ * entries are the full G4's with the same (q, wq) bit for bit, since no entry mixes transfers.  A
+ * rank feeds its handle every rank's measurements (the walkers' M and configurations are
+ * exchanged instead of G: an n x n M crosses the links in place of a D x D G, and recomputing a
+ * measurement's G costs less than moving it).  n_ranks must be in 1..n_k_ex.
+ *
+ * g4_shard writes rank's first transfer position and count.  g4_place_shard copies one channel of
+ * that rank's G4 slice (host memory, shard_count complex entries = the sub-list handle's
+ * dcaacc_tp_g4_size) into its place in the full G4 of cfg (host memory, full_count complex
+ * entries), layout (b1,b2,b3,b4,k1,w1,k2,w2,q,wq) on both sides; only cfg's sizes and transfer
+ * counts are read.  Host code only: neither touches a GPU. */
+int dcaacc_tp_g4_shard(int32_t n_k_ex, int32_t rank, int32_t n_ranks, int32_t* first, int32_t* count);
+int dcaacc_tp_g4_place_shard(const dcaacc_tp_config* cfg, int32_t rank, int32_t n_ranks, const double* shard,
+                             size_t shard_count, double* full, size_t full_count);
+
 /* Error-path testing (no reference counterpart; the reference has no device-side failure
  * detection on this path).  Every device wait of the library's kernels is bounded and, when it
  * runs out, sets an error word that the next synchronize / finalize turns into

@@ -91,6 +91,7 @@ dcaacc_tp_sign_sum dcaacc_tp_get_g4_normalized dcaacc_tp_static_device_fingerpri
 dcaacc_tp_mirror_mode dcaacc_tp_enable_timing dcaacc_tp_stage_times dcaacc_tp_set_graphs
 dcaacc_tp_graph_stats dcaacc_tp_tuning_settled dcaacc_tp_tuning_report dcaacc_tp_peek_g4
 dcaacc_tp_peek_g4_async dcaacc_tp_compute_g_noalloc dcaacc_tp_set_fault_injection
+dcaacc_tp_g4_shard dcaacc_tp_g4_place_shard
 dcaacc_sp_create dcaacc_sp_destroy dcaacc_sp_reset dcaacc_sp_accumulate dcaacc_sp_finalize
 dcaacc_sp_get_m_r_w dcaacc_sp_get_m_r_w_sqr dcaacc_sp_sum_to dcaacc_sp_get_single_measurement_m_r_w
 dcaacc_sp_get_single_measurement_f_tau dcaacc_sp_clear_single_measurement dcaacc_sp_f_tau_size
