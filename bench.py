@@ -571,6 +571,11 @@ def run_ours(args, world, rank, local):
     factorable = nb == 1 and nc == 16 and not fp64_main and not simt
     col_tc = factorable and col_env not in ("0", "1") and os.environ.get("DCAACC_TP_COL_FFT") != "0"
     factored_col = factorable and (col_tc or (col_env == "1" and os.environ.get("DCAACC_TP_COL_FFT") != "0"))
+    # 6 x 6 cluster with DCAACC_TP_FACTORED_COL=1: the column step factored on the CUDA cores with the
+    # 6 x 6 FFT.
+    wide_col = (nb == 1 and nc == 36 and not fp64_main and not simt and col_env == "1"
+                and os.environ.get("DCAACC_TP_COL_FFT") != "0")
+    factored_col = factored_col or wide_col
     if fp64_main:
         g4_path = "stream" if nb == 1 and nc * nc <= 256 and set(w.channels) <= {2, 3} else "fp64_other"
     elif simt:
@@ -589,7 +594,7 @@ def run_ours(args, world, rank, local):
                                    "staged": ["updateG4StagedKernel"],
                                    "pp3": ["updateG4PPMultibandKernel"],
                                    "stream": ["updateG4SinglebandStream"]}.get(g4_path, []),
-                     "col_transform": (["colFactorTcKernel"] if col_tc else
+                     "col_transform": (["colFactorTcKernel"] if col_tc else ["colFactorWideKernel"] if wide_col else
                                        ["colTwiddlePlanesKernel", "colFactorMmaKernel"] if factored_col
                                        else ["frontGemmKernel<1>"]),
                      "row_transform": ["frontGemmKernel<0>"],
@@ -649,7 +654,8 @@ def run_ours(args, world, rank, local):
             dense = mma = None
             kern = ("colFactorTcKernel (column step factored by orbital: per-site sums in tensor memory, "
                     "4 x 4 FFT, G0 factor)" if col_tc else
-                    "colTwiddlePlanesKernel + colFactorMmaKernel (orbital-factored column step)")
+                    "colFactorWideKernel (column step factored by orbital on the CUDA cores, 6 x 6 FFT, G0 factor)"
+                    if wide_col else "colTwiddlePlanesKernel + colFactorMmaKernel (orbital-factored column step)")
         elif dom == "col_transform":
             dense = per_step * float(np.sum(8.0 * D * D * ns)) * rows_done
             mma = per_step * float(np.sum((Dp // 128) ** 2 * rows_done * chunks * 24 * mma_flop))
@@ -667,8 +673,16 @@ def run_ours(args, world, rank, local):
             roof.update({"dense_form_flops": dense, "dense_form_tflops": dense / sec / 1e12,
                          "mma_issued_tflops": mma / sec / 1e12, "mma_frac_of_bf16_peak": mma / sec / 1e12 / bf16_tf})
         else:
-            roof["work_note"] = ("factored by orbital: the column NDFT per site on the tensor cores, then the 4 x 4 "
+            roof["work_note"] = ("factored by orbital: the column NDFT per site on the CUDA cores (FP32), then the "
+                                 "6 x 6 FFT over the sites; no dense product" if wide_col else
+                                 "factored by orbital: the column NDFT per site on the tensor cores, then the 4 x 4 "
                                  "FFT over the sites; no dense product")
+            # The same stage against HBM: it must read X' (four FP16 planes, 8 bytes per complex
+            # entry) and write G (FP32 complex) once, for the rows it computes.
+            mem_bytes = per_step * rows_done * float(np.sum(D * ns * 8.0 + D * D * 8.0))
+            roof["memory_view"] = {"algorithmic_bytes": mem_bytes, "achieved_gbs": mem_bytes / sec / 1e9,
+                                   "frac_of_hbm": mem_bytes / sec / 1e9 / hbm_gbs,
+                                   "note": "X' read and G written once per launch, for the rows computed"}
     else:
         # SIMT front-end stages are dominated by their global traffic (M / X' / G, complex of the
         # path's precision).

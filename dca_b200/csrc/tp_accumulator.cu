@@ -171,50 +171,52 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       }
     Fb_.alloc(fb.size());
     DCAACC_CUDA_CHECK(cudaMemcpy(Fb_.get(), fb.data(), Fb_.bytes(), cudaMemcpyHostToDevice));
-    // A 4 x 4 square cluster (integer sites (a, b), momenta 2 pi (m, n) / 4) makes the one-band
-    // cluster transform a 2D FFT: Fb(r, k) = e^{i 2 pi (m a + n b) / 4} Fb(r0, k), r0 the origin.
-    // Checked entry by entry; the column step uses it when it holds.
-    if (nb == 1 && nc == 16) {
-      int rmap[16], kmap[16], r0 = -1, ra[16], rb[16], km[16], kn[16];
-      std::fill(rmap, rmap + 16, -1);
-      std::fill(kmap, kmap + 16, -1);
+    // An L x L square cluster (L = 4 or 6; integer sites (a, b), momenta 2 pi (m, n) / L) makes
+    // the one-band cluster transform a 2D FFT: Fb(r, k) = e^{i 2 pi (m a + n b) / L} Fb(r0, k), r0
+    // the origin.  Checked entry by entry; the column step uses it when it holds.
+    if (nb == 1 && (nc == 16 || nc == 36)) {
+      const int L = nc == 16 ? 4 : 6;
+      int rmap[36], kmap[36], r0 = -1, ra[36], rb[36], km[36], kn[36];
+      std::fill(rmap, rmap + 36, -1);
+      std::fill(kmap, kmap + 36, -1);
       bool ok = true;
-      for (int r = 0; r < 16 && ok; ++r) {
+      for (int r = 0; r < nc && ok; ++r) {
         const double x = c.r_vecs[2 * r], y = c.r_vecs[2 * r + 1];
         const long a = std::lround(x), b = std::lround(y);
         ok = std::abs(x - a) < 1e-9 && std::abs(y - b) < 1e-9;
-        ra[r] = int(((a % 4) + 4) % 4);
-        rb[r] = int(((b % 4) + 4) % 4);
-        const int g = ra[r] + 4 * rb[r];
+        ra[r] = int(((a % L) + L) % L);
+        rb[r] = int(((b % L) + L) % L);
+        const int g = ra[r] + L * rb[r];
         ok = ok && rmap[g] < 0;
         rmap[g] = r;
         if (a == 0 && b == 0)
           r0 = r;
       }
-      for (int k = 0; k < 16 && ok; ++k) {
-        const double m = c.k_vecs[2 * k] * 4 / (2 * M_PI), n = c.k_vecs[2 * k + 1] * 4 / (2 * M_PI);
+      for (int k = 0; k < nc && ok; ++k) {
+        const double m = c.k_vecs[2 * k] * L / (2 * M_PI), n = c.k_vecs[2 * k + 1] * L / (2 * M_PI);
         const long mi = std::lround(m), ni = std::lround(n);
         ok = std::abs(m - mi) < 1e-9 && std::abs(n - ni) < 1e-9;
-        km[k] = int(((mi % 4) + 4) % 4);
-        kn[k] = int(((ni % 4) + 4) % 4);
-        const int g = km[k] + 4 * kn[k];
+        km[k] = int(((mi % L) + L) % L);
+        kn[k] = int(((ni % L) + L) % L);
+        const int g = km[k] + L * kn[k];
         ok = ok && kmap[g] < 0;
         kmap[g] = k;
       }
       ok = ok && r0 >= 0;
-      for (int k = 0; k < 16 && ok; ++k)
-        for (int r = 0; r < 16 && ok; ++r) {
+      for (int k = 0; k < nc && ok; ++k)
+        for (int r = 0; r < nc && ok; ++r) {
           const std::complex<double> f0(fb[size_t(k) * nc + r0].x, fb[size_t(k) * nc + r0].y);
           const std::complex<double> want =
-              std::exp(std::complex<double>(0, 2 * M_PI * (km[k] * ra[r] + kn[k] * rb[r]) / 4.0)) * f0;
+              std::exp(std::complex<double>(0, 2 * M_PI * (km[k] * ra[r] + kn[k] * rb[r]) / double(L))) * f0;
           ok = std::abs(want - std::complex<double>(fb[size_t(k) * nc + r].x, fb[size_t(k) * nc + r].y)) < 1e-9;
         }
       if (ok) {
         fft.on = 1;
         fft.r0 = r0;
-        for (int g = 0; g < 16; ++g) {
-          fft.rmap[g] = static_cast<unsigned char>(rmap[g]);
-          fft.kmap[g] = static_cast<unsigned char>(kmap[g]);
+        fft.L = L;
+        for (int g = 0; g < 36; ++g) {
+          fft.rmap[g] = static_cast<unsigned char>(g < nc ? rmap[g] : 0);
+          fft.kmap[g] = static_cast<unsigned char>(g < nc ? kmap[g] : 0);
         }
       }
     }
@@ -301,7 +303,10 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       // the dense GEMM) on tcgen05 with the per-site sums in tensor memory (tp_colfactor_tc.cu),
       // which also spares the dense step's Q operand.  DCAACC_TP_FACTORED_COL=0 keeps the dense
       // GEMM; =1 selects the other factored forms (mma.sync with the 4 x 4 FFT, or the CUDA cores
-      // with the 16 x 16 matrix transform, which DCAACC_TP_COL_FFT=0 forces), both slower.
+      // with the 16 x 16 matrix transform, which DCAACC_TP_COL_FFT=0 forces), both slower.  One
+      // band on a 6 x 6 cluster: DCAACC_TP_FACTORED_COL=1 selects the factored form on the CUDA
+      // cores with the 6 x 6 FFT (24x fewer flops than the dense GEMM, yet slower on B200: 57 ms
+      // against 39 ms per batch of 128 at Nw = 128).
       const char* fact_env = std::getenv("DCAACC_TP_FACTORED_COL");
       const char* fft_env = std::getenv("DCAACC_TP_COL_FFT");
       ftc_.fft = fft;
@@ -312,8 +317,9 @@ void TpAccumulator::init(const dcaacc_tp_config& c, const double* G0) {
       const int row0 = dims_.half_g ? fs.D / 2 : 0;
       ftc_.col_tc = !fact_off && !fact_on && colFactorApplies(dims_) && ftc_.fft.on &&
                     colFactorTcApplies(dims_, fs.D, row0, max_order_);
-      ftc_.factored_col = colFactorApplies(dims_) && (fact_on || ftc_.col_tc);
-      if (ftc_.factored_col && ftc_.fft.on && !ftc_.col_tc) {
+      const bool wide = colFactorWideApplies(dims_) && ftc_.fft.on && ftc_.fft.L == 6 && fact_on;
+      ftc_.factored_col = (colFactorApplies(dims_) && (fact_on || ftc_.col_tc)) || wide;
+      if (ftc_.factored_col && ftc_.fft.on && !ftc_.col_tc && !wide) {
         col_tp_.alloc(colTwiddlePlaneBytes(dims_, int(n_sec), fs.Kr));
         ftc_.tp = col_tp_.get();
       }

@@ -638,10 +638,270 @@ colFactorMmaKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, co
 
 }  // namespace tcf
 
+// ---- 6 x 6 clusters (one band, Nc = 36) on the CUDA cores ----
+//
+// The same two stages for a cluster whose per-site sums do not fit the 16-site tiles above.
+// CTA = (sector, 32 rows rho1, 8 frequencies w2), 8 warps, one CTA per SM.
+//  stage A  the warps take the sites one at a time from a shared counter (every site, empty ones
+//           included, so that each site's Z slot is written).  A warp stages its site's vertices
+//           in blocks of up to 32 in its own shared-memory area -- X' decoded from the row step's
+//           FP16 planes (hi + lo at the 32-vertex chunk's power-of-two scale, exact in FP32), lane
+//           = row, and conj T, lane = vertex -- and each lane sums a 4 x 2 tile of (rho1, w2) over
+//           them; the site's Z then goes to shared memory.  No CTA-wide barrier until every site
+//           is done, so a warp is never held up by the vertex counts of the other warps' sites.
+//  stage B  thread = one (rho1, w2) pair: the 6 x 6 FFT over the sites (6-point DFTs along both
+//           grid axes), the G0 factor and the delta term, written back over the pair's own Z
+//           slots in momentum order; then G leaves as whole 36-entry rows (k2 fastest), a warp
+//           writing 256 contiguous bytes per store instruction.
+// Work: 8 D NwExt n flops of site sums per sector (24x less than the dense GEMM's 8 D^2 n at
+// Nc = 36) plus the FFTs.
+namespace wide {
+
+constexpr int kRows = 32;                       // rows rho1 per CTA
+constexpr int kCols = 8;                        // frequencies w2 per CTA
+constexpr int kBlk = 32;                        // vertices per staged block of a site
+constexpr int kBP = kBlk + 1;                   // padded staging row (float2)
+constexpr int kWarps = 8;
+constexpr int kThreads = 32 * kWarps;           // = kRows * kCols: one (rho1, w2) pair per thread in stage B
+constexpr int kZP = kRows + 4;                  // Z row of one (site, w2), float2: conflict-free lane tiles
+constexpr int kZS = kCols * kZP + 1;            // one site's Z; odd, so that the output's reads spread
+constexpr int kStageW = (kRows + kCols) * kBP;  // one warp's staging: X' [kRows][kBP], conj T [kCols][kBP]
+static_assert(kThreads == kRows * kCols, "stage B: one pair per thread");
+
+template <int NC>
+constexpr size_t smemBytes() {
+  return sizeof(float2) * (size_t(NC) * kZS + size_t(kWarps) * kStageW + 2 * size_t(kCols) * NC) +
+         sizeof(int) * (3 * size_t(NC) + 2);
+}
+
+// X_m = sum_x e^{-2 pi i m x / 3} x_x in place.
+__device__ inline void dft3(float2& x0, float2& x1, float2& x2) {
+  constexpr float s = 0.86602540378443865f;  // sin(pi / 3)
+  const float2 t = cadd(x1, x2), u = csub(x1, x2);
+  const float2 m = make_float2(x0.x - 0.5f * t.x, x0.y - 0.5f * t.y);
+  const float2 v = make_float2(s * u.y, -s * u.x);  // -i s u
+  x0 = cadd(x0, t);
+  x1 = cadd(m, v);
+  x2 = csub(m, v);
+}
+
+// X_m = sum_x e^{-2 pi i m x / 6} z_x in place: 3-point DFTs of the even and odd samples, then
+// X_m = E_{m mod 3} + e^{-i pi m / 3} O_{m mod 3}.
+__device__ inline void dft6(float2& z0, float2& z1, float2& z2, float2& z3, float2& z4, float2& z5) {
+  constexpr float s = 0.86602540378443865f;
+  float2 e0 = z0, e1 = z2, e2 = z4, o0 = z1, o1 = z3, o2 = z5;
+  dft3(e0, e1, e2);
+  dft3(o0, o1, o2);
+  const float2 p1 = cmul(make_float2(0.5f, -s), o1);   // e^{-i pi / 3} O_1
+  const float2 p2 = cmul(make_float2(-0.5f, -s), o2);  // e^{-2 i pi / 3} O_2
+  z0 = cadd(e0, o0);
+  z3 = csub(e0, o0);
+  z1 = cadd(e1, p1);
+  z4 = csub(e1, p1);
+  z2 = cadd(e2, p2);
+  z5 = csub(e2, p2);
+}
+
+template <int NC, int L>
+__global__ void __launch_bounds__(kThreads, 1)
+colFactorWideKernel(const TpDims dims, const SectorDesc* __restrict__ sectors, const int* __restrict__ col_start,
+                    const double2* __restrict__ T, const __half* __restrict__ ac, const float* __restrict__ xInv,
+                    int Dp, int Kr, const double2* __restrict__ Fb, const double2* __restrict__ G0,
+                    float2* __restrict__ G, long g_sector_stride, int* __restrict__ gmax, int row0, const ColFft fft) {
+  static_assert(L == 6 && L * L == NC, "6 x 6 cluster");
+  extern __shared__ __align__(16) unsigned char smem[];
+  float2* Zs = reinterpret_cast<float2*>(smem);      // [site][w2][row], site stride kZS
+  float2* Sw = Zs + NC * kZS;                         // [warp] staging
+  float2* Cs = Sw + kWarps * kStageW;                 // [w2][k2] -(1/Nc) G0_s(k2, w2) conj Fb(r0, k2)
+  float2* Ds = Cs + kCols * NC;                       // [w2][k2] beta G0_s(k2, w2), the delta term
+  int* cs = reinterpret_cast<int*>(Ds + kCols * NC);  // [NC + 1] site starts (column order)
+  int* rm = cs + NC + 1;                              // [NC] FFT slot -> site
+  int* km = rm + NC;                                  // [NC] FFT slot -> momentum
+  int* next = km + NC;                                // the next unclaimed site
+
+  const int t = threadIdx.x, warp = t / 32, lane = t % 32;
+  const SectorDesc sd = sectors[blockIdx.z];
+  const int n = sd.n, nw_ext = dims.nw_ext, R = dims.R, D = R * nw_ext;
+  const int rho_0 = row0 + blockIdx.x * kRows, w2_0 = blockIdx.y * kCols;
+  const int kxc = Kr / 32;
+  const long plane = static_cast<long>(Dp) * 2 * Kr;
+  const __half* xp = ac + static_cast<long>(blockIdx.z) * 2 * plane;  // hi plane; lo at + plane
+  const float* xs_scale = xInv + static_cast<long>(blockIdx.z) * (Dp / 128) * kxc;
+  const double2* Tsec = T + static_cast<long>(sd.vtx_off) * nw_ext;  // T(w, j) at w n + j (column order)
+
+  for (int i = t; i <= NC; i += kThreads)
+    cs[i] = col_start[sd.orb_off + i];
+  if (t < NC) {
+    int rv = 0, kv = 0;
+#pragma unroll
+    for (int g = 0; g < NC; ++g)
+      if (g == t) {
+        rv = fft.rmap[g];
+        kv = fft.kmap[g];
+      }
+    rm[t] = rv;
+    km[t] = kv;
+  }
+  if (t == 0)
+    *next = 0;
+  {
+    const double2* g0s = G0 + static_cast<long>(sd.spin) * nw_ext * NC;  // G0_s(k, w) at k + NC w (one band)
+    for (int i = t; i < kCols * NC; i += kThreads) {
+      const int k = i % NC, w2 = w2_0 + i / NC;
+      double2 g0 = w2 < nw_ext ? g0s[k + NC * w2] : make_double2(0., 0.);
+      Ds[i] = make_float2(static_cast<float>(dims.beta * g0.x), static_cast<float>(dims.beta * g0.y));
+      const double2 f = Fb[k * NC + fft.r0];  // the band phase e^{-i k a}: conj Fb(r0, k) (x_r0 = 0)
+      g0 = make_double2(g0.x * f.x + g0.y * f.y, g0.y * f.x - g0.x * f.y);
+      Cs[i] = make_float2(static_cast<float>(-g0.x / NC), static_cast<float>(-g0.y / NC));
+    }
+  }
+  __syncthreads();
+
+  // Stage A.
+  const int rg = lane / 4, wg = lane % 4;  // lane tile: rows rg + 8 a, frequencies wg + 4 b
+  float2* Xw = Sw + warp * kStageW;        // [kRows][kBP]
+  float2* Tw = Xw + kRows * kBP;           // [kCols][kBP]
+  const int rho_l = rho_0 + lane;          // the row this lane stages
+  const bool row_in = rho_l < D;           // rows past D (last tile) stay zero
+  const __half* xrow = xp + static_cast<long>(row_in ? rho_l : 0) * 2 * Kr;
+  const float* srow = xs_scale + (row_in ? rho_l / 128 : 0) * kxc;
+  for (;;) {
+    int r = 0;
+    if (lane == 0)
+      r = atomicAdd(next, 1);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r >= NC)
+      break;
+    const int lo = cs[r], hi = cs[r + 1];
+    float2 acc[4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        acc[a][b] = make_float2(0.f, 0.f);
+    for (int b0 = lo; b0 < hi; b0 += kBlk) {
+      const int cnt = min(kBlk, hi - b0);
+      __syncwarp();  // the previous block's reads are done
+      // X'(rho_l, j) for j in [b0, b0 + cnt): 8-vertex groups (16-byte vectors of each plane part).
+      for (int g = b0 / 8; 8 * g < b0 + cnt; ++g) {
+        uint4 hr = make_uint4(0, 0, 0, 0), hm = hr, lr = hr, lm = hr;
+        float sc = 0.f;
+        if (row_in) {
+          const __half* p = xrow + 8 * g;
+          hr = *reinterpret_cast<const uint4*>(p);
+          hm = *reinterpret_cast<const uint4*>(p + Kr);
+          lr = *reinterpret_cast<const uint4*>(p + plane);
+          lm = *reinterpret_cast<const uint4*>(p + plane + Kr);
+          sc = srow[g / 4];  // the 32-vertex chunk of this group
+        }
+        const __half* a = reinterpret_cast<const __half*>(&hr);
+        const __half* b = reinterpret_cast<const __half*>(&hm);
+        const __half* c = reinterpret_cast<const __half*>(&lr);
+        const __half* d = reinterpret_cast<const __half*>(&lm);
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+          const int v = 8 * g + x - b0;
+          if (v >= 0 && v < cnt)
+            Xw[lane * kBP + v] = make_float2((__half2float(a[x]) + __half2float(c[x])) * sc,
+                                             (__half2float(b[x]) + __half2float(d[x])) * sc);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kCols; ++u) {
+        const int w2 = w2_0 + u;
+        const double2 tv =
+            (lane < cnt && w2 < nw_ext) ? Tsec[static_cast<long>(w2) * n + b0 + lane] : make_double2(0., 0.);
+        Tw[u * kBP + lane] = make_float2(static_cast<float>(tv.x), -static_cast<float>(tv.y));  // conj T
+      }
+      __syncwarp();
+#pragma unroll 2
+      for (int v = 0; v < cnt; ++v) {
+        float2 x[4], y[2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+          x[a] = Xw[(rg + 8 * a) * kBP + v];
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+          y[b] = Tw[(wg + 4 * b) * kBP + v];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b)
+            cfma(acc[a][b], x[a], y[b]);
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        Zs[r * kZS + (wg + 4 * b) * kZP + rg + 8 * a] = acc[a][b];
+  }
+  __syncthreads();  // Z of every site is in place
+
+  // Stage B: the pair (row, wl) -> G(rho; k2, w2) for all k2.
+  const int row = t % kRows, wl = t / kRows;
+  const int rho = rho_0 + row, w2 = w2_0 + wl;
+  float gabs = 0.f;
+  {
+    float2* zp = Zs + wl * kZP + row;  // slot of site r: zp[r * kZS]
+    float2 z[NC];
+#pragma unroll
+    for (int g = 0; g < NC; ++g)
+      z[g] = zp[rm[g] * kZS];
+#pragma unroll
+    for (int b = 0; b < L; ++b)  // along the first grid axis
+      dft6(z[L * b], z[L * b + 1], z[L * b + 2], z[L * b + 3], z[L * b + 4], z[L * b + 5]);
+#pragma unroll
+    for (int m = 0; m < L; ++m)  // along the second
+      dft6(z[m], z[m + L], z[m + 2 * L], z[m + 3 * L], z[m + 4 * L], z[m + 5 * L]);
+    const int k1 = rho % R, w1 = rho / R;
+    const bool diag = w2 == w1;  // the delta term sits at k2 = k1 of the diagonal block
+    const bool in = rho < D && w2 < nw_ext;
+    const float2* cw = Cs + wl * NC;
+    const float2* dw = Ds + wl * NC;
+#pragma unroll
+    for (int g = 0; g < NC; ++g) {
+      const int k2 = km[g];
+      float2 x = cmul(cw[k2], z[g]);
+      if (diag && k2 == k1)
+        x = cadd(x, dw[k2]);
+      if (in)
+        gabs = fmaxf(gabs, fmaxf(fabsf(x.x), fabsf(x.y)));
+      zp[k2 * kZS] = x;
+    }
+  }
+  __syncthreads();
+  // Out: segment s = row + kRows wl is G's row (k1, w1; w2) of NC entries k2, contiguous in G;
+  // consecutive segments are consecutive rows k1 of one (w1, w2) block.
+  float2* gsec = G + g_sector_stride * (2 * sd.slot + sd.spin);
+  for (int idx = t; idx < kRows * kCols * NC; idx += kThreads) {
+    const int s = idx / NC, k2 = idx % NC;
+    const int rs = s % kRows, ws = s / kRows;
+    const int rho_s = rho_0 + rs, w2_s = w2_0 + ws;
+    if (rho_s < D && w2_s < nw_ext) {
+      const int k1 = rho_s % R, w1 = rho_s / R;
+      gsec[((static_cast<long>(w1) * nw_ext + w2_s) * R + k1) * R + k2] = Zs[k2 * kZS + ws * kZP + rs];
+    }
+  }
+  if (gmax) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      gabs = fmaxf(gabs, __shfl_xor_sync(0xffffffffu, gabs, off));
+    if (lane == 0)
+      atomicMax(gmax + 2 * sd.slot + sd.spin, __float_as_int(gabs));
+  }
+}
+
+}  // namespace wide
+
 }  // namespace
 
 bool colFactorApplies(const TpDims& d) {
   return d.nb == 1 && d.nc == 16 && d.nw_ext % tcf::kCols == 0;
+}
+
+bool colFactorWideApplies(const TpDims& d) {
+  return d.nb == 1 && d.nc == 36;
 }
 
 size_t colTwiddlePlaneBytes(const TpDims& d, int n_sectors, int Kr) {
@@ -655,6 +915,17 @@ int launchColFactor(const FrontendArgs& a, const FrontTcWorkspace& w, float2* G,
   if (gmax)
     DCAACC_CUDA_CHECK(cudaMemsetAsync(gmax, 0, sizeof(int) * size_t(a.n_sectors), stream));
   const int row0 = d.half_g ? s.D / 2 : 0;  // half G: the rows of the upper frequency half
+  if (colFactorWideApplies(d)) {  // 6 x 6 cluster, the 6 x 6 FFT (the caller checked fft)
+    constexpr size_t smem = wide::smemBytes<36>();
+    auto k = wide::colFactorWideKernel<36, 6>;
+    DCAACC_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const dim3 grid((s.D - row0 + wide::kRows - 1) / wide::kRows, (d.nw_ext + wide::kCols - 1) / wide::kCols,
+                    a.n_sectors);
+    k<<<grid, wide::kThreads, smem, stream>>>(d, a.sectors, a.col_start, a.Tc, static_cast<const __half*>(w.ac),
+                                              w.xInv, s.Dp, s.Kr, a.Fb, a.G0, G, g_sector_stride, gmax, row0, w.fft);
+    DCAACC_LAUNCH_CHECK();
+    return 1;
+  }
   if (w.fft.on && w.tp) {
     auto* tp = static_cast<__half*>(w.tp);
     const long per = long(d.nw_ext) * s.Kr;

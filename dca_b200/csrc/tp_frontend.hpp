@@ -51,13 +51,14 @@ struct FrontTcShape {
   int n_sectors;
   size_t pr_elems, mb_elems, ac_elems, bq_elems;  // FP16 elements of P, M, X' and Q planes
 };
-// The cluster transform of a 4 x 4 square cluster as a 2D FFT: grid point g = a + 4 b is site
-// rmap[g] (coordinates (a, b)) and momentum kmap[g] (2 pi (a, b) / 4); r0 is the site at the
-// origin.  Set up on the host when the cluster's phase table has exactly that structure.
+// The cluster transform of an L x L square cluster (L = 4 or 6) as a 2D FFT: grid point g = a + L b
+// is site rmap[g] (coordinates (a, b)) and momentum kmap[g] (2 pi (a, b) / L); r0 is the site at
+// the origin.  Set up on the host when the cluster's phase table has exactly that structure.
 struct ColFft {
   int on;
   int r0;
-  unsigned char rmap[16], kmap[16];
+  int L;
+  unsigned char rmap[36], kmap[36];
 };
 
 struct FrontTcWorkspace {
@@ -72,7 +73,7 @@ struct FrontTcWorkspace {
   float* xInv = nullptr;   // [sector][Dp][Kr / 32] inverse scales of X' row chunks
   int n_sm = 0;            // SMs of the device (persistent GEMM grids)
   bool factored_col = false;  // the column step runs factored by orbital (tp_colfactor.cu), not as a GEMM
-  ColFft fft{};               // ... with its cluster transform as a 4 x 4 FFT (when fft.on)
+  ColFft fft{};               // ... with its cluster transform as an L x L FFT (when fft.on)
   void* tp = nullptr;         // ... FFT form: FP16 planes of the column twiddles (colTwiddlePlaneBytes)
   bool col_tc = false;        // ... FFT form with the per-site sums in tensor memory (tp_colfactor_tc.cu)
   CUtensorMap tm_pr, tm_mb, tm_ac, tm_bq;  // TMA descriptors of the four plane arrays
@@ -97,6 +98,8 @@ int launchFrontendTcCol(const FrontendArgs& a, const FrontTcWorkspace& w, float2
 // With the FFT cluster transform it runs on the tensor cores and needs colTwiddlePlaneBytes of
 // workspace (FrontTcWorkspace::tp); otherwise on the CUDA cores.
 bool colFactorApplies(const TpDims& d);
+// One band on a 36-site cluster: the factored column step with the 6 x 6 FFT (when ColFft has L = 6).
+bool colFactorWideApplies(const TpDims& d);
 size_t colTwiddlePlaneBytes(const TpDims& d, int n_sectors, int Kr);
 // The tensor-memory form (tp_colfactor_tc.cu): one band, 4 x 4 cluster, rows in whole 128-row tiles.
 bool colFactorTcApplies(const TpDims& d, int D, int row0, int max_order);

@@ -644,3 +644,32 @@ def test_factored_column_step_matches_dense(monkeypatch, full_g, fft, mode):
         print("factored / dense column step, relative errors:", rel_err(f, want), rel_err(d, want))
         assert rel_err(f, want) <= MIXED_TOL
         assert rel_err(d, want) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("full_g", ["0", "1"])
+def test_factored_column_step_6x6_matches_dense(monkeypatch, full_g):
+    """One band, 6 x 6 cluster (Nc = 36): the column step factored by orbital on the CUDA cores with
+    the 6 x 6 FFT (DCAACC_TP_FACTORED_COL=1) against the dense tensor-core GEMM (the default) and
+    the FP64 path, with half G (mirror symmetry) and with all of G.  An empty spin sector, and a
+    measurement whose 150 vertices sit on three sites (sites of more than one 32-vertex block)."""
+    import dataclasses
+    w = _small("c5", nw_half=32, n_sp=128, n_range=(30, 150))
+    case = case_from_workload(w, 6)
+    case.measurements[2] = W.make_measurement(w, 2, n_override=(0, 57))
+    m = W.make_measurement(w, 4, n_override=(150, 41))
+    rng = np.random.default_rng(11)
+    sites = rng.integers(0, 3, 150).astype(np.int32)
+    s0 = dataclasses.replace(m.sectors[0], left_site=sites, right_site=sites.copy())
+    case.measurements[4] = W.Measurement(m.sign, (s0, m.sectors[1]))
+    monkeypatch.setenv("DCAACC_TP_FULL_G", full_g)
+    monkeypatch.setenv("DCAACC_TP_FACTORED_COL", "1")
+    fact = _run_timed(case, False, monkeypatch, max_batch=4)
+    monkeypatch.delenv("DCAACC_TP_FACTORED_COL")
+    dense = _run_timed(case, False, monkeypatch, max_batch=4)
+    exact = run_gpu(case, precision=0, max_batch=1)
+    assert fact.mirror_mode() == dense.mirror_mode() == (0 if full_g == "1" else 3)
+    for f, d, want in zip(fact.get_G4(), dense.get_G4(), exact.get_G4()):
+        print("6x6 factored / dense column step, relative errors:", rel_err(f, want), rel_err(d, want))
+        assert not np.array_equal(f, d)  # two different column steps ran
+        assert rel_err(f, want) <= MIXED_TOL
+        assert rel_err(d, want) <= MIXED_TOL
