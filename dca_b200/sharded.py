@@ -18,7 +18,9 @@ benchmark configurations, whose G4 fits on one GPU, independent replicas (replic
 Exchange: one torch.distributed all_gather per accumulate call for the vertex data and signs (a
 host array, staged through the device on NCCL) and one for the M matrices, which stay on the
 device on NCCL and reach the accumulator as device M.  Every rank then feeds its handle the
-measurements of rank 0, 1, ..., n_ranks - 1 in that order.  get_G4 all-gathers the slices and
+measurements of rank 0, 1, ..., n_ranks - 1 in that order and processes them before the call
+returns (the gathered M buffers belong to the call), so a call should carry about a batch's worth
+of measurements across the ranks (max_batch / n_ranks per rank in mixed precision).  get_G4 all-gathers the slices and
 assembles the full G4 on every rank (dcaacc_tp_g4_place_shard).  In a single process without a
 process group the shard is the whole transfer list and nothing is exchanged.
 """
@@ -187,14 +189,27 @@ class ShardedTpAccumulator:
     def accumulate_batch(self, Ms: Sequence, configs: Sequence, signs: Sequence) -> float:
         """Collective: every rank's measurements of this call, in rank order, into this rank's slice.
         Returns the flops of this rank's handle."""
-        parts = [(Ms, configs, signs)] if self._dist is None else self._exchange(Ms, configs, signs)
+        if self._dist is None:
+            if hasattr(self.local, "accumulate_batch"):
+                return self.local.accumulate_batch(Ms, configs, signs)
+            return sum(self.local.accumulate(M_pair, cfg, s) or 0.0 for M_pair, cfg, s in zip(Ms, configs, signs))
+        parts = self._exchange(Ms, configs, signs)
         flops = 0.0
         for Ms_r, cf_r, sg_r in parts:
+            if not sg_r:
+                continue
             if hasattr(self.local, "accumulate_batch"):
                 flops += self.local.accumulate_batch(Ms_r, cf_r, sg_r) or 0.0
             else:
                 for M_pair, cfg, s in zip(Ms_r, cf_r, sg_r):
                     flops += self.local.accumulate(M_pair, cfg, s) or 0.0
+        # The gathered M buffers are this call's temporaries, while a mixed-precision handle reads a
+        # measurement's M only when its batch runs: process what is queued and wait for it before
+        # the buffers go (a rank's call returns with its handle idle).
+        if hasattr(self.local, "flush"):
+            self.local.flush()
+        if hasattr(self.local, "synchronizeCopy"):
+            self.local.synchronizeCopy()
         return flops
 
     def finalize(self):

@@ -192,29 +192,36 @@ def test_slices_on_one_gpu_assemble_the_full_g4(wname):
 @pytest.mark.gpu
 def test_exchange_over_a_one_rank_nccl_group():
     """The sharded accumulator over a real NCCL group (one rank on this GPU): device-resident M goes
-    through the all_gather and reaches the handle as device M; the result is the plain handle's."""
+    through the all_gather and reaches the handle as device M; the result is the plain handle's, in
+    FP64 and in mixed precision with batches larger than a call (each call processes what it
+    gathered before its buffers go; freshly allocated tensors in between would expose a late read)."""
     import torch
     import torch.distributed as dist
     from dca_b200.accumulators import TpAccumulator
     from dca_b200.sharded import ShardedTpAccumulator
     case, _ = golden("sq2_all")
-    ms = case.measurements
-    p = case.tp_params()
-    want = _fill(TpAccumulator(case.G0, p), ms)
+    ms = case.measurements * 3
     os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(_free_port())})
     torch.cuda.set_device(0)
     dist.init_process_group("nccl", rank=0, world_size=1)
     try:
-        acc = ShardedTpAccumulator(case.G0, p)
-        assert acc.n_ranks == 1 and acc.shard == (0, len(p.k_ex))
-        acc.resetAccumulation(0)
-        for m in ms:
-            Md = [torch.from_numpy(np.asarray(s.M)).cuda() for s in m.sectors]
-            acc.accumulate(Md, list(m.sectors), m.sign)
-        acc.finalize()
-        got = acc.get_G4()
-        torch.cuda.synchronize()
+        for precision, tol in ((0, 1e-13), (1, 1e-6)):
+            p = case.tp_params(precision=precision, max_batch=4)
+            want = _fill(TpAccumulator(case.G0, case.tp_params()), ms)
+            acc = ShardedTpAccumulator(case.G0, p)
+            assert acc.n_ranks == 1 and acc.shard == (0, len(p.k_ex))
+            acc.resetAccumulation(0)
+            for m in ms:
+                Md = [torch.from_numpy(np.asarray(s.M)).cuda() for s in m.sectors]
+                acc.accumulate(Md, list(m.sectors), m.sign)
+                del Md
+                # Fresh allocations of the gathered buffers' sizes take their freed blocks back.
+                junk = [torch.full((k,), float("nan"), dtype=torch.float64, device="cuda") for k in (1, 16, 256, 2048)]
+                del junk
+            acc.finalize()
+            got = acc.get_G4()
+            torch.cuda.synchronize()
+            for g, w in zip(got, want):
+                assert rel_err(g, w) <= tol, (precision, rel_err(g, w))
     finally:
         dist.destroy_process_group()
-    for g, w in zip(got, want):
-        assert rel_err(g, w) <= 1e-13
