@@ -717,15 +717,15 @@ def run_ours(args, world, rank, local):
 
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "fp64" if fp64_main else "fp32 (G, G4 partials) + fp64 (running G4)",
         "data": "synthetic (seeded; dca_b200.workloads)",
-        "config": {"workload": w.describe(),
-                   "measurements_per_step": B, "precision": args.precision,
-                   "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2 (G4 {len(w.channels) * n_g4 * 16 / 1e6:.0f} MB, "
-                         f"G {B * 2 * D * D * 8 / 1e9:.1f} GB per batch)"},
+        "config": bench_config(w, world),
+        "warmup_batches_run": warmup,
+        "warmup_note": "untimed batches: at least --warmup, and on until the launch-shape tuner has settled "
+                       "and both CUDA graphs exist",
+        "measurements_per_step": B, "precision": args.precision,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "cuda_graphs": graph_info,
@@ -753,6 +753,20 @@ def run_ours(args, world, rank, local):
     return result
 
 
+def bench_config(w, world):
+    """The workload both arms measure (the same dict in both lines): the configuration with its
+    batch, how the GPU arm spreads it, and its data sizes against L2."""
+    cl = w.cluster()
+    nwe = 2 * w.nw_half + 2 * w.ext()
+    D = w.nb * cl.nc * nwe
+    n_g4 = w.nb ** 4 * cl.nc ** 2 * (2 * w.nw_half) ** 2 * len(w.exchange_momenta(cl.nc)) * len(w.exchange_frequencies())
+    g4_mb, g_gb = len(w.channels) * n_g4 * 16 / 1e6, w.batch * 2 * D * D * 8 / 1e9
+    big = g4_mb + 1e3 * g_gb > 126.0
+    return {"workload": w.describe(), "parallelism": f"replicas x{world}",
+            "l2": f"inputs {'larger' if big else 'smaller'} than L2 (G4 {g4_mb:.0f} MB, G {g_gb:.1f} GB per batch)"
+                  + ("" if big else "; L2 is not flushed between steps")}
+
+
 def run_reference_arm(args, world, rank):
     """The reference's CPU accumulator on the host cores: one step = one measurement in each of the
     P processes.  The run is bounded to a few minutes: at most 2 warm-up and 6 timed steps, and
@@ -770,8 +784,8 @@ def run_reference_arm(args, world, rank):
             "ms_per_step": 1e3 * cb["window_s"] / timed,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
             "data": "synthetic (seeded; dca_b200.workloads)",
-            "config": {"workload": w.describe(with_batch=False),
-                       "parallelism": f"{cb['cores']} CPU processes, one per core"},
+            "config": bench_config(w, world),
+            "parallelism": f"{cb['cores']} CPU processes, one per core, one measurement at a time each",
             "cpu_baseline": cb,
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
