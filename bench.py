@@ -769,14 +769,14 @@ def bench_config(w, world):
 
 def run_reference_arm(args, world, rank):
     """The reference's CPU accumulator on the host cores: one step = one measurement in each of the
-    P processes.  The run is bounded to a few minutes: at most 2 warm-up and 6 timed steps, and
-    the line reports the steps actually timed."""
+    P processes.  The run is bounded to a few minutes (about 3 s per c3 measurement and core): at
+    most 5 warm-up and 20 timed steps, and the line reports the steps actually run."""
     from dca_b200 import workloads as W
     w = workload(args)
     if rank != 0:
         return None
-    timed = max(1, min(args.steps, 6))
-    warm = min(args.warmup, 2)
+    timed = max(1, min(args.steps, 20))
+    warm = min(args.warmup, 5)
     cb = run_cpu_reference(w, timed, warm)
     val = cb["value"]
     return {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
