@@ -17,7 +17,7 @@ per-spin expansion orders n ~ U[50, 400], batches of 64 measurements, synthetic 
              value_blocking_readback: the same loop with a blocking read per step
   roofline   the dominant stage, timed with CUDA events on the accumulator's stream around each
              stage's launches, in a second pass over the same steps (eager launches): the
-             survey's algorithmic flops (front-end stages) or bytes (G4 update) per launch over
+             algorithmic flops (front-end stages) or bytes (G4 update) per launch over
              that time, against the measured dense BF16 peak or HBM copy bandwidth
              (MEASURED_PEAKS.json); update_g4_roofline gives the G4 stage in every run, with the
              DRAM bytes its kernels actually move (committed ncu capture) beside the effective rate
@@ -542,7 +542,8 @@ def run_ours(args, world, rank, local):
     ns = np.array([s.n for m in pool for s in m.sectors], dtype=np.float64)  # both batches of the pool
     per_step = B / len(pool)  # sectors of one step = per_step * (all sectors of the pool)
 
-    # Algorithmic work of each stage, per step (one batch), from the survey's per-spin counts:
+    # Algorithmic work of each stage, per step (one batch), from the per-spin counts of the reference's
+    # two-stage NDFT, cluster transform and G0 products (no dense reformulation credited):
     # row step 8 NwExt n^2 (row NDFT) + 8 Nc D^2 (row half of the cluster transform); column step
     # 8 NwExt^2 n_orb n (column NDFT) + 8 Nc D^2 (column half) + 12 D^2 (G0 epilogue, one band) or
     # 16 nb D^2; G4 update: the FP64 read-modify-write of every running-G4 entry of every channel
@@ -640,7 +641,7 @@ def run_ours(args, world, rank, local):
             if k in g4_roof:
                 roof[k] = g4_roof[k]
     elif dom in ("col_transform", "row_transform") and tc_front:
-        # Tensor-core front-end: the survey's algorithmic flops against the measured dense BF16 peak.
+        # Tensor-core front-end: the algorithmic flops against the measured dense BF16 peak.
         # Beside it, the work the kernel is built to do (the dense complex product over all vertices,
         # split FP16: three MMAs per complex multiply-add pair) and its issued MMA rate (128 x 128
         # tiles, K padded to 32) against the same peak.
@@ -666,8 +667,8 @@ def run_ours(args, world, rank, local):
             kern = "frontGemmKernel<0> (row step, X' = P M)"
         roof = {"kernel": kern, "bound": "tensor", "achieved": alg_flops[dom] / sec / 1e12, "peak": bf16_tf,
                 "unit": "TFLOP/s", "algorithmic_flops": alg_flops[dom],
-                "peak_note": "measured dense BF16 burst peak; algorithmic flops per the survey's per-spin "
-                             "count, so the dense reformulation's extra work is not credited",
+                "peak_note": "measured dense BF16 burst peak; algorithmic flops per spin of the reference's "
+                             "two-stage form, so the dense reformulation's extra work is not credited",
                 }
         if dense is not None:
             roof.update({"dense_form_flops": dense, "dense_form_tflops": dense / sec / 1e12,

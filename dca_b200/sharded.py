@@ -20,8 +20,8 @@ host array, staged through the device on NCCL) and one for the M matrices, which
 device on NCCL and reach the accumulator as device M.  Every rank then feeds its handle the
 measurements of rank 0, 1, ..., n_ranks - 1 in that order and processes them before the call
 returns (the gathered M buffers belong to the call), so a call should carry about a batch's worth
-of measurements across the ranks (max_batch / n_ranks per rank in mixed precision).  get_G4 all-gathers the slices and
-assembles the full G4 on every rank (dcaacc_tp_g4_place_shard).  In a single process without a
+of measurements across the ranks (max_batch / n_ranks per rank in mixed precision).  get_G4
+all-gathers the slices and assembles the full G4 on every rank (dcaacc_tp_g4_place_shard).  In a single process without a
 process group the shard is the whole transfer list and nothing is exchanged.
 """
 
