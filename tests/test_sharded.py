@@ -150,6 +150,52 @@ def test_gloo_ranks_assemble_the_full_g4(tmp_path, oracle_lib, world):
             assert np.array_equal(sl[c], want_sl.reshape(-1, order="F"))
 
 
+def _uneven_rank(rank, world, port, out_dir):
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    import torch.distributed as dist
+    from dca_b200 import replicas
+    from dca_b200.sharded import ShardedTpAccumulator
+    replicas.init_from_env("gloo", timeout_s=60)
+    try:
+        case, _ = golden("sq2_all")
+        ms = case.measurements
+        acc = ShardedTpAccumulator(case.G0, case.tp_params(), local_factory=_OracleAdapter)
+        acc.resetAccumulation(0)
+        for call in _uneven_calls(ms, rank):
+            acc.accumulate_batch([[s.M for s in m.sectors] for m in call], [list(m.sectors) for m in call],
+                                 [m.sign for m in call])
+        acc.finalize()
+        np.save(os.path.join(out_dir, f"g4_{rank}.npy"), np.stack(acc.get_G4()))
+    finally:
+        dist.destroy_process_group()
+
+
+def _uneven_calls(ms, rank):
+    """Three collective calls in which the ranks bring different numbers of measurements, none
+    included: rank 0 brings 2, 0, 1; rank 1 brings 0, 3, 1."""
+    return [[ms[0], ms[1]], [], [ms[2]]] if rank == 0 else [[], [ms[2], ms[0], ms[1]], [ms[0]]]
+
+
+def test_gloo_ranks_with_uneven_calls(tmp_path, oracle_lib):
+    """The exchange gathers parts of different lengths (and empty ones) per call; every rank adds
+    them in call order, rank 0's part first, and assembles the same G4 as one oracle fed that order."""
+    import torch.multiprocessing as mp
+    world = 2
+    mp.spawn(_uneven_rank, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    case, _ = golden("sq2_all")
+    ms = case.measurements
+    ref = oracle_lib.OracleTp(case.G0, case.tp_params())
+    per_rank = [_uneven_calls(ms, r) for r in range(world)]
+    for i in range(3):
+        for r in range(world):
+            for m in per_rank[r][i]:
+                ref.accumulate([s.M for s in m.sectors], list(m.sectors), m.sign)
+    want = np.stack(ref.get_G4())
+    for rank in range(world):
+        assert np.array_equal(np.load(tmp_path / f"g4_{rank}.npy"), want)
+
+
 def _fill(acc, ms):
     acc.resetAccumulation(0)
     for m in ms:
